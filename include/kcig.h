@@ -1,0 +1,149 @@
+/*
+ * kcig.h -- C ABI of the B200 adjoint angle-domain Kirchhoff CIG migration.
+ *
+ * Drop-in replacement for the adjoint (adj=1) path of the reference tool
+ * kirchmig2d_cig (src/kirchmig2d_cig.cpp) and of the library routines it
+ * calls (SERECKIRCH/include/kirmig.h, SERECKIRCH/include/tinterpsr.h).  All
+ * arguments are plain pointers and sizes.  No entry point exits the process:
+ * every function returns KCIG_OK (0) or a negative KCIG_ERR_* status, and
+ * kcig_last_error() gives the message the reference would have printed.
+ *
+ * Array layouts follow the reference files exactly:
+ *   data   [ns][nh][nt]   (time fastest)                 seismic_data=
+ *   tables [npos][nx][nz] (depth fastest, index ix*nz+iz) stable= sderiv= rtable= rderiv=
+ *   image  [ng][nx][nz]                                   migration=
+ */
+#ifndef KCIG_H
+#define KCIG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KCIG_OK 0
+#define KCIG_ERR_ARG (-1)         /* invalid parameter or size                    */
+#define KCIG_ERR_CUDA (-2)        /* a CUDA call failed                           */
+#define KCIG_ERR_IO (-3)          /* file missing, truncated or malformed         */
+#define KCIG_ERR_UNSUPPORTED (-4) /* valid for the reference, not built here      */
+#define KCIG_ERR_NOMEM (-5)       /* device or host allocation failed             */
+#define KCIG_ERR_DEVICE (-6)      /* a kernel reported a bounded-wait or bounds fault */
+
+#define KCIG_MEM_HOST 0   /* pointer is ordinary or pinned host memory         */
+#define KCIG_MEM_DEVICE 1 /* pointer is device memory of the plan's device      */
+
+/* Parameters of kirchmig2d_cig.  Field meanings and defaults are those of
+ * src/kirchmig2d_cig.cpp:494-958; kcig_params_init() fills the defaults. */
+typedef struct kcig_params {
+    int adj;                 /* 1 = migration (only adj=1 is built)           :565-568 */
+    int cig;                 /* 0 stack, 1 common-image gathers               :569-572 */
+    int cig_is_angle;        /* mode=angle (1) or mode=offset (0)             :554-563 */
+    int cmp;                 /* receiver position = s+h (1) or h (0)          :573-576 */
+    int half_angle;          /* 0 full opening angle, 1 half                  :585-586 */
+    int isdiff;              /* diff=1: central derivative after doubint      :599     */
+    int interp_type;         /* 'h' Hermite, 'l' linear, 'p' partial          :952-958 */
+    int angle_interp;        /* two-bin linear (1) or nearest-bin (0)          :845-846 */
+    int angle_grad_radius;   /* finite-difference radius, >=1                  :851-854 */
+    int angle_smooth;        /* triangle smoothing radius, 0 = off             :855-858 */
+    int aperture_trace;      /* -1 = no trace-index aperture                   :544-548 */
+    int aperture_trace_taper;/*                                                 :859-862 */
+    int direct_mute;         /*                                                 :707-762 */
+    int direct_mute_invert;
+    int direct_mute_qc_shot; /* -1 = no QC dump (CLI only)                      */
+    float tau, aperture, aperture_taper, aperture_rmin, aperture_rtaper, antialias;
+    float angle_taper_start, angle_taper_end;
+    float oazmin, oazmax, oaztaper;
+    float direct_mute_slope, direct_mute_intercept, direct_mute_taper;
+    /* output axis as given (parse_output_axis, :323-368); resolved per plan */
+    int axis_min_given, axis_max_given, axis_step_given, axis_n_given;
+    float axis_min, axis_max, axis_step;
+    int axis_n;
+} kcig_params;
+
+/* Axes of the data cube and of the traveltime tables (header values as the
+ * reference reads them, cast to float: :651-661, :765-802). */
+typedef struct kcig_geometry {
+    int nt, nh, ns;
+    float t0, dt, h0, dh, s0, ds;
+    int nz, nx;
+    float z0, dz, x0, dx;
+    int sny;
+    float sy0, sdy;
+    int rny;
+    float ry0, rdy;
+} kcig_geometry;
+
+typedef struct kcig_plan kcig_plan;
+
+/* Message of the last failing call on this thread (never NULL). */
+const char *kcig_last_error(void);
+
+/* Reference defaults (kirchmig2d_cig.cpp:494-958 with mode=angle unset). */
+int kcig_params_init(kcig_params *p);
+
+/* Parse key=value tokens and par=<file> exactly as se_par_init +
+ * kirchmig2d_cig's parameter block do (SEFILESYSTEM/src/se_par_sep.cpp:185-340,
+ * src/kirchmig2d_cig.cpp:494-958), including the validation errors of the
+ * direct mute.  argv[0] is skipped.  File keys (seismic_data=, ...) are
+ * ignored here; kcig_run_cli handles them. */
+int kcig_params_parse(int argc, char **argv, kcig_params *p);
+
+/* Resolve the output (n3,o3,d3) axis for these data axes, as
+ * parse_output_axis (src/kirchmig2d_cig.cpp:323-368). */
+int kcig_output_axis(const kcig_params *p, const kcig_geometry *g, int *ng, float *g0, float *dg);
+
+/* Create a migration plan on the current CUDA device.  Validates sizes like
+ * the reference's dimension checks (:651-661, :765-802).  scratch_bytes caps
+ * the plan's device scratch (0 = choose from free device memory). */
+int kcig_plan_create(const kcig_params *p, const kcig_geometry *g, unsigned long long scratch_bytes,
+                     kcig_plan **out);
+int kcig_plan_destroy(kcig_plan *plan);
+
+/* Use this CUDA stream (cudaStream_t) for all work of the plan (0 = legacy). */
+int kcig_plan_set_stream(kcig_plan *plan, void *stream);
+
+/* Traveltime tables and their position derivatives ([npos][nx][nz]).  Host
+ * tables are copied to the device; device tables are used in place and must
+ * outlive the plan.  Passing the same stable/rtable pointers shares one copy. */
+int kcig_plan_set_tables(kcig_plan *plan, const float *stable, const float *sderiv,
+                         const float *rtable, const float *rderiv, int memory);
+
+/* Optional spatial gradient volumes sgradx/sgradz/rgradx/rgradz (all four or
+ * none, :627-642), same layout as the tables. */
+int kcig_plan_set_gradients(kcig_plan *plan, const float *sgradx, const float *sgradz,
+                            const float *rgradx, const float *rgradz, int memory);
+
+/* Adjoint migration: image[ng][nx][nz] = sum over traces (zeroed first, as
+ * the reference memsets out, :964-965).  data and image are both host or both
+ * device pointers (memory).  Replaces the shot/trace loop :979-1339. */
+int kcig_migrate(kcig_plan *plan, const float *data, float *image, int memory);
+
+/* Number of summation-kernel launches and the device time (ms, CUDA events)
+ * of the last kcig_migrate; either pointer may be NULL. */
+int kcig_plan_last_stats(const kcig_plan *plan, int *sum_launches, float *sum_ms, int *all_launches);
+
+/* The drop-in executable: same argv, files, defaults, messages and exit
+ * status as kirchmig2d_cig adj=1.  Returns 0 on success, else a KCIG_ERR_*. */
+int kcig_run_cli(int argc, char **argv);
+
+/* ---- building blocks, device buffers, on `stream` ----------------------- */
+
+/* SERECKIRCH/src/kirmig.cpp:8-24 doubint (+ :381-394 diff2 when isdiff=1)
+ * for ntr traces of nt samples: in [ntr][nt] float, out [ntr][nt] double
+ * (each causal/anticausal running sum accumulated in FP64). */
+int kcig_doubint_device(const float *in, double *out, int ntr, int nt, int isdiff, float dt,
+                        void *stream);
+
+/* Leg fields of one source (is_source=1) or receiver position of a plan with
+ * tables set, [nx][nz] each: traveltime T (double), position derivative Tx
+ * (float, not scaled by the data spacing), direction phi = atan2(gz, gx) of
+ * the stabilised traveltime gradient (double; NaN where the gradient
+ * vanishes) and the aperture leg weight w (float) --
+ * src/kirchmig2d_cig.cpp:987-1052 (source), :1148-1201 (receiver), :226-269.
+ * Any output pointer may be NULL. */
+int kcig_leg_fields_device(kcig_plan *plan, int is_source, double pos, double *T, float *Tx,
+                           double *phi, float *w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KCIG_H */

@@ -1,0 +1,214 @@
+"""B200-native adjoint angle-domain Kirchhoff CIG migration (kirchmig2d_cig adj=1).
+
+The compute path is the in-tree CUDA library ``libkcig.so`` (C ABI declared in
+include/kcig.h).  This module is its thin Python face, mirroring the
+reference's interface: parameters are the tool's own ``key=value`` strings,
+arrays use the reference layouts (data [ns][nh][nt], tables [npos][nx][nz],
+image [ng][nx][nz]).  There is no CPU implementation behind it: if the
+library is missing or no GPU is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
+           "run_cli", "doubint_device", "leg_fields_device", "library_path", "cli_path"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+library_path = os.path.join(_HERE, "libkcig.so")
+cli_path = os.path.join(_HERE, "bin", "kirchmig2d_cig")
+
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+
+class KcigError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("kcig error %d: %s" % (code, msg))
+        self.code = code
+        self.msg = msg
+
+
+class Params(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "adj", "cig", "cig_is_angle", "cmp", "half_angle", "isdiff", "interp_type", "angle_interp",
+        "angle_grad_radius", "angle_smooth", "aperture_trace", "aperture_trace_taper", "direct_mute",
+        "direct_mute_invert", "direct_mute_qc_shot")] + [(n, ctypes.c_float) for n in (
+        "tau", "aperture", "aperture_taper", "aperture_rmin", "aperture_rtaper", "antialias",
+        "angle_taper_start", "angle_taper_end", "oazmin", "oazmax", "oaztaper", "direct_mute_slope",
+        "direct_mute_intercept", "direct_mute_taper")] + [(n, ctypes.c_int) for n in (
+        "axis_min_given", "axis_max_given", "axis_step_given", "axis_n_given")] + [
+        (n, ctypes.c_float) for n in ("axis_min", "axis_max", "axis_step")] + [("axis_n", ctypes.c_int)]
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("nt", "nh", "ns")] + \
+               [(n, ctypes.c_float) for n in ("t0", "dt", "h0", "dh", "s0", "ds")] + \
+               [(n, ctypes.c_int) for n in ("nz", "nx")] + \
+               [(n, ctypes.c_float) for n in ("z0", "dz", "x0", "dx")] + \
+               [("sny", ctypes.c_int)] + [(n, ctypes.c_float) for n in ("sy0", "sdy")] + \
+               [("rny", ctypes.c_int)] + [(n, ctypes.c_float) for n in ("ry0", "rdy")]
+
+
+_lib = None
+
+
+def lib():
+    """Load libkcig.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(library_path):
+            raise ImportError("libkcig.so is missing: build it with `python -m kirch_datuming_b200.build` (%s)"
+                              % library_path)
+        L = ctypes.CDLL(library_path)
+        P, G = ctypes.POINTER(Params), ctypes.POINTER(Geometry)
+        vp, fp, dp = ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p
+        L.kcig_last_error.restype = ctypes.c_char_p
+        L.kcig_params_init.argtypes = [P]
+        L.kcig_params_parse.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), P]
+        L.kcig_output_axis.argtypes = [P, G, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                       ctypes.POINTER(ctypes.c_float)]
+        L.kcig_plan_create.argtypes = [P, G, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+        L.kcig_plan_destroy.argtypes = [vp]
+        L.kcig_plan_set_stream.argtypes = [vp, vp]
+        L.kcig_plan_set_tables.argtypes = [vp, fp, fp, fp, fp, ctypes.c_int]
+        L.kcig_plan_set_gradients.argtypes = [vp, fp, fp, fp, fp, ctypes.c_int]
+        L.kcig_migrate.argtypes = [vp, fp, fp, ctypes.c_int]
+        L.kcig_plan_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
+                                           ctypes.POINTER(ctypes.c_int)]
+        L.kcig_run_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+        L.kcig_doubint_device.argtypes = [fp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp]
+        L.kcig_leg_fields_device.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, fp, dp, fp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise KcigError(rc, lib().kcig_last_error().decode())
+
+
+def _argv(tokens):
+    toks = ["kirchmig2d_cig"] + [str(t) for t in tokens]
+    arr = (ctypes.c_char_p * len(toks))(*[t.encode() for t in toks])
+    return len(toks), arr
+
+
+def params(*tokens, **kw) -> Params:
+    """kcig_params from kirchmig2d_cig key=value tokens (and/or keywords)."""
+    toks = list(tokens) + ["%s=%s" % (k, v) for k, v in kw.items()]
+    p = Params()
+    argc, argv = _argv(toks)
+    _check(lib().kcig_params_parse(argc, argv, ctypes.byref(p)))
+    return p
+
+
+def geometry(**kw) -> Geometry:
+    g = Geometry()
+    for k, v in kw.items():
+        setattr(g, k, v)
+    return g
+
+
+def output_axis(p: Params, g: Geometry):
+    ng, g0, dg = ctypes.c_int(), ctypes.c_float(), ctypes.c_float()
+    _check(lib().kcig_output_axis(ctypes.byref(p), ctypes.byref(g), ctypes.byref(ng), ctypes.byref(g0),
+                                  ctypes.byref(dg)))
+    return ng.value, g0.value, dg.value
+
+
+def _ptr(a):
+    """(pointer, memory kind) of a numpy array or a CUDA torch tensor."""
+    if a is None:
+        return None, MEM_HOST
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data, MEM_HOST
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr(), (MEM_DEVICE if a.is_cuda else MEM_HOST)
+    raise TypeError(type(a))
+
+
+class Plan:
+    """One migration set-up: kcig_plan_create + tables, then migrate() calls."""
+
+    def __init__(self, p: Params, g: Geometry, scratch_bytes: int = 0, stream=None):
+        self._h = ctypes.c_void_p()
+        _check(lib().kcig_plan_create(ctypes.byref(p), ctypes.byref(g), scratch_bytes, ctypes.byref(self._h)))
+        self.params, self.geometry = p, g
+        self.ng, self.g0, self.dg = output_axis(p, g)
+        self._keep = []
+        if stream is not None:
+            _check(lib().kcig_plan_set_stream(self._h, ctypes.c_void_p(stream)))
+
+    def set_tables(self, stable, sderiv, rtable=None, rderiv=None):
+        rtable = stable if rtable is None else rtable
+        rderiv = sderiv if rderiv is None else rderiv
+        ptrs = [_ptr(x) for x in (stable, sderiv, rtable, rderiv)]
+        mem = {m for _, m in ptrs}
+        if len(mem) != 1:
+            raise ValueError("tables must all be host or all be device arrays")
+        self._keep += [stable, sderiv, rtable, rderiv]
+        _check(lib().kcig_plan_set_tables(self._h, *[p for p, _ in ptrs], mem.pop()))
+
+    def set_gradients(self, sgradx, sgradz, rgradx, rgradz):
+        ptrs = [_ptr(x) for x in (sgradx, sgradz, rgradx, rgradz)]
+        self._keep += [sgradx, sgradz, rgradx, rgradz]
+        _check(lib().kcig_plan_set_gradients(self._h, *[p for p, _ in ptrs], ptrs[0][1]))
+
+    def migrate(self, data, image):
+        (dp_, m1), (ip, m2) = _ptr(data), _ptr(image)
+        if m1 != m2:
+            raise ValueError("data and image must both be host or both be device arrays")
+        _check(lib().kcig_migrate(self._h, dp_, ip, m1))
+        return image
+
+    def stats(self):
+        a, b, c = ctypes.c_int(), ctypes.c_float(), ctypes.c_int()
+        _check(lib().kcig_plan_last_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"sum_launches": a.value, "sum_ms": b.value, "launches": c.value}
+
+    def close(self):
+        if self._h:
+            lib().kcig_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_cli(args) -> int:
+    """In-process kirchmig2d_cig; returns 0 or the negative KCIG_ERR_* code."""
+    argc, argv = _argv(args)
+    return lib().kcig_run_cli(argc, argv)
+
+
+def doubint_device(traces, isdiff: int = 0, dt: float = 1.0, stream=None):
+    """doubint (+diff2) of a CUDA float32 tensor [ntr][nt] -> float64 tensor."""
+    import torch
+    if not (traces.is_cuda and traces.dtype == torch.float32 and traces.is_contiguous()):
+        raise ValueError("expects a contiguous CUDA float32 tensor")
+    ntr, nt = traces.shape
+    out = torch.empty((ntr, nt), dtype=torch.float64, device=traces.device)
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    _check(lib().kcig_doubint_device(traces.data_ptr(), out.data_ptr(), ntr, nt, int(isdiff), float(dt),
+                                     ctypes.c_void_p(st)))
+    torch.cuda.current_stream().synchronize()
+    return out
+
+
+def leg_fields_device(plan: Plan, is_source: int, pos: float):
+    """(T float64, Tx float32, phi float64, w float32) device tensors [nx*nz] of one leg."""
+    import torch
+    g = plan.geometry
+    n = g.nz * g.nx
+    T, phi = (torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(2))
+    Tx, w = (torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(2))
+    _check(lib().kcig_leg_fields_device(plan._h, int(is_source), float(pos), T.data_ptr(), Tx.data_ptr(),
+                                        phi.data_ptr(), w.data_ptr()))
+    return T, Tx, phi, w

@@ -1,0 +1,106 @@
+// Internal declarations shared by the kcig sources (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/kcig.h"
+
+namespace kcig {
+
+// ------------------------------------------------------------------ errors --
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+#define KCIG_CUDA(call)                                               \
+    do {                                                              \
+        cudaError_t e__ = (call);                                     \
+        if (e__ != cudaSuccess) return ::kcig::cuda_error(e__, #call); \
+    } while (0)
+
+#define KCIG_TRY(expr)            \
+    do {                          \
+        int rc__ = (expr);        \
+        if (rc__ != KCIG_OK) return rc__; \
+    } while (0)
+
+// Interpolation of one leg (source or receiver) along the table position
+// axis, resolved on the host in double precision from the reference's
+// branch rules (src/kirchmig2d_cig.cpp:987-1029 and :1148-1180).
+struct LegInterp {
+    int i0;        // left slice
+    int i1;        // right slice, or -1: take slice i0 unchanged (clamped end)
+    int type;      // 'h', 'l', 'p'
+    int k1, k2;    // 'p' slice shifts (tinterpsr.cpp:86-87)
+    double c[4];   // T  = c0*p0 + c1*m0 + c2*p1 + c3*m1
+    double e[4];   // Tx = e0*p0 + e1*m0 + e2*p1 + e3*m1
+    double t, dxp; // in-interval fraction and position spacing ('p')
+    int gi0, gi1;  // gradient-volume slices (interp_volume_linear_stream, :294-322)
+    double gw;     // weight of gi1 (0: copy gi0)
+    double pos;    // surface position of the leg (aperture)
+    float scale;   // ds (source) or dh (receiver): Tx is stored as Tx*scale
+};
+
+// Device views of a batch of leg fields.  The opening angle of a pair is the
+// difference of the two legs' gradient directions, so each leg stores the
+// polar angle phi = atan2(gz, gx) of its stabilised gradient (FP64, NaN when
+// the gradient vanishes) instead of the two components.
+struct LegFields {
+    double2 *TP;  // [n][nzx] {traveltime T, gradient direction phi}
+    float2 *XW;   // [n][nzx] {Tx*scale, aperture leg weight}
+};
+
+struct FieldArgs {
+    const float *tab, *der;       // [npos][nzx]
+    const float *gxv, *gzv;       // gradient volumes or null
+    const LegInterp *legs;        // [n] device
+    int n, nz, nx;
+    float dz, dx, x0;
+    int radius, smooth, angle, use_grad;
+    float aper, aper_taper, rmin, rtaper;
+};
+
+// Workspace for the gradient pipeline: 4 double planes per position.
+int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st);
+
+struct PreludeArgs {
+    const float *data;      // [ns][nh][nt] whole data cube on the device
+    double2 *D;             // [ntr][nt] {D[i], D[i+1]}, ntr = nshots * nhc
+    const double *mute_sx;  // [ntr] source x (mute)   (null: no mute)
+    const double *mute_rx;  // [ntr] receiver x (mute)
+    int ntr, nt, isdiff, invert;
+    int nh, nhc, shot0, rcv0;  // batch = shots shot0.., receivers rcv0..rcv0+nhc-1
+    double t0, dt, slope, intercept, taper;
+};
+int launch_prelude(const PreludeArgs &a, cudaStream_t st);
+int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdiff, double dt,
+                         cudaStream_t st);
+
+struct SumArgs {
+    const double2 *STP;    // [nsb][nzx] source {T, phi}
+    const float2 *SXW;     // [nsb][nzx] source {Tx*ds, w}
+    const double2 *RTP;    // [nrf][nzx] receiver {T, phi}
+    const float2 *RXW;     // [nrf][nzx] receiver {Tx*dh, w}
+    const double2 *D;      // [ntr][nt]
+    const float *trw;      // [nsb*nh] trace weight, 0 = skip
+    const int *rfi;        // [nsb*nh] receiver field index
+    const int *igo;        // [nsb*nh] offset-mode bin
+    float *image;          // [ng][nzx]
+    int zero_init;
+    int nz, nx, nt, nsb, nh, ng;
+    int mode;              // 0 angle two-bin, 1 angle nearest, 2 single bin (offset/stack)
+    int shared_r;          // receiver fields indexed by ih only (cmp=0)
+    int half;
+    double t0, dt, inv_dt, tau;
+    double deg;            // radians -> output degrees (180/pi, halved for half_angle)
+    double ug0, uinv;      // u = (deg*theta - g0) * uinv, the bin coordinate
+    float dtf, aal, g0, dg;
+    float oazmin, oazmax, oaztaper, ats, ate;
+    int gchunk0, gchunk1;  // bin range handled by this launch
+};
+int launch_sum(const SumArgs &a, cudaStream_t st, int *launches);
+
+}  // namespace kcig

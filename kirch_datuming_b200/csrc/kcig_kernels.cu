@@ -1,0 +1,611 @@
+// sm_100a kernels of the adjoint angle-domain Kirchhoff summation.
+//
+//   K1 k_prelude      per-trace direct mute + doubint (FP64 running sums) +
+//                     optional diff2, written as {D[i], D[i+1]} pairs so a
+//                     linear-interpolated pick is one 16-byte load.
+//   K2 k_leg_*        per source/receiver position: table interpolation along
+//                     the position axis, traveltime gradient, triangle
+//                     smoothing and the aperture leg weight ("leg fields").
+//   K3 k_sum          the summation: one CTA owns an image tile, keeps its
+//                     angle bins in shared memory, and loops over every trace.
+//
+// Reference: src/kirchmig2d_cig.cpp (the adj=1 loop :979-1339),
+// SERECKIRCH/src/kirmig.cpp (doubint :8-24, kirmig_pick :34-58) and
+// SERECKIRCH/src/tinterpsr.cpp (:37-188).
+#include <math.h>
+#include <stdio.h>
+
+#include "kcig_common.h"
+
+namespace kcig {
+
+static constexpr double kPi = 3.14159265358979323846;
+
+// =============================================================== K1 prelude ==
+// One warp per trace.  The trace is staged in shared memory as double, muted
+// (kirchmig2d_cig.cpp:110-129), then integrated causally and anticausally
+// (kirmig.cpp:8-24) with every running sum in FP64: each lane scans a
+// contiguous chunk and a warp scan of the chunk totals links the chunks.
+// FP64 sums keep the later second differences (the pick) accurate, which an
+// FP32 running sum of a long trace does not.
+__device__ __forceinline__ double warp_excl_scan(double v, double *total)
+{
+    const int lane = threadIdx.x & 31;
+    double x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    *total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+__device__ __forceinline__ double warp_excl_suffix_scan(double v, double *total)
+{
+    const int lane = threadIdx.x & 31;
+    double x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double y = __shfl_down_sync(0xffffffffu, x, o);
+        if (lane + o < 32) x += y;
+    }
+    *total = __shfl_sync(0xffffffffu, x, 0);
+    return x - v;
+}
+
+__device__ void doubint_warp(double *s, int nt)
+{
+    const int lane = threadIdx.x & 31;
+    const int chunk = (nt + 31) / 32;
+    const int a = min(nt, lane * chunk), b = min(nt, a + chunk);
+    double tot, loc = 0.0;
+    for (int i = a; i < b; i++) loc += s[i];
+    double off = warp_excl_scan(loc, &tot);
+    for (int i = a; i < b; i++) { off += s[i]; s[i] = off; }
+    __syncwarp();
+    loc = 0.0;
+    for (int i = a; i < b; i++) loc += s[i];
+    off = warp_excl_suffix_scan(loc, &tot);
+    for (int i = b - 1; i >= a; i--) { off += s[i]; s[i] = off; }
+    __syncwarp();
+}
+
+__device__ void diff2_warp(double *s, int nt, double dt)
+{
+    // kirchmig2d_cig.cpp:381-394: central difference, one-sided at the ends.
+    // Each lane rewrites its chunk in place, carrying the original values of
+    // the neighbours it still needs; chunk-boundary neighbours are read first.
+    const int lane = threadIdx.x & 31;
+    if (nt < 2) return;
+    const int chunk = (nt + 31) / 32;
+    const int a = min(nt, lane * chunk), b = min(nt, a + chunk);
+    double prev = (a > 0 && a < nt) ? s[a - 1] : 0.0;
+    const double nextv = (b < nt && a < b) ? s[b] : 0.0;
+    double cur = (a < b) ? s[a] : 0.0;
+    __syncwarp();
+    for (int i = a; i < b; i++) {
+        const double nx = (i + 1 < b) ? s[i + 1] : nextv;
+        double v;
+        if (i == 0) v = (nx - cur) / dt;
+        else if (i == nt - 1) v = (cur - prev) / dt;
+        else v = (nx - prev) / (2.0 * dt);
+        s[i] = v;
+        prev = cur;
+        cur = nx;
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
+{
+    extern __shared__ double smem_d[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tr = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (tr >= a.ntr) return;
+    double *s = smem_d + (size_t)warp * a.nt;
+    const int k = tr / a.nhc, r = tr % a.nhc;
+    const float *x = a.data + ((size_t)(a.shot0 + k) * a.nh + (a.rcv0 + r)) * a.nt;
+    double boundary = 0.0;
+    const bool mute = a.mute_sx != nullptr;
+    if (mute) {
+        const double off = a.slope * fabs(a.mute_rx[tr] - a.mute_sx[tr]);
+        boundary = a.invert ? a.intercept - off : a.intercept + off;
+    }
+    for (int i = lane; i < a.nt; i += 32) {
+        double v = (double)x[i];
+        if (mute) {
+            const double t = a.t0 + (double)i * a.dt;
+            double w = 0.0;
+            if (t >= boundary + a.taper) w = 1.0;
+            else if (t > boundary) w = 0.5 * (1.0 - cos(kPi * ((t - boundary) / a.taper)));
+            v *= w;
+        }
+        s[i] = v;
+    }
+    __syncwarp();
+    doubint_warp(s, a.nt);
+    if (a.isdiff == 1) diff2_warp(s, a.nt, a.dt);
+    double2 *out = a.D + (size_t)tr * a.nt;
+    for (int i = lane; i < a.nt; i += 32) {
+        double2 e;
+        e.x = s[i];
+        e.y = (i + 1 < a.nt) ? s[i + 1] : 0.0;
+        out[i] = e;
+    }
+}
+
+__global__ void __launch_bounds__(64) k_doubint_plain(const float *in, double *out, int ntr, int nt,
+                                                      int isdiff, double dt)
+{
+    extern __shared__ double smem_d[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tr = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (tr >= ntr) return;
+    double *s = smem_d + (size_t)warp * nt;
+    for (int i = lane; i < nt; i += 32) s[i] = (double)in[(size_t)tr * nt + i];
+    __syncwarp();
+    doubint_warp(s, nt);
+    if (isdiff == 1) diff2_warp(s, nt, dt);
+    for (int i = lane; i < nt; i += 32) out[(size_t)tr * nt + i] = s[i];
+}
+
+static int prelude_block(int nt, int *warps)
+{
+    const size_t per = (size_t)nt * sizeof(double);
+    if (per * 2 <= 96 * 1024) { *warps = 2; return 0; }
+    if (per <= 200 * 1024) { *warps = 1; return 0; }
+    return -1;
+}
+
+int launch_prelude(const PreludeArgs &a, cudaStream_t st)
+{
+    if (a.ntr <= 0) return KCIG_OK;
+    int warps;
+    if (prelude_block(a.nt, &warps))
+        return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", a.nt);
+    const size_t sm = (size_t)warps * a.nt * sizeof(double);
+    KCIG_CUDA(cudaFuncSetAttribute(k_prelude, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_prelude<<<(a.ntr + warps - 1) / warps, 32 * warps, sm, st>>>(a);
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
+int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdiff, double dt,
+                         cudaStream_t st)
+{
+    if (ntr <= 0) return KCIG_OK;
+    int warps;
+    if (prelude_block(nt, &warps))
+        return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", nt);
+    const size_t sm = (size_t)warps * nt * sizeof(double);
+    KCIG_CUDA(cudaFuncSetAttribute(k_doubint_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_doubint_plain<<<(ntr + warps - 1) / warps, 32 * warps, sm, st>>>(in, out, ntr, nt, isdiff, dt);
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
+// ============================================================ K2 leg fields ==
+// kirchmig2d_cig.cpp:226-269: raised-cosine aperture legs, max-combined with
+// the shallow floor disk.  Evaluated once per (position, image point) instead
+// of once per pair: the value depends only on this leg.
+__device__ double leg_cone(double leg, double aper, double band)
+{
+    if (!isfinite(leg)) return 0.0;
+    if (band <= 0.0) return (leg <= aper) ? 1.0 : 0.0;
+    const double inner = aper - band;
+    if (leg <= inner) return 1.0;
+    if (leg >= aper) return 0.0;
+    return 0.5 * (1.0 + cos(kPi * ((leg - inner) / band)));
+}
+
+__device__ double leg_floor(double d, double rmin, double rt)
+{
+    if (rmin <= 0.0) return 0.0;
+    if (rt <= 0.0) return (d <= rmin) ? 1.0 : 0.0;
+    const double inner = rmin - rt;
+    if (inner <= 0.0) {
+        if (d >= rmin) return 0.0;
+        return 0.5 * (1.0 + cos(kPi * (d / rmin)));
+    }
+    if (d <= inner) return 1.0;
+    if (d >= rmin) return 0.0;
+    return 0.5 * (1.0 + cos(kPi * ((d - inner) / rt)));
+}
+
+// Table interpolation (tinterpsr.cpp:37-188) in double, aperture weight, and
+// the input-gradient interpolation (kirchmig2d_cig.cpp:294-322).
+__global__ void k_leg_interp(FieldArgs a, LegFields out, double *work)
+{
+    const int nzx = a.nz * a.nx;
+    const int j = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nzx) return;
+    const LegInterp L = a.legs[j];
+    const size_t base = (size_t)j * nzx;
+    double T, Tx;
+    if (L.i1 < 0) {
+        T = a.tab[(size_t)L.i0 * nzx + i];
+        Tx = a.der[(size_t)L.i0 * nzx + i];
+    } else if (L.type == 'p') {
+        // tinterp_partial / dinterp_partial (tinterpsr.cpp:72-140).  The
+        // reference's right-slice derivative terms index below the slice for
+        // the first k2 lateral columns (tinterpsr.cpp:119-124), and with one
+        // lateral column a one-sided term indexes past it; such an index is
+        // clamped to the first/last column at the same depth, so every read
+        // stays inside the table.
+        const float *p0 = a.tab + (size_t)L.i0 * nzx, *p1 = a.tab + (size_t)L.i1 * nzx;
+        const int n1 = a.nz, k1 = L.k1, k2 = L.k2, nn = nzx;
+        const double t = L.t, dd = a.dx, dxp = L.dxp;
+        auto cl = [&](int j) -> int { return j < 0 ? i % n1 : (j >= nn ? nn - n1 + i % n1 : j); };
+        auto P1 = [&](int j) -> double { return (double)p1[cl(j)]; };
+        auto P0 = [&](int j) -> double { return (double)p0[cl(j)]; };
+        if (i - k1 * n1 >= 0 && i + k2 * n1 < nn) {
+            T = (1.0 - t) * p0[i - k1 * n1] + t * p1[i + k2 * n1];
+            double dv = (-(double)p0[i - k1 * n1] + p1[i + k2 * n1]) / dxp;
+            if (i - (k1 + 1) * n1 >= 0 && i - (k1 - 1) * n1 < nn)
+                dv -= (1.0 - t) * (-(double)p0[i - (k1 + 1) * n1] + p0[i - (k1 - 1) * n1]) / (2.0 * dd);
+            else if (i - (k1 + 1) * n1 < 0)
+                dv -= (1.0 - t) * (-(double)p0[i - k1 * n1] + P0(i - (k1 - 1) * n1)) / dd;
+            else
+                dv -= (1.0 - t) * (-(double)p0[i - (k1 + 1) * n1] + p0[i - k1 * n1]) / dd;
+            if (i - (k2 + 1) * n1 >= 0 && i - (k2 - 1) * n1 < nn)
+                dv -= t * (-(double)p1[i - (k2 + 1) * n1] + p1[i - (k2 - 1) * n1]) / (2.0 * dd);
+            else if (i - (k2 + 1) * n1 < 0)
+                dv -= t * (-P1(i - k2 * n1) + P1(i - (k2 - 1) * n1)) / dd;
+            else
+                dv -= t * (-(double)p1[i - (k2 + 1) * n1] + p1[i - k2 * n1]) / dd;
+            Tx = dv;
+        } else {
+            T = (1.0 - t) * p0[i] + t * p1[i];
+            Tx = (-(double)p0[i] + p1[i]) / dxp;
+        }
+    } else {
+        const double p0 = a.tab[(size_t)L.i0 * nzx + i], p1 = a.tab[(size_t)L.i1 * nzx + i];
+        const double m0 = a.der[(size_t)L.i0 * nzx + i], m1 = a.der[(size_t)L.i1 * nzx + i];
+        T = L.c[0] * p0 + L.c[1] * m0 + L.c[2] * p1 + L.c[3] * m1;
+        Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
+    }
+    const int iz = i % a.nz, ix = i / a.nz;
+    const double dz = a.dz;
+    const double zdist = fmax(fabs((double)iz * dz), fmax(1.0e-12, 1.0e-6 * fabs(dz)));
+    const double ximg = (double)a.x0 + (double)ix * (double)a.dx;
+    const double d = fabs(L.pos - ximg);
+    const double legdeg = atan(d / zdist) * 180.0 / kPi;
+    const double w = fmax(leg_cone(legdeg, a.aper, a.aper_taper), leg_floor(d, a.rmin, a.rtaper));
+    out.TP[base + i] = make_double2(T, 0.0);
+    // reference: stablex[i]*ds, an FP32 product of the FP32 table derivative
+    out.XW[base + i] = make_float2((float)Tx * L.scale, (float)w);
+    if (a.angle && a.use_grad) {
+        double gx, gz;
+        const size_t s0 = (size_t)L.gi0 * nzx + i;
+        if (L.gw == 0.0) {
+            gx = a.gxv[s0];
+            gz = a.gzv[s0];
+        } else {
+            const size_t s1 = (size_t)L.gi1 * nzx + i;
+            gx = (1.0 - L.gw) * a.gxv[s0] + L.gw * a.gxv[s1];
+            gz = (1.0 - L.gw) * a.gzv[s0] + L.gw * a.gzv[s1];
+        }
+        work[(size_t)j * 4 * nzx + i] = gx;
+        work[(size_t)j * 4 * nzx + nzx + i] = gz;
+    }
+}
+
+// compute_grad_plane (kirchmig2d_cig.cpp:130-152, :424-435) in double.
+__global__ void k_leg_fd(FieldArgs a, LegFields out, double *work)
+{
+    const int nzx = a.nz * a.nx;
+    const int j = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nzx) return;
+    const double2 *T = out.TP + (size_t)j * nzx;
+    const int iz = i % a.nz, ix = i / a.nz;
+    const int r = a.radius < 1 ? 1 : a.radius;
+    double gx = 0.0, gz = 0.0;
+    if (a.nx > 1 && a.dx != 0.0f) {
+        const int il = max(0, ix - r), ir = min(a.nx - 1, ix + r);
+        if (ir != il) gx = (T[(size_t)ir * a.nz + iz].x - T[(size_t)il * a.nz + iz].x) / ((double)(ir - il) * a.dx);
+    }
+    if (a.nz > 1 && a.dz != 0.0f) {
+        const int it = max(0, iz - r), ib = min(a.nz - 1, iz + r);
+        if (ib != it) gz = (T[(size_t)ix * a.nz + ib].x - T[(size_t)ix * a.nz + it].x) / ((double)(ib - it) * a.dz);
+    }
+    work[(size_t)j * 4 * nzx + i] = gx;
+    work[(size_t)j * 4 * nzx + nzx + i] = gz;
+}
+
+// One box average (kirchmig2d_cig.cpp:438-466) along z (axis=0) or x (axis=1)
+// of planes pin -> pout of every position (component c: planes c and c+2).
+__global__ void k_box(int nz, int nx, int r, int axis, int pin, int pout, double *work)
+{
+    const int nzx = nz * nx;
+    const int j = blockIdx.y;
+    const int c = blockIdx.z;  // component
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nzx) return;
+    const double *in = work + ((size_t)j * 4 + pin + c) * nzx;
+    double *o = work + ((size_t)j * 4 + pout + c) * nzx;
+    const int iz = i % nz, ix = i / nz;
+    double s = 0.0;
+    int a0, b0;
+    if (axis == 0) {
+        a0 = max(0, iz - r); b0 = min(nz - 1, iz + r);
+        for (int k = a0; k <= b0; k++) s += in[(size_t)ix * nz + k];
+    } else {
+        a0 = max(0, ix - r); b0 = min(nx - 1, ix + r);
+        for (int k = a0; k <= b0; k++) s += in[(size_t)k * nz + iz];
+    }
+    o[i] = s / (double)(b0 - a0 + 1);
+}
+
+// Direction of the stabilised gradient.  scattering_angle_deg_from_grad
+// (:171-187) returns NaN when either gradient vanishes; phi = NaN carries that.
+__global__ void k_leg_pack(FieldArgs a, LegFields out, const double *work)
+{
+    const int nzx = a.nz * a.nx;
+    const int j = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nzx) return;
+    const double gx = work[(size_t)j * 4 * nzx + i];
+    const double gz = work[(size_t)j * 4 * nzx + nzx + i];
+    double2 *tp = out.TP + (size_t)j * nzx + i;
+    const double phi = (sqrt(gx * gx + gz * gz) <= 1.0e-12) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                             : atan2(gz, gx);
+    tp->y = phi;
+}
+
+int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st)
+{
+    if (a.n <= 0) return KCIG_OK;
+    const int nzx = a.nz * a.nx;
+    const dim3 blk(256), grd((nzx + 255) / 256, a.n);
+    k_leg_interp<<<grd, blk, 0, st>>>(a, out, work);
+    KCIG_CUDA(cudaGetLastError());
+    if (!a.angle) return KCIG_OK;
+    if (!a.use_grad) {
+        k_leg_fd<<<grd, blk, 0, st>>>(a, out, work);
+        KCIG_CUDA(cudaGetLastError());
+    }
+    if (a.smooth > 0) {
+        // smooth_grad_component (:486-492): two separable passes z then x;
+        // planes {0,1} hold (gx,gz), {2,3} are the scratch pair.
+        const dim3 g3((nzx + 255) / 256, a.n, 2);
+        for (int pass = 0; pass < 2; pass++) {
+            k_box<<<g3, blk, 0, st>>>(a.nz, a.nx, a.smooth, 0, 0, 2, work);
+            k_box<<<g3, blk, 0, st>>>(a.nz, a.nx, a.smooth, 1, 2, 0, work);
+        }
+        KCIG_CUDA(cudaGetLastError());
+    }
+    k_leg_pack<<<grd, blk, 0, st>>>(a, out, work);
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
+// ============================================================ K3 summation ==
+// kirchmig2d_cig.cpp:226-238 (cosine ramp helpers) in the FP32 of the
+// reference: weights only scale a pick, so FP32 rounding is harmless here.
+__device__ __forceinline__ float taper_weight(float ang, float start, float end)
+{
+    if (start < 0.0f || end <= start) return 1.0f;
+    if (ang <= start) return 1.0f;
+    if (ang >= end) return 0.0f;
+    const float x = (ang - start) / (end - start);
+    return 0.5f * (1.0f + cosf(3.14159265358979f * x));
+}
+
+__device__ __forceinline__ float depth_weight(float ang, float cutoff, float band)
+{
+    if (band <= 0.0f) return (ang <= cutoff) ? 1.0f : 0.0f;
+    if (ang <= cutoff) return 1.0f;
+    if (ang >= cutoff + band) return 0.0f;
+    const float u = (ang - cutoff) / band;
+    return 0.5f * (1.0f + cosf(3.14159265358979f * u));
+}
+
+// kirmig_pick (kirmig.cpp:34-58), adj branch.  The time-to-sample mapping and
+// the six-term sum run in FP64: with long traces and multi-second times the
+// FP32 fractional sample position alone costs more than the 1e-5 image error
+// budget.  Returns false when the reference would return without picking.
+__device__ __forceinline__ bool pick(const double2 *__restrict__ Dk, double ti, float deltat,
+                                     const SumArgs &a, float *out)
+{
+    // every test is written so that a NaN time (a NaN table entry) fails it,
+    // as the reference's integer conversion of a NaN does (kirmig.cpp:41-49)
+    const double ft0 = (ti - a.t0) * a.inv_dt;
+    const double fl = floor(ft0);
+    if (!(fl >= 0.0 && fl < (double)(a.nt - 1))) return false;
+    const double dl = (double)deltat;
+    const double tm = ti - dl - a.dt;
+    const double ftm0 = (tm - a.t0) * a.inv_dt;
+    const double flm = floor(ftm0);
+    if (!(flm >= 0.0 && flm <= fl)) return false;
+    const double tp = ti + dl + a.dt;
+    const double ftp0 = (tp - a.t0) * a.inv_dt;
+    const double flp = floor(ftp0);
+    if (!(flp >= fl && flp < (double)(a.nt - 1))) return false;
+    const double2 q0 = __ldg(Dk + (int)fl);
+    const double2 qm = __ldg(Dk + (int)flm);
+    const double2 qp = __ldg(Dk + (int)flp);
+    const double ft = ft0 - fl, ftm = ftm0 - flm, ftp = ftp0 - flp;
+    const float den = a.dtf + (float)(tp - tm);
+    float imp = a.dtf / den;
+    imp *= imp;
+    const double s = 2.0 * fma(ft, q0.y - q0.x, q0.x) - fma(ftm, qm.y - qm.x, qm.x) -
+                     fma(ftp, qp.y - qp.x, qp.x);
+    *out = (float)((double)imp * s);
+    return true;
+}
+
+// One CTA owns a TZ x TX image tile (one thread per image point) and keeps
+// its [bins][points] FP32 accumulators in shared memory: each thread only
+// touches its own column, so there are no atomics and no block barriers.
+// Shots are taken KB at a time with their leg fields in registers; each
+// receiver's leg fields are loaded once per shot block when receivers are
+// shared by all shots (cmp=0).  Per pair (kirchmig2d_cig.cpp:1206-1339):
+// aperture gate, FP64 traveltime sum, opening angle as the folded difference
+// of the two legs' gradient directions (exact in FP64, no per-pair arc
+// tangent), angle tapers, linear angle bins, the antialiased pick.
+template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
+__global__ void __launch_bounds__(TZ *TX) k_sum(const __grid_constant__ SumArgs a)
+{
+    constexpr int P = TZ * TX;
+    constexpr double kTwoPi = 6.283185307179586476925;
+    extern __shared__ float acc[];  // [nbins][P]
+    const int tid = threadIdx.x;
+    const int tiles_z = (a.nz + TZ - 1) / TZ;
+    const int tz = blockIdx.x % tiles_z, tx = blockIdx.x / tiles_z;
+    const int iz = tz * TZ + (tid % TZ), ix = tx * TX + (tid / TZ);
+    const bool valid = (iz < a.nz) && (ix < a.nx);
+    const int nzx = a.nz * a.nx;
+    const int i = valid ? ix * a.nz + iz : 0;
+    const int gc0 = a.gchunk0, nb = a.gchunk1 - a.gchunk0;
+
+    for (int b = 0; b < nb; b++)
+        acc[b * P + tid] = (a.zero_init || !valid) ? 0.0f : a.image[(size_t)(gc0 + b) * nzx + i];
+    if (!valid) return;  // no block-wide synchronisation follows
+
+    // cutoff of angle_depth_mute_weight (:200-211) depends only on depth
+    const float zf = (a.nz > 1) ? (float)iz / (float)(a.nz - 1) : 0.0f;
+    const float cutoff = a.oazmin + zf * (a.oazmax - a.oazmin);
+    const double ulo = -1.0e-5, uhi = (double)(a.ng - 1) + 1.0e-5;
+
+    for (int sb = 0; sb < a.nsb; sb += KB) {
+        double2 sTP[KB];
+        float2 sXW[KB];
+#pragma unroll
+        for (int k = 0; k < KB; k++) {
+            if (sb + k < a.nsb) {
+                sTP[k] = __ldg(a.STP + (size_t)(sb + k) * nzx + i);
+                sXW[k] = __ldg(a.SXW + (size_t)(sb + k) * nzx + i);
+            } else {
+                sTP[k] = make_double2(0.0, 0.0);
+                sXW[k] = make_float2(0.f, 0.f);
+            }
+        }
+        for (int r = 0; r < a.nh; r++) {
+            double2 rTP = make_double2(0.0, 0.0);
+            float2 rXW = make_float2(0.f, 0.f);
+            if (SHARED_R) {
+                rTP = __ldg(a.RTP + (size_t)r * nzx + i);
+                rXW = __ldg(a.RXW + (size_t)r * nzx + i);
+            }
+#pragma unroll
+            for (int k = 0; k < KB; k++) {
+                if (sb + k >= a.nsb) break;
+                const int trc = (sb + k) * a.nh + r;
+                const float tw = __ldg(a.trw + trc);
+                if (tw == 0.0f) continue;  // trace removed by aperture_trace / offset bin
+                if (!SHARED_R) {
+                    const int ri = __ldg(a.rfi + trc);
+                    rTP = __ldg(a.RTP + (size_t)ri * nzx + i);
+                    rXW = __ldg(a.RXW + (size_t)ri * nzx + i);
+                }
+                const float apw = sXW[k].y * rXW.y;
+                if (!(apw > 0.0f)) continue;
+                const double ti = sTP[k].x + rTP.x + a.tau;
+                const float txw = fmaxf(fabsf(sXW[k].x), fabsf(rXW.x));
+                const double2 *Dk = a.D + (size_t)trc * a.nt;
+                if (MODE == 2) {
+                    float picked;
+                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
+                    const int ig = __ldg(a.igo + trc) - gc0;
+                    if (ig < 0 || ig >= nb) continue;
+                    acc[ig * P + tid] += tw * apw * picked;
+                    continue;
+                }
+                // opening angle (:171-187): atan2(|s x r|, s.r) is the
+                // difference of the gradient directions folded to [0, pi]
+                double th = fabs(sTP[k].y - rTP.y);
+                if (th > 3.141592653589793238463) th = kTwoPi - th;
+                if (!(th == th)) continue;  // a vanishing gradient: angle NaN, weight 0
+                const double angd = th * a.deg;
+                const float ang = (float)angd;
+                const float aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw * apw;
+                if (!(aw > 0.0f)) continue;
+                const double u = (angd - a.ug0) * a.uinv;
+                if (MODE == 0) {
+                    // value_to_linear_bins (:54-79)
+                    if (!(u >= ulo && u <= uhi)) continue;
+                    int ig0, ig1;
+                    float w0, w1;
+                    if (u <= 0.0) { ig0 = ig1 = 0; w0 = 1.0f; w1 = 0.0f; }
+                    else if (u >= (double)(a.ng - 1)) { ig0 = ig1 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
+                    else {
+                        const double fl = floor(u);
+                        ig0 = (int)fl;
+                        ig1 = ig0 + 1;
+                        const double f1 = u - fl;
+                        w1 = (float)f1;
+                        w0 = (float)(1.0 - f1);
+                    }
+                    float picked;
+                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
+                    picked *= aw;
+                    ig0 -= gc0;
+                    ig1 -= gc0;
+                    if (ig0 >= 0 && ig0 < nb) acc[ig0 * P + tid] += w0 * picked;
+                    if (ig1 != ig0 && w1 > 0.0f && ig1 >= 0 && ig1 < nb) acc[ig1 * P + tid] += w1 * picked;
+                } else {
+                    // value_to_nearest_bin (:35-41)
+                    const double fn = floor(u + 0.5);
+                    if (!(fn >= 0.0 && fn < (double)a.ng)) continue;
+                    float picked;
+                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
+                    const int il = (int)fn - gc0;
+                    if (il >= 0 && il < nb) acc[il * P + tid] += aw * picked;
+                }
+            }
+        }
+    }
+    for (int b = 0; b < nb; b++) a.image[(size_t)(gc0 + b) * nzx + i] = acc[b * P + tid];
+}
+
+template <int TZ, int TX, int KB, bool SR, int MODE>
+static int launch_sum_t(const SumArgs &a, int nb, cudaStream_t st)
+{
+    constexpr int P = TZ * TX;
+    const size_t sm = (size_t)nb * P * sizeof(float);
+    auto kern = k_sum<TZ, TX, KB, SR, MODE>;
+    KCIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int tiles = ((a.nz + TZ - 1) / TZ) * ((a.nx + TX - 1) / TX);
+    kern<<<tiles, P, sm, st>>>(a);
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
+template <int TZ, int TX, int KB>
+static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
+{
+    if (a.shared_r) {
+        if (a.mode == 0) return launch_sum_t<TZ, TX, KB, true, 0>(a, nb, st);
+        if (a.mode == 1) return launch_sum_t<TZ, TX, KB, true, 1>(a, nb, st);
+        return launch_sum_t<TZ, TX, KB, true, 2>(a, nb, st);
+    }
+    if (a.mode == 0) return launch_sum_t<TZ, TX, 1, false, 0>(a, nb, st);
+    if (a.mode == 1) return launch_sum_t<TZ, TX, 1, false, 1>(a, nb, st);
+    return launch_sum_t<TZ, TX, 1, false, 2>(a, nb, st);
+}
+
+// Shared memory holds [bins][points] FP32 accumulators: 256-point tiles while
+// the bins fit in 100 KB (two CTAs per SM), smaller tiles above, and bin
+// chunks of at most 384 bins beyond that.
+int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
+{
+    const int maxb = 384;
+    for (int g = 0; g < a0.ng; g += maxb) {
+        SumArgs a = a0;
+        a.gchunk0 = g;
+        a.gchunk1 = min(a0.ng, g + maxb);
+        const int nb = a.gchunk1 - a.gchunk0;
+        int rc;
+        if ((size_t)nb * 256 * 4 <= 100 * 1024) rc = launch_sum_mode<16, 16, 4>(a, nb, st);
+        else if ((size_t)nb * 128 * 4 <= 200 * 1024) rc = launch_sum_mode<16, 8, 4>(a, nb, st);
+        else rc = launch_sum_mode<8, 8, 4>(a, nb, st);
+        if (rc) return rc;
+        if (launches) (*launches)++;
+    }
+    return KCIG_OK;
+}
+
+}  // namespace kcig

@@ -1,0 +1,627 @@
+// Migration plan: host orchestration of the shot/trace loop of
+// src/kirchmig2d_cig.cpp:979-1339 (adj=1) around the K1/K2/K3 kernels.
+//
+// The host resolves, once per trace and in double precision, everything the
+// reference computes per trace with scalar code: source/receiver positions,
+// the table slices and interpolation weights (:987-1029, :1148-1180), the
+// trace-index aperture (:1082-1099) and the offset bin (:1100-1105).  The GPU
+// does all per-sample and per-image-point work.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "kcig_common.h"
+
+using namespace kcig;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes)
+    {
+        if (bytes <= n && p) return KCIG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (bytes == 0) return KCIG_OK;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return cuda_error(e, "cudaMalloc(scratch)");
+        }
+        n = bytes;
+        return KCIG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+struct kcig_plan {
+    kcig_params p;
+    kcig_geometry g;
+    int ng = 1;
+    float g0 = 0.f, dg = 1.f;
+    int device = 0;
+    cudaStream_t st = 0;
+    unsigned long long budget = 0;
+    const float *stab = nullptr, *sder = nullptr, *rtab = nullptr, *rder = nullptr;
+    const float *sgx = nullptr, *sgz = nullptr, *rgx = nullptr, *rgz = nullptr;
+    DevBuf own_stab, own_sder, own_rtab, own_rder, own_sgx, own_sgz, own_rgx, own_rgz;
+    DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
+    int sum_launches = 0, all_launches = 0;
+    float sum_ms = 0.f;
+};
+
+namespace {
+
+int upload(DevBuf &b, const void *src, size_t bytes, cudaStream_t st)
+{
+    KCIG_TRY(b.ensure(bytes));
+    KCIG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st));
+    return KCIG_OK;
+}
+
+// Slice choice and weights of one leg.  Which slice a position falls in is a
+// discrete decision that, for a position on a table node, depends on the
+// rounding of the reference's FP32 expression (pos - o)/d; it is therefore
+// taken in that same FP32 arithmetic (posf is the position as the reference
+// computes it in float).  The in-interval coordinate and all weights are FP64
+// (from pos).  Returns the slice index the reference assigns to ist
+// (:987-1016) or uses for the receiver (:1148-1180).
+int leg_interp(const kcig_plan *P, int is_source, float posf, double pos, LegInterp *L)
+{
+    const kcig_geometry &g = P->g;
+    const int n = is_source ? g.sny : g.rny;
+    const float of = is_source ? g.sy0 : g.ry0;
+    const float df = is_source ? g.sdy : g.rdy;
+    const double o = of, d = df;
+    memset(L, 0, sizeof *L);
+    L->type = P->p.interp_type;
+    L->pos = pos;
+    L->i1 = -1;
+    float f = 0.0f;
+    bool left;
+    if (is_source) {
+        left = (n <= 1 || df == 0.0f);
+        if (!left) f = (posf - of) / df;
+        if (!left && f <= 0.0f) left = true;
+    } else {
+        if (n > 1 && df != 0.0f) f = (posf - of) / df;
+        left = (n <= 1 || df == 0.0f || f <= 0.0f);
+    }
+    int ret;
+    if (left) {
+        L->i0 = 0;
+        ret = 0;
+    } else if (f >= (float)(n - 1)) {
+        L->i0 = n - 1;
+        ret = n - 1;
+    } else {
+        const int i0 = (int)floorf(f);
+        const double x = pos - (o + (double)i0 * d);
+        const double t = x / d;
+        L->i0 = i0;
+        L->i1 = i0 + 1;
+        L->t = t;
+        L->dxp = d;
+        ret = i0;
+        if (L->type == 'l') {
+            // tinterp_linear / dinterp_linear (tinterpsr.cpp:37-70)
+            L->c[0] = 1.0 - t; L->c[2] = t;
+            L->e[0] = -1.0 / d; L->e[2] = 1.0 / d;
+        } else if (L->type == 'p') {
+            L->k1 = (int)(x / (double)g.dx + 0.5);
+            L->k2 = (int)((d - x) / (double)g.dx + 0.5);
+        } else {
+            // tinterp_hermite / dinterp_hermite (tinterpsr.cpp:142-188)
+            const double h00 = 2. * t * t * t - 3. * t * t + 1.;
+            const double h10 = t * t * t - 2. * t * t + t;
+            const double h01 = -2. * t * t * t + 3. * t * t;
+            const double h11 = t * t * t - t * t;
+            const double g00 = -6. * t * (1. - t);
+            const double g10 = (1. - t) * (1. - 3. * t);
+            const double g01 = 6. * t * (1. - t);
+            const double g11 = 3. * t * t - 2. * t;
+            L->c[0] = h00; L->c[1] = h10 * d; L->c[2] = h01; L->c[3] = h11 * d;
+            L->e[0] = g00 / d; L->e[1] = g10; L->e[2] = g01 / d; L->e[3] = g11;
+        }
+    }
+    // interp_volume_linear_stream (:294-322) for the optional gradient files
+    L->gi0 = 0;
+    L->gi1 = 0;
+    L->gw = 0.0;
+    if (n > 1 && df != 0.0f) {
+        const float fg = (posf - of) / df;
+        if (fg <= 0.0f) L->gi0 = 0;
+        else if (fg >= (float)(n - 1)) L->gi0 = n - 1;
+        else {
+            L->gi0 = (int)floorf(fg);
+            L->gi1 = L->gi0 + 1;
+            L->gw = (pos - o) / d - (double)L->gi0;
+        }
+    }
+    return ret;
+}
+
+int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &legs, double2 *TP, float2 *XW)
+{
+    const kcig_geometry &g = P->g;
+    const size_t nzx = (size_t)g.nz * g.nx;
+    const int angle = P->p.cig && P->p.cig_is_angle;
+    const int FB = std::max(1, std::min<int>((int)legs.size(), (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
+    if (angle) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
+    KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
+    if (!legs.empty())
+        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
+                                  P->st));
+    for (size_t j0 = 0; j0 < legs.size(); j0 += FB) {
+        FieldArgs a;
+        a.tab = is_source ? P->stab : P->rtab;
+        a.der = is_source ? P->sder : P->rder;
+        a.gxv = is_source ? P->sgx : P->rgx;
+        a.gzv = is_source ? P->sgz : P->rgz;
+        a.legs = P->d_legs.as<LegInterp>() + j0;
+        a.n = (int)std::min<size_t>(FB, legs.size() - j0);
+        a.nz = g.nz;
+        a.nx = g.nx;
+        a.dz = g.dz;
+        a.dx = g.dx;
+        a.x0 = g.x0;
+        a.radius = P->p.angle_grad_radius;
+        a.smooth = P->p.angle_smooth;
+        a.angle = angle;
+        a.use_grad = P->sgx != nullptr;
+        a.aper = P->p.aperture;
+        a.aper_taper = P->p.aperture_taper;
+        a.rmin = P->p.aperture_rmin;
+        a.rtaper = P->p.aperture_rtaper;
+        LegFields out{TP + j0 * nzx, XW + j0 * nzx};
+        KCIG_TRY(launch_leg_fields(a, out, P->d_work.as<double>(), P->st));
+        P->all_launches += 1 + (angle ? (a.use_grad ? 0 : 1) + (a.smooth > 0 ? 4 : 0) + 1 : 0);
+    }
+    return KCIG_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI --
+extern "C" int kcig_plan_create(const kcig_params *p, const kcig_geometry *g, unsigned long long scratch_bytes,
+                                kcig_plan **out)
+{
+    if (!p || !g || !out) return set_error(KCIG_ERR_ARG, "kcig_plan_create: null argument");
+    *out = nullptr;
+    if (!p->adj) return set_error(KCIG_ERR_UNSUPPORTED, "adj=0 (forward modelling) is not built; only adj=1 is.");
+    if (g->nt < 1 || g->nh < 1 || g->ns < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for seismic_data= (t,h/r,s)");
+    if (g->nz < 1 || g->nx < 1 || g->sny < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for stable= (z,x,s)");
+    if (g->rny < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for rtable= (z,x,r)");
+    if (!(g->dt > 0.0f)) return set_error(KCIG_ERR_ARG, "time sampling d1 of seismic_data= must be positive");
+    if ((long long)g->nz * g->nx > 0x7fffffffLL) return set_error(KCIG_ERR_ARG, "image grid too large");
+    if (p->direct_mute && p->direct_mute_qc_shot >= g->ns)
+        return set_error(KCIG_ERR_ARG, "direct_mute_qc_shot=%d is outside the input shot range [0,%d].",
+                         p->direct_mute_qc_shot, g->ns - 1);
+    kcig_plan *P = new kcig_plan();
+    P->p = *p;
+    P->g = *g;
+    if (P->g.nh == 1) P->g.dh = 0.0f;  // :700-701
+    if (P->g.ns == 1) P->g.ds = 0.0f;
+    int rc = kcig_output_axis(p, &P->g, &P->ng, &P->g0, &P->dg);
+    if (rc) {
+        delete P;
+        return rc;
+    }
+    cudaGetDevice(&P->device);
+    P->budget = scratch_bytes;
+    if (P->budget == 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            delete P;
+            return set_error(KCIG_ERR_CUDA, "no CUDA device available");
+        }
+        P->budget = (unsigned long long)(fr > (6ull << 30) ? (fr - (4ull << 30)) * 0.8 : fr / 2);
+        P->budget = std::min<unsigned long long>(P->budget, 96ull << 30);
+    }
+    *out = P;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_destroy(kcig_plan *P)
+{
+    if (!P) return KCIG_OK;
+    DevBuf *bufs[] = {&P->own_stab, &P->own_sder, &P->own_rtab, &P->own_rder, &P->own_sgx, &P->own_sgz,
+                      &P->own_rgx,  &P->own_rgz,  &P->d_data,   &P->d_image,  &P->d_rT,   &P->d_rF,
+                      &P->d_sT,     &P->d_sF,   &P->d_work,   &P->d_D,      &P->d_legs, &P->d_tr};
+    for (DevBuf *b : bufs) b->release();
+    delete P;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_set_stream(kcig_plan *P, void *stream)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "null plan");
+    P->st = (cudaStream_t)stream;
+    return KCIG_OK;
+}
+
+static int bind_volume(kcig_plan *P, DevBuf &own, const float *src, int npos, int memory, const float **dst,
+                       const float *alias_src, const float *alias_dev)
+{
+    const size_t bytes = (size_t)npos * P->g.nz * P->g.nx * sizeof(float);
+    if (!src) return set_error(KCIG_ERR_ARG, "missing table pointer");
+    if (memory == KCIG_MEM_DEVICE) {
+        *dst = src;
+        return KCIG_OK;
+    }
+    if (alias_src == src && alias_dev) {
+        *dst = alias_dev;
+        return KCIG_OK;
+    }
+    KCIG_TRY(upload(own, src, bytes, P->st));
+    *dst = own.as<float>();
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_set_tables(kcig_plan *P, const float *stable, const float *sderiv, const float *rtable,
+                                    const float *rderiv, int memory)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "null plan");
+    KCIG_TRY(bind_volume(P, P->own_stab, stable, P->g.sny, memory, &P->stab, nullptr, nullptr));
+    KCIG_TRY(bind_volume(P, P->own_sder, sderiv, P->g.sny, memory, &P->sder, nullptr, nullptr));
+    const bool same = (P->g.rny == P->g.sny);
+    KCIG_TRY(bind_volume(P, P->own_rtab, rtable, P->g.rny, memory, &P->rtab, same ? stable : nullptr, P->stab));
+    KCIG_TRY(bind_volume(P, P->own_rder, rderiv, P->g.rny, memory, &P->rder, same ? sderiv : nullptr, P->sder));
+    KCIG_CUDA(cudaStreamSynchronize(P->st));
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_set_gradients(kcig_plan *P, const float *sgradx, const float *sgradz, const float *rgradx,
+                                       const float *rgradz, int memory)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "null plan");
+    const int n = (sgradx != nullptr) + (sgradz != nullptr) + (rgradx != nullptr) + (rgradz != nullptr);
+    if (n == 0) {
+        P->sgx = P->sgz = P->rgx = P->rgz = nullptr;
+        return KCIG_OK;
+    }
+    if (n != 4)
+        return set_error(KCIG_ERR_ARG,
+                         "For mode=angle, please provide all of sgradx=, sgradz=, rgradx=, and rgradz=, or provide none of them.");
+    KCIG_TRY(bind_volume(P, P->own_sgx, sgradx, P->g.sny, memory, &P->sgx, nullptr, nullptr));
+    KCIG_TRY(bind_volume(P, P->own_sgz, sgradz, P->g.sny, memory, &P->sgz, nullptr, nullptr));
+    const bool same = (P->g.rny == P->g.sny);
+    KCIG_TRY(bind_volume(P, P->own_rgx, rgradx, P->g.rny, memory, &P->rgx, same ? sgradx : nullptr, P->sgx));
+    KCIG_TRY(bind_volume(P, P->own_rgz, rgradz, P->g.rny, memory, &P->rgz, same ? sgradz : nullptr, P->sgz));
+    KCIG_CUDA(cudaStreamSynchronize(P->st));
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_last_stats(const kcig_plan *P, int *sum_launches, float *sum_ms, int *all_launches)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "null plan");
+    if (sum_launches) *sum_launches = P->sum_launches;
+    if (sum_ms) *sum_ms = P->sum_ms;
+    if (all_launches) *all_launches = P->all_launches;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_leg_fields_device(kcig_plan *P, int is_source, double pos, double *T, float *Tx, double *phi,
+                                      float *w)
+{
+    if (!P || !P->stab) return set_error(KCIG_ERR_ARG, "kcig_leg_fields_device: plan without tables");
+    const size_t nzx = (size_t)P->g.nz * P->g.nx;
+    std::vector<LegInterp> legs(1);
+    leg_interp(P, is_source, (float)pos, pos, &legs[0]);
+    legs[0].scale = 1.0f;
+    DevBuf tp, xw;
+    int rc = tp.ensure(nzx * sizeof(double2));
+    if (!rc) rc = xw.ensure(nzx * sizeof(float2));
+    if (!rc) rc = compute_fields(P, is_source, legs, tp.as<double2>(), xw.as<float2>());
+    // unpack {T, phi} and {Tx, w} into the caller's planes
+    struct Cp { void *dst; const char *src; size_t el, pitch; } cps[4] = {
+        {T, tp.as<char>(), sizeof(double), sizeof(double2)},
+        {phi, tp.as<char>() + sizeof(double), sizeof(double), sizeof(double2)},
+        {Tx, xw.as<char>(), sizeof(float), sizeof(float2)},
+        {w, xw.as<char>() + sizeof(float), sizeof(float), sizeof(float2)}};
+    for (int q = 0; q < 4 && rc == KCIG_OK; q++) {
+        if (!cps[q].dst) continue;
+        cudaError_t e = cudaMemcpy2DAsync(cps[q].dst, cps[q].el, cps[q].src, cps[q].pitch, cps[q].el, nzx,
+                                          cudaMemcpyDeviceToDevice, P->st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpy2DAsync(leg fields)");
+    }
+    cudaError_t e = cudaStreamSynchronize(P->st);
+    if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(leg fields)");
+    tp.release();
+    xw.release();
+    return rc;
+}
+
+extern "C" int kcig_doubint_device(const float *in, double *out, int ntr, int nt, int isdiff, float dt, void *stream)
+{
+    if (!in || !out || ntr < 0 || nt < 1) return set_error(KCIG_ERR_ARG, "kcig_doubint_device: bad arguments");
+    return launch_doubint_plain(in, out, ntr, nt, isdiff, (double)dt, (cudaStream_t)stream);
+}
+
+extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int memory)
+{
+    if (!P || !data || !image) return set_error(KCIG_ERR_ARG, "kcig_migrate: null argument");
+    if (!P->stab) return set_error(KCIG_ERR_ARG, "kcig_migrate: tables not set");
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    const size_t nzx = (size_t)g.nz * g.nx;
+    const int angle = p.cig && p.cig_is_angle;
+    P->sum_launches = 0;
+    P->all_launches = 0;
+    P->sum_ms = 0.f;
+    cudaStream_t st = P->st;
+
+    // data and image on the device
+    const float *d_data = data;
+    float *d_img = image;
+    const size_t data_bytes = (size_t)g.ns * g.nh * g.nt * sizeof(float);
+    if (memory == KCIG_MEM_HOST) {
+        KCIG_TRY(upload(P->d_data, data, data_bytes, st));
+        d_data = P->d_data.as<float>();
+        KCIG_TRY(P->d_image.ensure((size_t)P->ng * nzx * sizeof(float)));
+        d_img = P->d_image.as<float>();
+    }
+
+    // per-trace scalars (:1054-1105), all in double
+    const double ds = g.ns == 1 ? 0.0 : (double)g.ds, dh = g.nh == 1 ? 0.0 : (double)g.dh;
+    // positions in FP64 for every continuous use, and as the reference's
+    // float expressions (:980, :1055, :1061) for its discrete decisions
+    std::vector<double> sx(g.ns), hx(g.nh);
+    std::vector<float> sxf(g.ns), hxf(g.nh);
+    for (int is = 0; is < g.ns; is++) {
+        sx[is] = (double)g.s0 + (double)is * ds;
+        sxf[is] = g.s0 + (float)is * (float)ds;
+    }
+    for (int ih = 0; ih < g.nh; ih++) {
+        hx[ih] = (double)g.h0 + (double)ih * dh;
+        hxf[ih] = g.h0 + (float)ih * (float)dh;
+    }
+    std::vector<LegInterp> slegs(g.ns);
+    std::vector<int> ist(g.ns);
+    for (int is = 0; is < g.ns; is++) {
+        ist[is] = leg_interp(P, 1, sxf[is], sx[is], &slegs[is]);
+        slegs[is].scale = (float)ds;
+    }
+    const size_t ntr_all = (size_t)g.ns * g.nh;
+    std::vector<float> trw(ntr_all);
+    std::vector<int> igo(ntr_all, 0);
+    std::vector<double> msx(ntr_all), mrx(ntr_all);
+    for (int is = 0; is < g.ns; is++)
+        for (int ih = 0; ih < g.nh; ih++) {
+            const size_t t = (size_t)is * g.nh + ih;
+            const double rpos = p.cmp ? sx[is] + hx[ih] : hx[ih];
+            const float rposf = p.cmp ? sxf[is] + hxf[ih] : hxf[ih];
+            msx[t] = sx[is];
+            mrx[t] = rpos;
+            float rf = 0.0f;
+            if (g.rny > 1 && g.rdy != 0.0f) rf = (rposf - g.ry0) / g.rdy;
+            const int iht = (g.rny > 1 && g.rdy != 0.0f) ? (int)floorf(rf) : 0;
+            double w = 1.0;
+            if (p.aperture_trace != -1) {
+                const double ad = fabs((double)(iht - ist[is]));
+                if (ad >= (double)p.aperture_trace) w = 0.0;
+                else if (p.aperture_trace_taper > 0) {
+                    const double tb = std::max(0.0, (double)(p.aperture_trace - p.aperture_trace_taper));
+                    if (ad > tb) {
+                        const double den = (double)p.aperture_trace - tb;
+                        if (den > 0.0) w = 0.5 * (1.0 + cos(M_PI * ((ad - tb) / den)));
+                    }
+                }
+            }
+            if (p.cig && !p.cig_is_angle) {
+                // value_to_nearest_bin(h) (:35-41), a discrete decision in float
+                int ig = -1;
+                if (P->ng > 0 && P->dg > 0.0f && isfinite(hxf[ih])) {
+                    ig = (int)floorf((hxf[ih] - P->g0) / P->dg + 0.5f);
+                    if (ig < 0 || ig >= P->ng) ig = -1;
+                }
+                if (ig < 0) w = 0.0;
+                igo[t] = ig < 0 ? 0 : ig;
+            }
+            trw[t] = (float)w;
+        }
+
+    // scratch plan: receivers shared across shots (cmp=0) are computed once
+    const bool shared_r = !p.cmp;
+    const size_t leg_bytes = nzx * (sizeof(double2) + sizeof(float2));
+    const unsigned long long budget = P->budget;
+    int nhc = g.nh;
+    if (shared_r && (unsigned long long)nhc * leg_bytes > budget / 2)
+        nhc = (int)std::max<unsigned long long>(1, (budget / 2) / leg_bytes);
+    const size_t work_bytes = angle ? (size_t)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1) * 4 * nzx * 8 : 0;
+    const size_t per_shot = leg_bytes + (size_t)nhc * g.nt * sizeof(double2) + (size_t)nhc * 32 +
+                            (shared_r ? 0 : (size_t)nhc * leg_bytes);
+    const unsigned long long fixed = (shared_r ? (unsigned long long)nhc * leg_bytes : 0) + work_bytes;
+    long long room = (long long)budget - (long long)fixed;
+    int nsb = (int)std::max<long long>(1, room / (long long)per_shot);
+    nsb = std::min(nsb, g.ns);
+
+    if (shared_r) {
+        KCIG_TRY(P->d_rT.ensure((size_t)nhc * nzx * sizeof(double2)));
+        KCIG_TRY(P->d_rF.ensure((size_t)nhc * nzx * sizeof(float2)));
+    } else {
+        KCIG_TRY(P->d_rT.ensure((size_t)nsb * g.nh * nzx * sizeof(double2)));
+        KCIG_TRY(P->d_rF.ensure((size_t)nsb * g.nh * nzx * sizeof(float2)));
+    }
+    KCIG_TRY(P->d_sT.ensure((size_t)nsb * nzx * sizeof(double2)));
+    KCIG_TRY(P->d_sF.ensure((size_t)nsb * nzx * sizeof(float2)));
+    KCIG_TRY(P->d_D.ensure((size_t)nsb * nhc * g.nt * sizeof(double2)));
+    const size_t trn = (size_t)nsb * nhc;
+    // one allocation: doubles first (8-byte aligned), then floats and ints
+    KCIG_TRY(P->d_tr.ensure(trn * (2 * sizeof(double) + sizeof(float) + 2 * sizeof(int))));
+    double *d_msx = P->d_tr.as<double>();
+    double *d_mrx = d_msx + trn;
+    float *d_trw = (float *)(d_mrx + trn);
+    int *d_rfi = (int *)(d_trw + trn);
+    int *d_igo = d_rfi + trn;
+
+    std::vector<cudaEvent_t> evs;
+    bool first = true;
+    std::vector<float> h_trw(trn);
+    std::vector<int> h_rfi(trn), h_igo(trn);
+    std::vector<double> h_msx(trn), h_mrx(trn);
+    int rc = KCIG_OK;
+
+    for (int r0 = 0; r0 < g.nh && rc == KCIG_OK; r0 += nhc) {
+        const int nhb = std::min(nhc, g.nh - r0);
+        if (shared_r) {
+            std::vector<LegInterp> rl(nhb);
+            for (int r = 0; r < nhb; r++) {
+                leg_interp(P, 0, hxf[r0 + r], hx[r0 + r], &rl[r]);
+                rl[r].scale = (float)dh;
+            }
+            rc = compute_fields(P, 0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+            if (rc) break;
+        }
+        for (int s0 = 0; s0 < g.ns && rc == KCIG_OK; s0 += nsb) {
+            const int nsh = std::min(nsb, g.ns - s0);
+            std::vector<LegInterp> sl(slegs.begin() + s0, slegs.begin() + s0 + nsh);
+            rc = compute_fields(P, 1, sl, P->d_sT.as<double2>(), P->d_sF.as<float2>());
+            if (rc) break;
+            // per-trace arrays of this (shot batch, receiver chunk)
+            std::vector<LegInterp> rl;
+            std::map<std::pair<double, float>, int> seen;  // (FP64, float) receiver position
+            for (int k = 0; k < nsh; k++)
+                for (int r = 0; r < nhb; r++) {
+                    const size_t t = (size_t)(s0 + k) * g.nh + (r0 + r);
+                    const size_t b = (size_t)k * nhb + r;
+                    h_trw[b] = trw[t];
+                    h_igo[b] = igo[t];
+                    h_msx[b] = msx[t];
+                    h_mrx[b] = mrx[t];
+                    if (shared_r) {
+                        h_rfi[b] = r;
+                    } else {
+                        const std::pair<double, float> key(mrx[t], sxf[s0 + k] + hxf[r0 + r]);
+                        auto it = seen.find(key);
+                        if (it == seen.end()) {
+                            LegInterp L;
+                            leg_interp(P, 0, key.second, key.first, &L);
+                            L.scale = (float)dh;
+                            it = seen.emplace(key, (int)rl.size()).first;
+                            rl.push_back(L);
+                        }
+                        h_rfi[b] = it->second;
+                    }
+                }
+            if (!shared_r) {
+                rc = compute_fields(P, 0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+                if (rc) break;
+            }
+            const size_t nb = (size_t)nsh * nhb;
+            {
+                const void *srcs[5] = {h_trw.data(), h_rfi.data(), h_igo.data(), h_msx.data(), h_mrx.data()};
+                void *dsts[5] = {d_trw, d_rfi, d_igo, d_msx, d_mrx};
+                const size_t sz[5] = {sizeof(float), sizeof(int), sizeof(int), sizeof(double), sizeof(double)};
+                for (int q = 0; q < 5 && rc == KCIG_OK; q++) {
+                    cudaError_t e = cudaMemcpyAsync(dsts[q], srcs[q], nb * sz[q], cudaMemcpyHostToDevice, st);
+                    if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(trace tables)");
+                }
+                if (rc) break;
+            }
+            PreludeArgs pa;
+            pa.data = d_data;
+            pa.D = P->d_D.as<double2>();
+            pa.mute_sx = p.direct_mute ? d_msx : nullptr;
+            pa.mute_rx = d_mrx;
+            pa.ntr = (int)nb;
+            pa.nt = g.nt;
+            pa.isdiff = p.isdiff;
+            pa.invert = p.direct_mute_invert;
+            pa.nh = g.nh;
+            pa.nhc = nhb;
+            pa.shot0 = s0;
+            pa.rcv0 = r0;
+            pa.t0 = g.t0;
+            pa.dt = g.dt;
+            pa.slope = p.direct_mute_slope;
+            pa.intercept = p.direct_mute_intercept;
+            pa.taper = p.direct_mute_taper;
+            rc = launch_prelude(pa, st);
+            if (rc) break;
+            P->all_launches++;
+
+            SumArgs sa;
+            memset(&sa, 0, sizeof sa);
+            sa.STP = P->d_sT.as<double2>();
+            sa.SXW = P->d_sF.as<float2>();
+            sa.RTP = P->d_rT.as<double2>();
+            sa.RXW = P->d_rF.as<float2>();
+            sa.D = P->d_D.as<double2>();
+            sa.trw = d_trw;
+            sa.rfi = d_rfi;
+            sa.igo = d_igo;
+            sa.image = d_img;
+            sa.zero_init = first ? 1 : 0;
+            sa.nz = g.nz;
+            sa.nx = g.nx;
+            sa.nt = g.nt;
+            sa.nsb = nsh;
+            sa.nh = nhb;
+            sa.ng = P->ng;
+            sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
+            sa.shared_r = shared_r ? 1 : 0;
+            sa.half = p.half_angle;
+            sa.t0 = g.t0;
+            sa.dt = g.dt;
+            sa.inv_dt = 1.0 / (double)g.dt;
+            sa.tau = p.tau;
+            sa.deg = (p.half_angle ? 90.0 : 180.0) / M_PI;
+            sa.ug0 = P->g0;
+            sa.uinv = 1.0 / (double)P->dg;
+            sa.dtf = g.dt;
+            sa.aal = p.antialias;
+            sa.g0 = P->g0;
+            sa.dg = P->dg;
+            sa.oazmin = p.oazmin;
+            sa.oazmax = p.oazmax;
+            sa.oaztaper = p.oaztaper;
+            sa.ats = p.angle_taper_start;
+            sa.ate = p.angle_taper_end;
+            cudaEvent_t e0, e1;
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            evs.push_back(e0);
+            evs.push_back(e1);
+            cudaEventRecord(e0, st);
+            int nl = 0;
+            rc = launch_sum(sa, st, &nl);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            P->sum_launches += nl;
+            P->all_launches += nl;
+            first = false;
+            // the host-side arrays are reused by the next batch
+            if (s0 + nsb < g.ns || r0 + nhc < g.nh) {
+                cudaError_t e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) {
+                    rc = cuda_error(e, "cudaStreamSynchronize(batch)");
+                    break;
+                }
+            }
+        }
+    }
+    if (rc == KCIG_OK && memory == KCIG_MEM_HOST) {
+        cudaError_t e = cudaMemcpyAsync(image, d_img, (size_t)P->ng * nzx * sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(image)");
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == KCIG_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(migrate)");
+    for (size_t i = 0; i + 1 < evs.size(); i += 2) {
+        float ms = 0.f;
+        if (rc == KCIG_OK && cudaEventElapsedTime(&ms, evs[i], evs[i + 1]) == cudaSuccess) P->sum_ms += ms;
+        cudaEventDestroy(evs[i]);
+        cudaEventDestroy(evs[i + 1]);
+    }
+    return rc;
+}

@@ -1,0 +1,127 @@
+"""Generate the golden fixtures of the parity tests.
+
+Runs the UNMODIFIED reference tools built from their sources by
+``make -C oracle ref`` (oracle/_ref/{shotgen,eikods2d,kirchmig2d_cig}) on a
+small seeded workload and stores inputs and reference images in
+tests/golden/golden.npz, with the parameter tokens of each case in
+tests/golden/cases.json.  Needs the reference tree (only in the build
+container); the tests only read the committed outputs.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from kirch_datuming_b200 import rsf, synth  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+
+# small model: v(z) = 1.5 + 0.6 z on a 41 x 81 grid of 10 m, tables every 20 m
+NZ, NX, DZ = 41, 81, 0.01
+NPOS_EVERY = 2
+NT, DT = 301, 0.002
+
+COMMON = ["adj=1"]
+MUTE = ["direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05"]
+CASES = {
+    "base": dict(data="cmp0", tokens=["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60",
+                                      "angle_step=1", "angle_n=61"] + MUTE),
+    "cmp1_half": dict(data="cmp1", tokens=["cig=1", "mode=angle", "cmp=1", "half_angle=1", "angle_min=0",
+                                           "angle_max=45", "angle_step=1.5", "angle_n=31"] + MUTE),
+    "options": dict(data="cmp0", tokens=["cig=1", "mode=angle", "cmp=0", "angle_interp=0", "diff=1",
+                                         "type=linear", "tau=0.01", "antialias=0.5", "aperture=60",
+                                         "aperture_taper=5", "aperture_rmin=0.1", "aperture_rtaper=0.05",
+                                         "angle_taper_start=30", "angle_taper_end=50", "oazmin=70",
+                                         "oazmax=40", "oaztaper=5", "angle_min=0", "angle_max=60",
+                                         "angle_step=2", "angle_n=31"] + MUTE),
+    "trace_aperture": dict(data="cmp0", tokens=["cig=1", "mode=angle", "cmp=0", "aperture_trace=8",
+                                                "aperture_trace_taper=4", "type=partial",
+                                                "angle_grad_radius=1", "angle_smooth=0", "direct_mute=1",
+                                                "direct_mute_invert=1", "direct_mute_slope=0.3",
+                                                "direct_mute_intercept=0.3", "direct_mute_taper=0.04",
+                                                "angle_min=0", "angle_max=60", "angle_step=1",
+                                                "angle_n=61"]),
+    "offset": dict(data="cmp1", tokens=["cig=1", "mode=offset", "cmp=1"] + MUTE),
+    "stack": dict(data="cmp0", tokens=["cig=0", "cmp=0"] + MUTE),
+    "grads": dict(data="cmp0", grads=True, tokens=["cig=1", "mode=angle", "cmp=0", "angle_smooth=1",
+                                                   "angle_min=0", "angle_max=60", "angle_step=1",
+                                                   "angle_n=61"] + MUTE),
+    "default_axis": dict(data="cmp0", tokens=["cig=1", "mode=angle", "cmp=0", "oazmin=180", "oazmax=180"]),
+}
+
+DATA = {
+    # shots off the 20 m table grid, receivers on it (fixed spread)
+    "cmp0": dict(ns=5, s0=0.05, ds=0.17, nh=21, h0=0.2, dh=0.02, cmp=0),
+    # receivers move with the shot: r = s + h, split spread
+    "cmp1": dict(ns=4, s0=0.23, ds=0.11, nh=17, h0=-0.16, dh=0.02, cmp=1),
+}
+
+
+def run(cmd, cwd):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("%s failed:\n%s\n%s" % (cmd, r.stdout[-3000:], r.stderr[-3000:]))
+    return r.stdout + r.stderr
+
+
+def main():
+    out = {}
+    meta = {"nz": NZ, "nx": NX, "dz": DZ, "nt": NT, "dt": DT, "cases": {}, "data": {}}
+    with tempfile.TemporaryDirectory() as wd:
+        v = synth.velocity_linear_vz(NZ, NX, DZ)
+        rsf.write(f"{wd}/vel.rsf", v, [NZ, NX], [0, 0], [DZ, DZ])
+        npos = (NX - 1) // NPOS_EVERY + 1
+        run([f"{REF}/shotgen", "shotfile=sht.rsf", f"nshot={npos}", "oy=0", f"dy={DZ * NPOS_EVERY}"], wd)
+        run([f"{REF}/eikods2d", "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf",
+             "tds1=tds.rsf", "gradz=gz.rsf", "gradx=gx.rsf", "b1=2", "b2=2"], wd)
+        hT, T = rsf.read(f"{wd}/time.rsf")
+        _, D = rsf.read(f"{wd}/tds.rsf")
+        _, GX = rsf.read(f"{wd}/gx.rsf")
+        _, GZ = rsf.read(f"{wd}/gz.rsf")
+        meta["table"] = dict(n=hT.n[:3], o=hT.o[:3], d=hT.d[:3])
+        out["T"], out["tds"], out["gradx"], out["gradz"] = T, D, GX, GZ
+        tabs = torch.from_numpy(T.reshape(hT.n[2], NX, NZ))
+        refl_rows = [(np.full(NX, r), a) for r, a in zip((12, 22, 33), synth.reflectivities(3, 11))]
+        for name, d in DATA.items():
+            g = synth.Geometry(nz=NZ, nx=NX, dz=DZ, dx=DZ, z0=0, x0=0, nt=NT, dt=DT, t0=0, npos=hT.n[2],
+                               p0=hT.o[2], dp=hT.d[2], **d)
+            data = synth.shot_gathers(tabs, g, refl_rows, 20.0, seed=5).numpy()
+            out["data_" + name] = data
+            meta["data"][name] = d
+            rsf.write(f"{wd}/data_{name}.rsf", data, [NT, d["nh"], d["ns"]], [0, d["h0"], d["s0"]],
+                      [DT, d["dh"], d["ds"]], extra={"unit1": "s"})
+        for cname, c in CASES.items():
+            args = [f"seismic_data=data_{c['data']}.rsf", f"migration=mig_{cname}.rsf", "stable=time.rsf",
+                    "sderiv=tds.rsf", "rtable=time.rsf", "rderiv=tds.rsf"] + COMMON + c["tokens"]
+            if c.get("grads"):
+                args += ["sgradx=gx.rsf", "sgradz=gz.rsf", "rgradx=gx.rsf", "rgradz=gz.rsf"]
+            log = run([f"{REF}/kirchmig2d_cig"] + args, wd)
+            h, img = rsf.read(f"{wd}/mig_{cname}.rsf")
+            with open(f"{wd}/mig_{cname}.rsf") as f:
+                header = f.read()
+            out["img_" + cname] = img
+            meta["cases"][cname] = dict(data=c["data"], tokens=COMMON + c["tokens"], grads=bool(c.get("grads")),
+                                        n=h.n[:3], o=h.o[:3], d=h.d[:3], extra=h.extra,
+                                        sha256=hashlib.sha256(img.tobytes()).hexdigest(),
+                                        info=[l.split("INFO:", 1)[1] for l in log.splitlines()
+                                              if "INFO:cig =" in l])
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+"""Parity of the CUDA path with the oracle and the reference, through the C ABI.
+
+Tolerances (relative L2, ||a-b||/||b|| in double as src/rsf_l2cmp.cpp:9-10):
+  * against the FP64 oracle: 1e-5 (the north-star bound for the table path);
+  * against the reference binary's FP32 image: 1.5x the distance between the
+    reference and the FP64 oracle, plus 1e-6 (the reference's own rounding is
+    the larger error; the GPU path must not add to it).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import _cases
+import kirch_datuming_b200 as kd
+import oracle
+from kirch_datuming_b200 import rsf
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-5
+
+
+def gpu_image(gd, case, device=False, scratch=0, data=None):
+    import torch
+    kp, geom, axis, _, use_grad = _cases.case_setup(gd, case)
+    T, D = gd.tables()
+    d = gd.data(case) if data is None else data
+    plan = kd.Plan(kp, kd.geometry(**geom), scratch_bytes=scratch)
+    img = np.zeros((axis[0], geom["nx"], geom["nz"]), np.float32)
+    if device:
+        tT, tD = torch.from_numpy(T).cuda(), torch.from_numpy(D).cuda()
+        plan.set_tables(tT, tD, tT, tD)
+        if use_grad:
+            gx, gz = (torch.from_numpy(x).cuda() for x in gd.grads())
+            plan.set_gradients(gx, gz, gx, gz)
+        dimg = torch.zeros(img.shape, dtype=torch.float32, device="cuda")
+        plan.migrate(torch.from_numpy(np.ascontiguousarray(d)).cuda(), dimg)
+        img = dimg.cpu().numpy()
+    else:
+        plan.set_tables(T, D, T, D)
+        if use_grad:
+            gx, gz = gd.grads()
+            plan.set_gradients(gx, gz, gx, gz)
+        plan.migrate(np.ascontiguousarray(d, dtype=np.float32), img)
+    stats = plan.stats()
+    plan.close()
+    return img, stats
+
+
+@pytest.fixture(scope="module")
+def o64(golden):
+    return {c: _cases.oracle_image(golden, c, fp64=True) for c in golden.cases}
+
+
+@pytest.mark.parametrize("case", _cases.Golden().cases)
+def test_gpu_vs_fp64_oracle(golden, o64, case):
+    img, stats = gpu_image(golden, case)
+    assert stats["sum_launches"] >= 1
+    err = oracle.rel_l2(img, o64[case])
+    assert err <= TOL_FP64, err
+
+
+@pytest.mark.parametrize("case", _cases.Golden().cases)
+def test_gpu_vs_reference_golden(golden, o64, case):
+    img, _ = gpu_image(golden, case)
+    ref = golden.image(case)
+    k = _cases.ub_columns(golden, case)
+    ref_err = oracle.rel_l2(ref[:, k:], o64[case][:, k:])
+    err = oracle.rel_l2(img[:, k:], ref[:, k:])
+    assert err <= 1.5 * ref_err + 1e-6, (err, ref_err)
+
+
+def test_device_pointers_match_host(golden):
+    a, _ = gpu_image(golden, "base")
+    b, _ = gpu_image(golden, "base", device=True)
+    assert np.array_equal(a, b)
+
+
+def test_small_scratch_batches_match(golden, o64):
+    # a scratch cap of a few MB forces several shot batches and receiver chunks
+    for case in ("base", "cmp1_half"):
+        img, stats = gpu_image(golden, case, scratch=3 << 20)
+        assert stats["sum_launches"] > 1
+        assert oracle.rel_l2(img, o64[case]) <= TOL_FP64
+
+
+def test_zero_data_and_linearity(golden):
+    d = golden.data("base")
+    z, _ = gpu_image(golden, "base", data=np.zeros_like(d))
+    assert not np.any(z)
+    rng = np.random.default_rng(1)
+    e = rng.standard_normal(d.shape).astype(np.float32)
+    a, _ = gpu_image(golden, "base", data=d)
+    b, _ = gpu_image(golden, "base", data=e)
+    c, _ = gpu_image(golden, "base", data=(2.0 * d + 0.5 * e).astype(np.float32))
+    assert oracle.rel_l2(c, 2.0 * a.astype(np.float64) + 0.5 * b) < 1e-5
+
+
+def test_many_bins_chunked(golden):
+    # more bins than one launch keeps in shared memory: several bin chunks
+    import oracle as O
+    kp = kd.params("cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=90", "angle_step=0.2",
+                   "oazmin=180", "oazmax=180")
+    geom = golden.geometry_dict("base")
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    assert axis[0] == 451
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    img = np.zeros((axis[0], geom["nx"], geom["nz"]), np.float32)
+    plan.migrate(np.ascontiguousarray(golden.data("base")), img)
+    assert plan.stats()["sum_launches"] == 2
+    op = _cases.oracle_params(kp, geom, axis)
+    ref = O.migrate_adj(op, golden.data("base"), T, D, T, D)
+    assert oracle.rel_l2(img, ref) <= TOL_FP64
+
+
+@pytest.mark.parametrize("ns,nh", [(1, 21), (5, 1), (1, 1)])
+def test_single_shot_or_receiver(golden, ns, nh):
+    import oracle as O
+    kp = kd.params(*golden.tokens("base"))
+    geom = golden.geometry_dict("base")
+    geom.update(ns=ns, nh=nh)
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    d = np.ascontiguousarray(golden.data("base")[:ns, :nh])
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    img = np.zeros((axis[0], geom["nx"], geom["nz"]), np.float32)
+    plan.migrate(d, img)
+    ref = O.migrate_adj(_cases.oracle_params(kp, geom, axis), d, T, D, T, D)
+    assert oracle.rel_l2(img, ref) <= TOL_FP64
+
+
+def test_doubint_device_vs_oracle(golden):
+    import torch
+    d = golden.data("base").reshape(-1, golden.meta["nt"])[:37]
+    for isdiff in (0, 1):
+        out = kd.doubint_device(torch.from_numpy(np.ascontiguousarray(d)).cuda(), isdiff=isdiff, dt=0.002)
+        out = out.cpu().numpy()
+        for k in range(d.shape[0]):
+            ref = oracle.doubint(d[k], isdiff=isdiff, dt=0.002)
+            assert np.allclose(out[k], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("is_source,pos", [(1, 0.05), (1, 0.3133), (0, 0.2), (0, 0.7999), (1, -0.1), (0, 1.5)])
+def test_leg_fields_vs_oracle(golden, is_source, pos):
+    kp, geom, axis, op, _ = _cases.case_setup(golden, "base")
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    pos = float(np.float32(pos))  # the oracle entry point takes a float position
+    gT, gTx, gphi, gw = (x.cpu().numpy() for x in kd.leg_fields_device(plan, is_source, pos))
+    oT, oTx, ogx, ogz = oracle.leg_fields(op, is_source, T, D, pos)
+    assert np.allclose(gT, oT, rtol=1e-12, atol=1e-12)
+    assert np.allclose(gTx, oTx, rtol=1e-6, atol=1e-6)
+    ophi = np.arctan2(ogz, ogx)
+    ok = np.hypot(ogx, ogz) > 1e-9
+    dphi = np.abs(np.angle(np.exp(1j * (gphi[ok] - ophi[ok]))))
+    assert dphi.max() < 1e-9
+    assert np.all((gw >= 0) & (gw <= 1))
+
+
+def test_cli_end_to_end(golden, o64, tmp_path):
+    meta = golden.meta
+    t = meta["table"]
+    T, D = golden.tables()
+    rsf.write(str(tmp_path / "time.rsf"), T, t["n"], t["o"], t["d"])
+    rsf.write(str(tmp_path / "tds.rsf"), D, t["n"], t["o"], t["d"])
+    dd = meta["data"]["cmp0"]
+    rsf.write(str(tmp_path / "data.rsf"), golden.data("base"), [meta["nt"], dd["nh"], dd["ns"]],
+              [0, dd["h0"], dd["s0"]], [meta["dt"], dd["dh"], dd["ds"]], extra={"unit1": "s"})
+    args = ["seismic_data=data.rsf", "migration=mig.rsf", "stable=time.rsf", "sderiv=tds.rsf", "rtable=time.rsf",
+            "rderiv=tds.rsf"] + golden.tokens("base") + ["direct_mute_qc_shot=2", "direct_mute_qc_before=qb.rsf",
+                                                          "direct_mute_qc_after=qa.rsf"]
+    r = subprocess.run([kd.cli_path] + args, cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "Done. Elapsed time" in r.stderr
+    h, img = rsf.read(str(tmp_path / "mig.rsf"))
+    c = meta["cases"]["base"]
+    assert h.n[:3] == c["n"] and h.native
+    assert [round(v, 9) for v in h.o[:3]] == [round(v, 9) for v in c["o"]]
+    assert [round(v, 9) for v in h.d[:3]] == [round(v, 9) for v in c["d"]]
+    for k in ("label1", "label2", "label3", "unit1", "unit3"):
+        assert h.extra[k] == c["extra"][k]
+    assert oracle.rel_l2(img.reshape(o64["base"].shape), o64["base"]) <= TOL_FP64
+    # QC gathers: the reference's FP32 mute of shot 2, before and after
+    hb, qb = rsf.read(str(tmp_path / "qb.rsf"))
+    ha, qa = rsf.read(str(tmp_path / "qa.rsf"))
+    assert hb.n[:2] == [meta["nt"], dd["nh"]] and hb.extra["label2"] == "Receiver"
+    shot = golden.data("base")[2]
+    assert np.array_equal(qb.reshape(shot.shape), shot)
+    s = np.float32(dd["s0"]) + np.float32(2) * np.float32(dd["ds"])
+    for ih in range(dd["nh"]):
+        rx = np.float32(dd["h0"]) + np.float32(ih) * np.float32(dd["dh"])
+        ref = oracle.mute(shot[ih], 0.0, meta["dt"], s, rx, 0.5, 0.0, 0.05, fp64=False)
+        assert np.array_equal(qa.reshape(shot.shape)[ih], ref)
+    # the in-process entry point writes the same image
+    cwd = os.getcwd()
+    try:
+        os.chdir(tmp_path)
+        assert kd.run_cli([a if not a.startswith("migration=") else "migration=mig2.rsf" for a in args]) == 0
+    finally:
+        os.chdir(cwd)
+    _, img2 = rsf.read(str(tmp_path / "mig2.rsf"))
+    assert np.array_equal(img, img2)
