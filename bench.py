@@ -1,0 +1,383 @@
+"""Benchmark of the adjoint angle-domain Kirchhoff CIG migration (kirchmig2d_cig adj=1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kcig|reference]
+
+Workload (the production-size table-path configuration): five-layer 2-D model
+with a salt-like lens, nz=601 x nx=1601 at 10 m; 400 shots x 400 receivers on
+a fixed spread (cmp=0) every 40 m; nt=3001 at 1 ms; 15 Hz Ricker gathers from
+the model's traveltime tables plus 20 dB noise (seeded, synthetic); FP32
+tables at the 400 source/receiver positions; 61 angle bins over 0-60 degrees.
+One step = one migration of all 160,000 traces: 1.54e11 image-point x trace
+pairs.  Every step reads inputs far larger than L2 (1.9 GB of traces, 3.1 GB
+of tables), so L2 holds nothing between steps.
+
+Prints one JSON line (rank 0).  Multi-GPU (torchrun): every rank migrates its
+own 400-shot survey (weak scaling) and the images are summed with one NCCL
+all-reduce inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# ------------------------------------------------------------------ workload --
+NZ, NX, DZ = 601, 1601, 0.01
+NPOS, DP = 400, 0.04          # source/receiver positions 0 .. 15.96 km
+NT, DT = 3001, 0.001
+FREQ = 15.0
+TOKENS = ["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60", "angle_step=1", "angle_n=61",
+          "direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05"]
+WORKLOAD = "five-layer salt 601x1601@10m, 400 shots x 400 receivers (cmp=0, 40 m), nt=3001 dt=1ms, 61 angle bins"
+B_PAIR = 16  # algorithmic HBM bytes per pair: the receiver leg's T, dT/dr, gx, gz in FP32
+
+
+def geometry_dict(ns=NPOS, nh=NPOS):
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    return dict(nt=NT, nh=nh, ns=ns, t0=0.0, dt=f(DT), h0=0.0, dh=f(DP), s0=0.0, ds=f(DP), nz=NZ, nx=NX, z0=0.0,
+                dz=f(DZ), x0=0.0, dx=f(DZ), sny=NPOS, sy0=0.0, sdy=f(DP), rny=NPOS, ry0=0.0, rdy=f(DP))
+
+
+def make_workload(seed: int):
+    """Velocity, tables and gathers on the current CUDA device."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import synth
+    v, refl = synth.five_layer_salt(NZ, NX, DZ, DZ, seed=7)
+    vel = torch.from_numpy(v).cuda()
+    T, D = kd.eikonal_tables(vel, DZ, DZ, NPOS, 0.0, DP, iterations=3)
+    g = synth.Geometry(nz=NZ, nx=NX, dz=DZ, dx=DZ, z0=0, x0=0, ns=NPOS, s0=0.0, ds=DP, nh=NPOS, h0=0.0, dh=DP,
+                       cmp=0, nt=NT, dt=DT, t0=0.0, npos=NPOS, p0=0.0, dp=DP)
+    amps = synth.reflectivities(len(refl), seed)
+    data = synth.shot_gathers(T, g, [(rows, a) for rows, a in zip(refl.values(), amps)], FREQ, seed=seed)
+    torch.cuda.synchronize()
+    return v, T, D, data
+
+
+# ------------------------------------------------------------------ clocks ---
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "of measured"
+    except Exception:
+        return 6650.0, "of fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per pair of the summation kernel from the committed ncu
+    summary (profiles/k_sum_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_sum_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_pair"])
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------- reference (CPU) --
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "kirchmig2d_cig")
+REF_EIK = os.path.join(ROOT, "oracle", "_ref", "eikods2d")
+SAMPLE_SHOT = 200          # shot at 8.0 km
+SAMPLE_RCV = (176, 48)     # 48 receivers, 7.04 .. 8.92 km
+
+
+def prepare_sample(wd: str, threads: int, tables=None):
+    """Write the inputs of a bounded sample of the workload: one shot x 48
+    receivers over the full 601x1601 image (4.62e7 pairs).  Tables are cut
+    from the GPU workload's tables when given, else made by the reference's
+    own eikods2d for the positions the sample uses."""
+    from kirch_datuming_b200 import rsf, synth
+    import torch
+    r0, nr = SAMPLE_RCV
+    p_lo, p_hi = min(r0, SAMPLE_SHOT) - 1, max(r0 + nr, SAMPLE_SHOT + 1) + 1
+    npos = p_hi - p_lo
+    v, refl = synth.five_layer_salt(NZ, NX, DZ, DZ, seed=7)
+    if tables is not None:
+        T = np.ascontiguousarray(tables[0][p_lo:p_hi]).ravel()
+        D = np.ascontiguousarray(tables[1][p_lo:p_hi]).ravel()
+        src = "the GPU workload"
+    elif os.path.exists(REF_EIK):
+        rsf.write(f"{wd}/vel.rsf", v, [NZ, NX], [0, 0], [DZ, DZ])
+        rsf.write(f"{wd}/sht.rsf", np.array([[0.0, (p_lo + k) * DP, 0.0] for k in range(npos)], np.float32),
+                  [3, npos], [0, 0], [DP, 1])
+        subprocess.run([REF_EIK, "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf", "tds1=tds.rsf",
+                        "b1=2", "b2=2"], cwd=wd, check=True, capture_output=True,
+                       env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        _, T = rsf.read(f"{wd}/time.rsf")
+        _, D = rsf.read(f"{wd}/tds.rsf")
+        src = "eikods2d"
+    else:
+        raise RuntimeError("no tables for the CPU sample")
+    rsf.write(f"{wd}/time.rsf", T, [NZ, NX, npos], [0, 0, p_lo * DP], [DZ, DZ, DP])
+    rsf.write(f"{wd}/tds.rsf", D, [NZ, NX, npos], [0, 0, p_lo * DP], [DZ, DZ, DP])
+    g = synth.Geometry(nz=NZ, nx=NX, dz=DZ, dx=DZ, z0=0, x0=0, ns=1, s0=SAMPLE_SHOT * DP, ds=DP, nh=nr,
+                       h0=r0 * DP, dh=DP, cmp=0, nt=NT, dt=DT, t0=0.0, npos=npos, p0=p_lo * DP, dp=DP)
+    amps = synth.reflectivities(len(refl), 1)
+    data = synth.shot_gathers(torch.from_numpy(np.asarray(T).reshape(npos, NX, NZ)), g,
+                              [(rows, a) for rows, a in zip(refl.values(), amps)], FREQ, seed=1).numpy()
+    rsf.write(f"{wd}/data.rsf", data, [NT, nr, 1], [0, r0 * DP, SAMPLE_SHOT * DP], [DT, DP, DP],
+              extra={"unit1": "s"})
+    return {"npos": npos, "p_lo": p_lo, "pairs": nr * NZ * NX, "tables": src,
+            "sample": "1 shot (x=8.0 km) x 48 receivers (7.04-8.92 km) over the full 601x1601 image: "
+                      "%.3g pairs, same parameters; tables from %s" % (nr * NZ * NX, src)}
+
+
+def run_sample(wd: str, threads: int, meta: dict):
+    """Time the reference tool (or, without it, the oracle port) on the
+    prepared sample; returns a cpu_baseline dict."""
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    kind = "reference" if os.path.exists(REF_BIN) else "port"
+    if kind == "reference":
+        t = time.perf_counter()
+        r = subprocess.run([REF_BIN, "seismic_data=data.rsf", "migration=mig.rsf", "stable=time.rsf",
+                            "sderiv=tds.rsf", "rtable=time.rsf", "rderiv=tds.rsf", "adj=1"] + TOKENS,
+                           cwd=wd, capture_output=True, text=True, env=env)
+        wall = time.perf_counter() - t
+        if r.returncode != 0:
+            raise RuntimeError("reference failed: " + r.stderr[-2000:])
+        m = re.search(r"Done\. Elapsed time: ([0-9.]+) s", r.stdout + r.stderr)
+        el = float(m.group(1)) if m else wall
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle
+        import _cases
+        import kirch_datuming_b200 as kd
+        from kirch_datuming_b200 import rsf
+        r0, nr = SAMPLE_RCV
+        _, data = rsf.read(f"{wd}/data.rsf")
+        _, T = rsf.read(f"{wd}/time.rsf")
+        _, D = rsf.read(f"{wd}/tds.rsf")
+        f = lambda x: float(np.float32(x))  # noqa: E731
+        geom = dict(geometry_dict(1, nr), s0=f(SAMPLE_SHOT * DP), h0=f(r0 * DP), sny=meta["npos"],
+                    rny=meta["npos"], sy0=f(meta["p_lo"] * DP), ry0=f(meta["p_lo"] * DP))
+        kp = kd.params(*TOKENS)
+        axis = kd.output_axis(kp, kd.geometry(**geom))
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        t = time.perf_counter()
+        oracle.migrate_adj(_cases.oracle_params(kp, geom, axis), data, T, D, T, D, fp64=False)
+        el = time.perf_counter() - t
+    return {"value": meta["pairs"] / el / 1e9, "unit": "Gpairs/s", "cores": threads, "kind": kind,
+            "seconds": round(el, 3), "sample": meta["sample"]}
+
+
+def cpu_sample(threads: int, tables=None):
+    wd = tempfile.mkdtemp(prefix="kcig_cpu_")
+    try:
+        return run_sample(wd, threads, prepare_sample(wd, threads, tables))
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+
+
+# -------------------------------------------------------------------- main ---
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kcig", choices=["kcig", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    metric = "Gpairs/s (image pt×trace) on 1 B200, surrogate vs table path, relL2≤1e-3"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        vals = []
+        wd = tempfile.mkdtemp(prefix="kcig_ref_")
+        try:
+            meta = prepare_sample(wd, threads)
+            for _ in range(min(args.warmup, 1)):  # one untimed run warms the page cache
+                run_sample(wd, threads, meta)
+            for _ in range(max(1, args.steps)):
+                vals.append(run_sample(wd, threads, meta))
+        finally:
+            shutil.rmtree(wd, ignore_errors=True)
+        base = vals[0]
+        v = statistics.median([x["value"] for x in vals])
+        sec = statistics.median([x["seconds"] for x in vals])
+        line = {"metric": metric, "value": v, "unit": "Gpairs/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD + "; reference timed on a bounded sample per step",
+                           "sample": base["sample"]},
+                "cpu_baseline": {"value": v, "unit": "Gpairs/s", "cores": threads, "kind": base["kind"],
+                                 "sample": base["sample"]},
+                "e2e": {"value": v, "unit": "Gpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import kirch_datuming_b200 as kd
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    v, T, D, data = make_workload(seed=11 + rank)
+    kp = kd.params(*TOKENS)
+    geom = geometry_dict()
+    st = torch.cuda.current_stream()
+    plan = kd.Plan(kp, kd.geometry(**geom), stream=st.cuda_stream)
+    plan.set_tables(T, D, T, D)
+    ng = plan.ng
+    image = torch.zeros((ng, NX, NZ), dtype=torch.float32, device="cuda")
+    pairs = NPOS * NPOS * NZ * NX
+
+    def step():
+        plan.migrate(data, image)
+        if dist is not None:
+            dist.all_reduce(image)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sum_ms, launches = [], 0
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(args.steps):
+        step()
+        s = plan.stats()
+        sum_ms.append(s["sum_ms"] / max(1, s["sum_launches"]))
+        launches += s["launches"]
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # end to end through the public C ABI with pinned host buffers
+    hT, hD = T.cpu().pin_memory(), D.cpu().pin_memory()
+    hdata = data.cpu().pin_memory()
+    himg = torch.zeros((ng, NX, NZ), dtype=torch.float32).pin_memory()
+    eplan = kd.Plan(kp, kd.geometry(**geom))
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eplan.set_tables(hT, hD, hT, hD)
+        eplan.migrate(hdata, himg)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.median(e2e_ms[1:]) if len(e2e_ms) > 1 else e2e_ms[0]
+    eplan.close()
+    h2d = hT.numel() * 4 + hD.numel() * 4 + hdata.numel() * 4
+    d2h = himg.numel() * 4
+
+    ksum_ms = statistics.median(sum_ms)
+    peak, peak_src = measured_peaks()
+    achieved = pairs * B_PAIR / (ksum_ms / 1e3) / 1e9
+    tpp = profiled_traffic()
+    line = {
+        "metric": metric, "value": world * pairs / (ms / 1e3) / 1e9, "unit": "Gpairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_gpu_step": pairs, "parallelism": "dp%d (shots per rank, "
+                   "image all-reduce)" % world if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (1.9 GB traces, 3.1 GB tables per step)",
+                   "tables": "GPU fast-sweeping eikonal (kcig_eikonal_tables), 400 positions"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "kernel": "k_sum", "kernel_ms": ksum_ms,
+                     "algorithmic_bytes_per_pair": B_PAIR,
+                     "traffic": (tpp * pairs) if tpp is not None else None},
+        "e2e": {"value": world * pairs / (e2e_ms / 1e3) / 1e9 if world == 1 else None, "unit": "Gpairs/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()))
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:300]}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

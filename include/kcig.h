@@ -143,6 +143,18 @@ int kcig_doubint_device(const float *in, double *out, int ntr, int nt, int isdif
 int kcig_leg_fields_device(kcig_plan *plan, int is_source, double pos, double *T, float *Tx,
                            double *phi, float *w);
 
+/* Traveltime tables for the migration, the role of eikods2d
+ * (src/eikods2d.cpp:149-765, SERECKIRCH/src/eikods.cpp:66-211): sources at
+ * depth zsrc and lateral positions p0 + k*dp (k < npos); vel [nx][nz] in
+ * km/s (device).  Writes time [npos][nx][nz] and, if deriv is not NULL, the
+ * derivative of time with respect to the source position [npos][nx][nz]
+ * (device).  First-order fast sweeping (iterations x 4 sweeps) with the
+ * straight-ray times inside the (b1, b2) box around the source; the position
+ * derivative is the centred difference of neighbouring positions' tables. */
+int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, float z0, float x0,
+                        int npos, float p0, float dp, float zsrc, int b1, int b2, int iterations,
+                        float *time, float *deriv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
-           "run_cli", "doubint_device", "leg_fields_device", "library_path", "cli_path"]
+           "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "library_path", "cli_path"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(_HERE, "libkcig.so")
@@ -82,6 +82,9 @@ def lib():
         L.kcig_run_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
         L.kcig_doubint_device.argtypes = [fp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp]
         L.kcig_leg_fields_device.argtypes = [vp, ctypes.c_int, ctypes.c_double, dp, fp, dp, fp]
+        L.kcig_eikonal_tables.argtypes = [fp, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 4 + [
+            ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+            fp, fp, vp]
         _lib = L
     return _lib
 
@@ -212,3 +215,23 @@ def leg_fields_device(plan: Plan, is_source: int, pos: float):
     _check(lib().kcig_leg_fields_device(plan._h, int(is_source), float(pos), T.data_ptr(), Tx.data_ptr(),
                                         phi.data_ptr(), w.data_ptr()))
     return T, Tx, phi, w
+
+
+def eikonal_tables(vel, dz: float, dx: float, npos: int, p0: float, dp: float, z0: float = 0.0,
+                   x0: float = 0.0, zsrc: float = 0.0, b1: int = 2, b2: int = 2, iterations: int = 3,
+                   deriv: bool = True):
+    """Traveltime tables on the GPU for sources at p0 + k*dp (k < npos).
+
+    vel: CUDA float32 tensor [nx][nz] (km/s).  Returns (time, deriv) CUDA
+    tensors [npos][nx][nz] (deriv None when not requested)."""
+    import torch
+    if not (vel.is_cuda and vel.dtype == torch.float32 and vel.is_contiguous()):
+        raise ValueError("vel must be a contiguous CUDA float32 tensor [nx][nz]")
+    nx, nz = vel.shape
+    t = torch.empty((npos, nx, nz), dtype=torch.float32, device=vel.device)
+    d = torch.empty_like(t) if deriv else None
+    st = torch.cuda.current_stream().cuda_stream
+    _check(lib().kcig_eikonal_tables(vel.data_ptr(), nz, nx, dz, dx, z0, x0, npos, p0, dp, zsrc, b1, b2,
+                                     iterations, t.data_ptr(), d.data_ptr() if deriv else None,
+                                     ctypes.c_void_p(st)))
+    return t, d

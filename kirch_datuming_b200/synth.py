@@ -90,15 +90,12 @@ def five_layer_salt(nz: int, nx: int, dz: float, dx: float, seed: int = 7):
     bump = np.exp(-((x - xc) / width) ** 2)
     top = base - 0.16 * zmax * bump
     bot = base + 0.08 * zmax * bump
-    v = np.empty((nx, nz), dtype=np.float32)
-    zz = z[None, :]
-    v[:] = 1.5
+    zz = np.broadcast_to(z[None, :], (nx, nz))
+    v = np.full((nx, nz), 1.5, dtype=np.float32)
     v[zz >= z1] = 2.0
-    v[np.broadcast_to(zz >= z2, v.shape)] = 2.6
-    below = zz >= base
-    v[np.broadcast_to(below, v.shape)] = 3.2
-    salt = (zz >= top[:, None]) & (zz < bot[:, None])
-    v[salt] = 4.5
+    v[zz >= z2] = 2.6
+    v[zz >= base] = 3.2
+    v[(zz >= top[:, None]) & (zz < bot[:, None])] = 4.5
     deep = 0.85 * zmax
     refl = {
         "z1": np.full(nx, int(round(z1 / dz))),
