@@ -38,6 +38,7 @@ sys.path.insert(0, ROOT)
 # ------------------------------------------------------------------ workload --
 NZ, NX, DZ = 601, 1601, 0.01
 NPOS, DP = 400, 0.04          # source/receiver positions 0 .. 15.96 km
+SIZES = {"full": (400, 0.04), "small": (64, 0.24)}  # small: the same grid, 64 x 64 positions (profiling)
 NT, DT = 3001, 0.001
 FREQ = 15.0
 TOKENS = ["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60", "angle_step=1", "angle_n=61",
@@ -46,7 +47,9 @@ WORKLOAD = "five-layer salt 601x1601@10m, 400 shots x 400 receivers (cmp=0, 40 m
 B_PAIR = 16  # algorithmic HBM bytes per pair: the receiver leg's T, dT/dr, gx, gz in FP32
 
 
-def geometry_dict(ns=NPOS, nh=NPOS):
+def geometry_dict(ns=None, nh=None):
+    ns = NPOS if ns is None else ns
+    nh = NPOS if nh is None else nh
     f = lambda v: float(np.float32(v))  # noqa: E731
     return dict(nt=NT, nh=nh, ns=ns, t0=0.0, dt=f(DT), h0=0.0, dh=f(DP), s0=0.0, ds=f(DP), nz=NZ, nx=NX, z0=0.0,
                 dz=f(DZ), x0=0.0, dx=f(DZ), sny=NPOS, sy0=0.0, sdy=f(DP), rny=NPOS, ry0=0.0, rdy=f(DP))
@@ -244,7 +247,14 @@ def main():
     ap.add_argument("--impl", default="kcig", choices=["kcig", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--size", default="full", choices=sorted(SIZES),
+                    help="small: 64 shots x 64 receivers every 240 m on the same grid (ncu captures)")
     args = ap.parse_args()
+    global NPOS, DP, WORKLOAD
+    NPOS, DP = SIZES[args.size]
+    if args.size != "full":
+        WORKLOAD = WORKLOAD.replace("400 shots x 400 receivers (cmp=0, 40 m)",
+                                    "%d shots x %d receivers (cmp=0, %g m)" % (NPOS, NPOS, DP * 1000))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -365,7 +375,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and args.size == "full":
         try:
             line["cpu_baseline"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()))
         except Exception as e:  # the baseline is reported, never required
