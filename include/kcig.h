@@ -143,6 +143,29 @@ int kcig_doubint_device(const float *in, double *out, int ntr, int nt, int isdif
 int kcig_leg_fields_device(kcig_plan *plan, int is_source, double pos, double *T, float *Tx,
                            double *phi, float *w);
 
+/* Allocation-free variant of kcig_leg_fields_device; it has no counterpart in
+ * the reference.  For callers that cannot allocate device memory -- a host
+ * application whose device memory belongs to its own allocator or is budgeted
+ * to the byte, or code running where a cudaMalloc would synchronise the device
+ * or fail -- it computes the same T, Tx, phi and w for one position without any
+ * allocation, using a fixed 16 MiB scratch array built into the library (each
+ * device that loads the library holds it until the process exits).  Limit:
+ * nz*nx <= 262144 points, else KCIG_ERR_ARG.  p/g give the parameters and the
+ * axes (the source or receiver position axis of g is used); table/deriv are
+ * the device tables [npos][nx][nz]; gradx/gradz are the optional device
+ * gradient volumes (both or NULL); outputs are caller-owned device arrays
+ * [nx][nz] (any may be NULL).  The first call on a device looks up the
+ * scratch array's device address, so make that first call before any stream
+ * capture.  All calls share the one array and leave the last call's contents
+ * in it (every value is written before it is read, so nothing needs clearing);
+ * calls that overlap on the GPU -- from other threads or other streams --
+ * race and must be serialised by the caller.  Runs on `stream` and returns
+ * after it completes. */
+int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry *g, const float *table,
+                            const float *deriv, const float *gradx, const float *gradz,
+                            int is_source, double pos, double *T, float *Tx, double *phi, float *w,
+                            void *stream);
+
 /* Traveltime tables for the migration, the role of eikods2d
  * (src/eikods2d.cpp:149-765, SERECKIRCH/src/eikods.cpp:66-211): sources at
  * depth zsrc and lateral positions p0 + k*dp (k < npos); vel [nx][nz] in

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "kcig_common.h"
@@ -624,4 +625,107 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
         cudaEventDestroy(evs[i + 1]);
     }
     return rc;
+}
+
+// ------------------------------------------------- allocation-free variant --
+// kcig_leg_fields_noalloc computes what kcig_leg_fields_device computes, for
+// callers that may not allocate device memory: host applications whose device
+// memory is owned by another allocator or budgeted to the byte, and code that
+// runs where a cudaMalloc would synchronise or fail.  Its scratch -- the leg
+// descriptor, the {T, phi} and {Tx, w} planes and the four FP64 gradient
+// planes -- lives in the fixed array below, which every device that loads the
+// library holds until the process exits.
+#define KCIG_NOALLOC_MAX_POINTS (1 << 18)  // nz*nx limit of the fixed scratch
+#define KCIG_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[KCIG_NOALLOC_SCRATCH_BYTES];
+static_assert(sizeof(LegInterp) <= 256, "descriptor slot");
+static_assert(256 + (size_t)KCIG_NOALLOC_MAX_POINTS * 56 <= KCIG_NOALLOC_SCRATCH_BYTES, "scratch layout");
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[256];  // device address of g_noalloc_scratch, per device ordinal
+
+// Host code cannot use g_noalloc_scratch as an address: the name denotes a
+// host-side shadow.  The device address is looked up once per device, with
+// that device current.
+int noalloc_scratch(void **out)
+{
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return set_error(KCIG_ERR_ARG, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return KCIG_OK;
+}
+}  // namespace
+
+extern "C" int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry *g, const float *table,
+                                       const float *deriv, const float *gradx, const float *gradz, int is_source,
+                                       double pos, double *T, float *Tx, double *phi, float *w, void *stream)
+{
+    if (!p || !g || !table || !deriv) return set_error(KCIG_ERR_ARG, "kcig_leg_fields_noalloc: null argument");
+    if ((gradx == nullptr) != (gradz == nullptr))
+        return set_error(KCIG_ERR_ARG, "kcig_leg_fields_noalloc: give both gradient volumes or neither");
+    if (g->nz < 1 || g->nx < 1 || (is_source ? g->sny : g->rny) < 1)
+        return set_error(KCIG_ERR_ARG, "kcig_leg_fields_noalloc: empty grid or position axis");
+    const long long nzx = (long long)g->nz * g->nx;
+    if (nzx > KCIG_NOALLOC_MAX_POINTS)
+        return set_error(KCIG_ERR_ARG, "kcig_leg_fields_noalloc: nz*nx=%lld exceeds the allocation-free limit %d",
+                         nzx, KCIG_NOALLOC_MAX_POINTS);
+    void *base = nullptr;
+    KCIG_TRY(noalloc_scratch(&base));
+    cudaStream_t st = (cudaStream_t)stream;
+    // scratch layout: [descriptor | {T,phi} | {Tx,w} | 4 gradient planes]
+    char *s = (char *)base;
+    LegInterp *d_leg = (LegInterp *)s;
+    double2 *d_tp = (double2 *)(s + 256);
+    float2 *d_xw = (float2 *)((char *)d_tp + (size_t)nzx * sizeof(double2));
+    double *d_work = (double *)((char *)d_xw + (size_t)nzx * sizeof(float2));
+
+    kcig_plan view;  // parameter/geometry view for leg_interp; owns no device memory
+    view.p = *p;
+    view.g = *g;
+    LegInterp L;
+    leg_interp(&view, is_source, (float)pos, pos, &L);
+    L.scale = 1.0f;
+    KCIG_CUDA(cudaMemcpyAsync(d_leg, &L, sizeof L, cudaMemcpyHostToDevice, st));
+    FieldArgs a;
+    a.tab = table;
+    a.der = deriv;
+    a.gxv = gradx;
+    a.gzv = gradz;
+    a.legs = d_leg;
+    a.n = 1;
+    a.nz = g->nz;
+    a.nx = g->nx;
+    a.dz = g->dz;
+    a.dx = g->dx;
+    a.x0 = g->x0;
+    a.radius = p->angle_grad_radius;
+    a.smooth = p->angle_smooth;
+    a.angle = p->cig && p->cig_is_angle;
+    a.use_grad = gradx != nullptr;
+    a.aper = p->aperture;
+    a.aper_taper = p->aperture_taper;
+    a.rmin = p->aperture_rmin;
+    a.rtaper = p->aperture_rtaper;
+    KCIG_TRY(launch_leg_fields(a, LegFields{d_tp, d_xw}, d_work, st));
+    struct Cp { void *dst; const char *src; size_t el, pitch; } cps[4] = {
+        {T, (const char *)d_tp, sizeof(double), sizeof(double2)},
+        {phi, (const char *)d_tp + sizeof(double), sizeof(double), sizeof(double2)},
+        {Tx, (const char *)d_xw, sizeof(float), sizeof(float2)},
+        {w, (const char *)d_xw + sizeof(float), sizeof(float), sizeof(float2)}};
+    for (const Cp &c : cps) {
+        if (!c.dst) continue;
+        KCIG_CUDA(cudaMemcpy2DAsync(c.dst, c.el, c.src, c.pitch, c.el, (size_t)nzx, cudaMemcpyDeviceToDevice, st));
+    }
+    KCIG_CUDA(cudaStreamSynchronize(st));
+    return KCIG_OK;
 }
