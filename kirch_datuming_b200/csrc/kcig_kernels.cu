@@ -1,8 +1,9 @@
 // sm_100a kernels of the adjoint angle-domain Kirchhoff summation.
 //
 //   K1 k_prelude      per-trace direct mute + doubint (FP64 running sums) +
-//                     optional diff2, written as {D[i], D[i+1]} pairs so a
-//                     linear-interpolated pick is one 16-byte load.
+//                     optional diff2, written as {D[i], D[i+1]-D[i]} pairs so
+//                     a linear-interpolated pick is one 16-byte load and one
+//                     fused multiply-add.
 //   K2 k_leg_*        per source/receiver position: table interpolation along
 //                     the position axis, traveltime gradient, triangle
 //                     smoothing and the aperture leg weight ("leg fields").
@@ -130,7 +131,7 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
     for (int i = lane; i < a.nt; i += 32) {
         double2 e;
         e.x = s[i];
-        e.y = (i + 1 < a.nt) ? s[i + 1] : 0.0;
+        e.y = (i + 1 < a.nt) ? s[i + 1] - s[i] : 0.0;
         out[i] = e;
     }
 }
@@ -403,54 +404,28 @@ __device__ __forceinline__ float depth_weight(float ang, float cutoff, float ban
     return 0.5f * (1.0f + cosf(3.14159265358979f * u));
 }
 
-// kirmig_pick (kirmig.cpp:34-58), adj branch.  The time-to-sample mapping and
-// the six-term sum run in FP64: with long traces and multi-second times the
-// FP32 fractional sample position alone costs more than the 1e-5 image error
-// budget.  Returns false when the reference would return without picking.
-__device__ __forceinline__ bool pick(const double2 *__restrict__ Dk, double ti, float deltat,
-                                     const SumArgs &a, float *out)
-{
-    // every test is written so that a NaN time (a NaN table entry) fails it,
-    // as the reference's integer conversion of a NaN does (kirmig.cpp:41-49)
-    const double ft0 = (ti - a.t0) * a.inv_dt;
-    const double fl = floor(ft0);
-    if (!(fl >= 0.0 && fl < (double)(a.nt - 1))) return false;
-    const double dl = (double)deltat;
-    const double tm = ti - dl - a.dt;
-    const double ftm0 = (tm - a.t0) * a.inv_dt;
-    const double flm = floor(ftm0);
-    if (!(flm >= 0.0 && flm <= fl)) return false;
-    const double tp = ti + dl + a.dt;
-    const double ftp0 = (tp - a.t0) * a.inv_dt;
-    const double flp = floor(ftp0);
-    if (!(flp >= fl && flp < (double)(a.nt - 1))) return false;
-    const double2 q0 = __ldg(Dk + (int)fl);
-    const double2 qm = __ldg(Dk + (int)flm);
-    const double2 qp = __ldg(Dk + (int)flp);
-    const double ft = ft0 - fl, ftm = ftm0 - flm, ftp = ftp0 - flp;
-    const float den = a.dtf + (float)(tp - tm);
-    float imp = a.dtf / den;
-    imp *= imp;
-    const double s = 2.0 * fma(ft, q0.y - q0.x, q0.x) - fma(ftm, qm.y - qm.x, qm.x) -
-                     fma(ftp, qp.y - qp.x, qp.x);
-    *out = (float)((double)imp * s);
-    return true;
-}
-
 // One CTA owns a TZ x TX image tile (one thread per image point) and keeps
 // its [bins][points] FP32 accumulators in shared memory: each thread only
 // touches its own column, so there are no atomics and no block barriers.
 // Shots are taken KB at a time with their leg fields in registers; each
 // receiver's leg fields are loaded once per shot block when receivers are
-// shared by all shots (cmp=0).  Per pair (kirchmig2d_cig.cpp:1206-1339):
-// aperture gate, FP64 traveltime sum, opening angle as the folded difference
-// of the two legs' gradient directions (exact in FP64, no per-pair arc
-// tangent), angle tapers, linear angle bins, the antialiased pick.
+// shared by all shots (cmp=0), one receiver ahead of use.  Per pair
+// (kirchmig2d_cig.cpp:1206-1339), cheapest rejections first: trace weight,
+// aperture gate, opening angle as the folded difference of the two legs'
+// gradient directions (exact in FP64, no per-pair arc tangent) and its bin
+// range, the angle tapers, then the antialiased pick from {D[i], D[i+1]-D[i]}
+// with its time-to-sample mapping and six-term sum in FP64.  Rejections are
+// mostly uniform across a warp (32 neighbouring image points), so skipping
+// them costs little.
+#ifndef KCIG_SUM_MINB
+#define KCIG_SUM_MINB 1  // resident CTAs per SM the register allocation must allow
+#endif
+
 template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
-__global__ void __launch_bounds__(TZ *TX) k_sum(const __grid_constant__ SumArgs a)
+__global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_constant__ SumArgs a)
 {
     constexpr int P = TZ * TX;
-    constexpr double kTwoPi = 6.283185307179586476925;
+    constexpr double kPiD = 3.141592653589793238463, kTwoPi = 6.283185307179586476925;
     extern __shared__ float acc[];  // [nbins][P]
     const int tid = threadIdx.x;
     const int tiles_z = (a.nz + TZ - 1) / TZ;
@@ -469,6 +444,8 @@ __global__ void __launch_bounds__(TZ *TX) k_sum(const __grid_constant__ SumArgs 
     const float zf = (a.nz > 1) ? (float)iz / (float)(a.nz - 1) : 0.0f;
     const float cutoff = a.oazmin + zf * (a.oazmax - a.oazmin);
     const double ulo = -1.0e-5, uhi = (double)(a.ng - 1) + 1.0e-5;
+    const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;  // u = th*uk - ub
+    const double top = (double)(a.nt - 1);
 
     for (int sb = 0; sb < a.nsb; sb += KB) {
         double2 sTP[KB];
@@ -483,12 +460,18 @@ __global__ void __launch_bounds__(TZ *TX) k_sum(const __grid_constant__ SumArgs 
                 sXW[k] = make_float2(0.f, 0.f);
             }
         }
+        double2 nTP = make_double2(0.0, 0.0);
+        float2 nXW = make_float2(0.f, 0.f);
+        if (SHARED_R) {
+            nTP = __ldg(a.RTP + i);
+            nXW = __ldg(a.RXW + i);
+        }
         for (int r = 0; r < a.nh; r++) {
-            double2 rTP = make_double2(0.0, 0.0);
-            float2 rXW = make_float2(0.f, 0.f);
-            if (SHARED_R) {
-                rTP = __ldg(a.RTP + (size_t)r * nzx + i);
-                rXW = __ldg(a.RXW + (size_t)r * nzx + i);
+            double2 rTP = nTP;
+            float2 rXW = nXW;
+            if (SHARED_R && r + 1 < a.nh) {  // next receiver, one ahead of use
+                nTP = __ldg(a.RTP + (size_t)(r + 1) * nzx + i);
+                nXW = __ldg(a.RXW + (size_t)(r + 1) * nzx + i);
             }
 #pragma unroll
             for (int k = 0; k < KB; k++) {
@@ -503,58 +486,62 @@ __global__ void __launch_bounds__(TZ *TX) k_sum(const __grid_constant__ SumArgs 
                 }
                 const float apw = sXW[k].y * rXW.y;
                 if (!(apw > 0.0f)) continue;
-                const double ti = sTP[k].x + rTP.x + a.tau;
-                const float txw = fmaxf(fabsf(sXW[k].x), fabsf(rXW.x));
-                const double2 *Dk = a.D + (size_t)trc * a.nt;
+                int b0 = 0;
+                float w0 = 1.0f, w1 = 0.0f, aw;
                 if (MODE == 2) {
-                    float picked;
-                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
-                    const int ig = __ldg(a.igo + trc) - gc0;
-                    if (ig < 0 || ig >= nb) continue;
-                    acc[ig * P + tid] += tw * apw * picked;
-                    continue;
-                }
-                // opening angle (:171-187): atan2(|s x r|, s.r) is the
-                // difference of the gradient directions folded to [0, pi]
-                double th = fabs(sTP[k].y - rTP.y);
-                if (th > 3.141592653589793238463) th = kTwoPi - th;
-                if (!(th == th)) continue;  // a vanishing gradient: angle NaN, weight 0
-                const double angd = th * a.deg;
-                const float ang = (float)angd;
-                const float aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw * apw;
-                if (!(aw > 0.0f)) continue;
-                const double u = (angd - a.ug0) * a.uinv;
-                if (MODE == 0) {
-                    // value_to_linear_bins (:54-79)
-                    if (!(u >= ulo && u <= uhi)) continue;
-                    int ig0, ig1;
-                    float w0, w1;
-                    if (u <= 0.0) { ig0 = ig1 = 0; w0 = 1.0f; w1 = 0.0f; }
-                    else if (u >= (double)(a.ng - 1)) { ig0 = ig1 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
-                    else {
-                        const double fl = floor(u);
-                        ig0 = (int)fl;
-                        ig1 = ig0 + 1;
-                        const double f1 = u - fl;
-                        w1 = (float)f1;
-                        w0 = (float)(1.0 - f1);
-                    }
-                    float picked;
-                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
-                    picked *= aw;
-                    ig0 -= gc0;
-                    ig1 -= gc0;
-                    if (ig0 >= 0 && ig0 < nb) acc[ig0 * P + tid] += w0 * picked;
-                    if (ig1 != ig0 && w1 > 0.0f && ig1 >= 0 && ig1 < nb) acc[ig1 * P + tid] += w1 * picked;
+                    b0 = __ldg(a.igo + trc) - gc0;
+                    if (b0 < 0 || b0 >= nb) continue;
+                    aw = tw * apw;
                 } else {
-                    // value_to_nearest_bin (:35-41)
-                    const double fn = floor(u + 0.5);
-                    if (!(fn >= 0.0 && fn < (double)a.ng)) continue;
-                    float picked;
-                    if (!pick(Dk, ti, txw * a.aal, a, &picked)) continue;
-                    const int il = (int)fn - gc0;
-                    if (il >= 0 && il < nb) acc[il * P + tid] += aw * picked;
+                    // opening angle (:171-187): atan2(|s x r|, s.r) is the
+                    // difference of the gradient directions folded to [0, pi]
+                    double th = fabs(sTP[k].y - rTP.y);
+                    th = (th > kPiD) ? kTwoPi - th : th;
+                    const double u = fma(th, uk, -ub);  // bin coordinate; NaN: vanishing gradient
+                    double fl;
+                    if (MODE == 0) {
+                        // value_to_linear_bins (:54-79)
+                        if (!(u >= ulo && u <= uhi)) continue;
+                        fl = floor(u);
+                    } else {
+                        // value_to_nearest_bin (:35-41)
+                        fl = floor(u + 0.5);
+                        if (!(fl >= 0.0 && fl < (double)a.ng)) continue;
+                    }
+                    const float ang = (float)(th * a.deg);
+                    aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw * apw;
+                    if (!(aw > 0.0f)) continue;
+                    if (MODE == 0) {
+                        if (u <= 0.0) { b0 = 0; w0 = 1.0f; w1 = 0.0f; }
+                        else if (u >= (double)(a.ng - 1)) { b0 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
+                        else {
+                            b0 = (int)fl;
+                            const double f1 = u - fl;
+                            w1 = (float)f1;
+                            w0 = (float)(1.0 - f1);
+                        }
+                    } else {
+                        b0 = (int)fl;
+                    }
+                    b0 -= gc0;
                 }
+                // kirmig_pick (kirmig.cpp:34-58): sample positions of t,
+                // t-deltat-dt and t+deltat+dt in FP64; every test fails on NaN
+                const double ft0 = (sTP[k].x + rTP.x + a.tau - a.t0) * a.inv_dt;
+                const double sh = fma((double)(fmaxf(fabsf(sXW[k].x), fabsf(rXW.x)) * a.aal), a.inv_dt, 1.0);
+                const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
+                const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
+                if (!(fl0 >= 0.0 && fl0 < top && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < top)) continue;
+                const double2 *Dk = a.D + (size_t)trc * a.nt;
+                const double2 q0 = __ldg(Dk + (int)fl0);
+                const double2 qm = __ldg(Dk + (int)flm);
+                const double2 qp = __ldg(Dk + (int)flp);
+                const float r1 = 1.0f / (1.0f + 2.0f * (float)sh);  // dt / (dt + tp - tm)
+                const double sum = 2.0 * fma(ft0 - fl0, q0.y, q0.x) - fma(ftm0 - flm, qm.y, qm.x) -
+                                   fma(ftp0 - flp, qp.y, qp.x);
+                const float picked = (float)((double)(r1 * r1) * sum) * aw;
+                if (b0 >= 0 && b0 < nb) acc[b0 * P + tid] += w0 * picked;
+                if (MODE == 0 && w1 > 0.0f && b0 + 1 >= 0 && b0 + 1 < nb) acc[(b0 + 1) * P + tid] += w1 * picked;
             }
         }
     }
@@ -587,6 +574,11 @@ static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
     return launch_sum_t<TZ, TX, 1, false, 2>(a, nb, st);
 }
 
+// Shots per block of the receiver-shared path (register-resident source legs).
+#ifndef KCIG_KB
+#define KCIG_KB 4
+#endif
+
 // Shared memory holds [bins][points] FP32 accumulators: 256-point tiles while
 // the bins fit in 100 KB (two CTAs per SM), smaller tiles above, and bin
 // chunks of at most 384 bins beyond that.
@@ -599,9 +591,9 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
         a.gchunk1 = min(a0.ng, g + maxb);
         const int nb = a.gchunk1 - a.gchunk0;
         int rc;
-        if ((size_t)nb * 256 * 4 <= 100 * 1024) rc = launch_sum_mode<16, 16, 4>(a, nb, st);
-        else if ((size_t)nb * 128 * 4 <= 200 * 1024) rc = launch_sum_mode<16, 8, 4>(a, nb, st);
-        else rc = launch_sum_mode<8, 8, 4>(a, nb, st);
+        if ((size_t)nb * 256 * 4 <= 100 * 1024) rc = launch_sum_mode<16, 16, KCIG_KB>(a, nb, st);
+        else if ((size_t)nb * 128 * 4 <= 200 * 1024) rc = launch_sum_mode<16, 8, KCIG_KB>(a, nb, st);
+        else rc = launch_sum_mode<8, 8, KCIG_KB>(a, nb, st);
         if (rc) return rc;
         if (launches) (*launches)++;
     }
