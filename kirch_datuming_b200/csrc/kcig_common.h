@@ -92,6 +92,7 @@ struct SumArgs {
     int zero_init;
     int nz, nx, nt, nsb, nh, ng;
     int mode;              // 0 angle two-bin, 1 angle nearest, 2 single bin (offset/stack)
+    int unit_tw;           // every trace weight of the batch is 1: trw is not read
     int shared_r;          // receiver fields indexed by ih only (cmp=0)
     int half;
     double t0, dt, inv_dt, tau;

@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
             for (int k = 0; k < KB; k++) {
                 if (sb + k >= a.nsb) break;
                 const int trc = (sb + k) * a.nh + r;
-                const float tw = __ldg(a.trw + trc);
+                const float tw = a.unit_tw ? 1.0f : __ldg(a.trw + trc);
                 if (tw == 0.0f) continue;  // trace removed by aperture_trace / offset bin
                 if (!SHARED_R) {
                     const int ri = __ldg(a.rfi + trc);

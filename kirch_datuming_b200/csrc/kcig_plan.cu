@@ -571,6 +571,8 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             sa.nh = nhb;
             sa.ng = P->ng;
             sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
+            // a uniform flag spares the pair loop a dependent load per pair
+            sa.unit_tw = std::all_of(h_trw.begin(), h_trw.begin() + nb, [](float v) { return v == 1.0f; }) ? 1 : 0;
             sa.shared_r = shared_r ? 1 : 0;
             sa.half = p.half_angle;
             sa.t0 = g.t0;
