@@ -417,8 +417,13 @@ __device__ __forceinline__ float depth_weight(float ang, float cutoff, float ban
 // with its time-to-sample mapping and six-term sum in FP64.  Rejections are
 // mostly uniform across a warp (32 neighbouring image points), so skipping
 // them costs little.
+// Resident CTAs per SM the register allocation must allow: 6 CTAs of 128
+// threads (24 warps) is the most the 61-bin accumulators' shared memory
+// admits without spilling registers; occupancy is what this latency-bound
+// loop needs (measured: 16x16 tiles at 2 CTAs/SM 16.2 ms, 16x8 at 6 CTAs/SM
+// 13.8 ms on the 64x64-position case of the benchmark model).
 #ifndef KCIG_SUM_MINB
-#define KCIG_SUM_MINB 1  // resident CTAs per SM the register allocation must allow
+#define KCIG_SUM_MINB 6
 #endif
 
 template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
@@ -574,14 +579,21 @@ static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
     return launch_sum_t<TZ, TX, 1, false, 2>(a, nb, st);
 }
 
-// Shots per block of the receiver-shared path (register-resident source legs).
+// Shots per block of the receiver-shared path (register-resident source
+// legs) and the tile of one CTA while the bins fit in 100 KB.
 #ifndef KCIG_KB
 #define KCIG_KB 4
 #endif
+#ifndef KCIG_TZ
+#define KCIG_TZ 16
+#endif
+#ifndef KCIG_TX
+#define KCIG_TX 8
+#endif
 
-// Shared memory holds [bins][points] FP32 accumulators: 256-point tiles while
-// the bins fit in 100 KB (two CTAs per SM), smaller tiles above, and bin
-// chunks of at most 384 bins beyond that.
+// Shared memory holds [bins][points] FP32 accumulators: TZ x TX-point tiles
+// while a launch's bins fit in 200 KB, 8x8 tiles beyond, and launches of at
+// most 384 bins.
 int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
 {
     const int maxb = 384;
@@ -591,8 +603,7 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
         a.gchunk1 = min(a0.ng, g + maxb);
         const int nb = a.gchunk1 - a.gchunk0;
         int rc;
-        if ((size_t)nb * 256 * 4 <= 100 * 1024) rc = launch_sum_mode<16, 16, KCIG_KB>(a, nb, st);
-        else if ((size_t)nb * 128 * 4 <= 200 * 1024) rc = launch_sum_mode<16, 8, KCIG_KB>(a, nb, st);
+        if ((size_t)nb * KCIG_TZ * KCIG_TX * 4 <= 200 * 1024) rc = launch_sum_mode<KCIG_TZ, KCIG_TX, KCIG_KB>(a, nb, st);
         else rc = launch_sum_mode<8, 8, KCIG_KB>(a, nb, st);
         if (rc) return rc;
         if (launches) (*launches)++;
