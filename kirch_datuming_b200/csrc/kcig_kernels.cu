@@ -356,6 +356,123 @@ __global__ void k_leg_pack(FieldArgs a, LegFields out, const double *work)
     tp->y = phi;
 }
 
+// compute_grad_plane + smooth_grad_component x2 + the direction, fused for
+// one kGradTile x kGradTile block of image points of one position.  The
+// interpolated traveltime is staged in shared memory with a halo of r + 2s
+// samples; the centred differences (radius r), the four box averages (radius
+// s; z, x, z, x as :438-492, both components per pass) and the arc tangent
+// all run there in FP64, and only the direction goes back to HBM.  Every
+// window is clamped to the GRID, as the reference's full-plane passes are,
+// so a tile reproduces them; divisions by a window's length are
+// multiplications by its reciprocal (one rounding apart).
+constexpr int kGradTile = 32;
+
+// One box average along z (AXIS 0) or x (AXIS 1) of the local cells
+// [z0,z1) x [x0,x1), already clipped to the grid; the window is clamped to
+// the grid's local range [glo, ghi) of that axis.  rcp[k] = 1 / (k + 1).
+template <int AXIS>
+__device__ __forceinline__ void box_tile(const double *in0, double *out0, const double *in1, double *out1, int W,
+                                         int s, int z0, int z1, int x0, int x1, int glo, int ghi, const double *rcp)
+{
+    for (int lx = x0 + (int)threadIdx.y; lx < x1; lx += blockDim.y)
+        for (int lz = z0 + (int)threadIdx.x; lz < z1; lz += blockDim.x) {
+            const int c = AXIS == 0 ? lz : lx;
+            const int a0 = max(c - s, glo), b0 = min(c + s, ghi - 1);
+            const int step = AXIS == 0 ? 1 : W;
+            const int base = AXIS == 0 ? lx * W + a0 : a0 * W + lz;
+            double s0 = 0.0, s1 = 0.0;
+            for (int k = 0; k <= b0 - a0; k++) {
+                s0 += in0[base + k * step];
+                s1 += in1[base + k * step];
+            }
+            out0[lx * W + lz] = s0 * rcp[b0 - a0];
+            out1[lx * W + lz] = s1 * rcp[b0 - a0];
+        }
+}
+
+__global__ void __launch_bounds__(256) k_leg_grad_fused(FieldArgs a, LegFields out)
+{
+    extern __shared__ double gsm[];
+    const int nz = a.nz, nx = a.nx;
+    const size_t nzx = (size_t)nz * nx;
+    const int r = a.radius < 1 ? 1 : a.radius, s = a.smooth;
+    const int H = r + 2 * s, W = kGradTile + 2 * H;
+    const int tiles_z = (nz + kGradTile - 1) / kGradTile;
+    const int gz0 = (int)(blockIdx.x % tiles_z) * kGradTile - H, gx0 = (int)(blockIdx.x / tiles_z) * kGradTile - H;
+    // the grid in local coordinates
+    const int zlo = max(0, -gz0), zhi = min(W, nz - gz0), xlo = max(0, -gx0), xhi = min(W, nx - gx0);
+    double *P0 = gsm, *P1 = P0 + W * W, *P2 = P1 + W * W, *P3 = P2 + W * W;
+    double *rcpb = P3 + W * W, *rcpx = rcpb + 2 * s + 1, *rcpz = rcpx + 2 * r + 1;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+    const double2 *TP = out.TP + (size_t)blockIdx.y * nzx;
+    double2 *TPo = out.TP + (size_t)blockIdx.y * nzx;
+
+    // the traveltimes of the tile and its halo, all loads in flight at once
+    for (int lx = xlo + (int)threadIdx.y; lx < xhi; lx += blockDim.y)
+        for (int lz = zlo + (int)threadIdx.x; lz < zhi; lz += blockDim.x) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(P0 + lx * W + lz);
+            const double2 *src = TP + (size_t)(gx0 + lx) * nz + (gz0 + lz);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+        }
+    for (int k = tid; k <= 2 * s; k += nthr) rcpb[k] = 1.0 / (double)(k + 1);
+    for (int k = tid; k <= 2 * r; k += nthr) {
+        rcpx[k] = k ? 1.0 / ((double)k * a.dx) : 0.0;
+        rcpz[k] = k ? 1.0 / ((double)k * a.dz) : 0.0;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+
+    // centred differences on [r, W-r)^2: gx -> P1, gz -> P2
+    const bool dox = nx > 1 && a.dx != 0.0f, doz = nz > 1 && a.dz != 0.0f;
+    for (int lx = max(r, xlo) + (int)threadIdx.y; lx < min(W - r, xhi); lx += blockDim.y)
+        for (int lz = max(r, zlo) + (int)threadIdx.x; lz < min(W - r, zhi); lz += blockDim.x) {
+            double vx = 0.0, vz = 0.0;
+            if (dox) {
+                const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
+                if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
+            }
+            if (doz) {
+                const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
+                if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
+            }
+            P1[lx * W + lz] = vx;
+            P2[lx * W + lz] = vz;
+        }
+    __syncthreads();
+
+    if (s > 0) {
+        // each pass narrows the cells it must produce by s along its own
+        // axis; the cells the next pass reads are always inside
+        const int i1 = r + s, i2 = H;
+        box_tile<0>(P1, P0, P2, P3, W, s, max(i1, zlo), min(W - i1, zhi), max(r, xlo), min(W - r, xhi), zlo, zhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<1>(P0, P1, P3, P2, W, s, max(i1, zlo), min(W - i1, zhi), max(i1, xlo), min(W - i1, xhi), xlo, xhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<0>(P1, P0, P2, P3, W, s, max(i2, zlo), min(W - i2, zhi), max(i1, xlo), min(W - i1, xhi), zlo, zhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<1>(P0, P1, P3, P2, W, s, max(i2, zlo), min(W - i2, zhi), max(i2, xlo), min(W - i2, xhi), xlo, xhi,
+                    rcpb);
+        __syncthreads();
+    }
+    // scattering_angle_deg_from_grad (:171-187) returns NaN for a vanishing gradient
+    for (int lx = max(H, xlo) + (int)threadIdx.y; lx < min(W - H, xhi); lx += blockDim.y)
+        for (int lz = max(H, zlo) + (int)threadIdx.x; lz < min(W - H, zhi); lz += blockDim.x) {
+            const double vx = P1[lx * W + lz], vz = P2[lx * W + lz];
+            const double phi = (sqrt(vx * vx + vz * vz) <= 1.0e-12) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                     : atan2(vz, vx);
+            TPo[(size_t)(gx0 + lx) * nz + (gz0 + lz)].y = phi;
+        }
+}
+
+size_t leg_grad_fused_smem(int radius, int smooth)
+{
+    const int r = radius < 1 ? 1 : radius, W = kGradTile + 2 * (r + 2 * smooth);
+    return (4 * (size_t)W * W + 2 * smooth + 1 + 2 * (2 * r + 1)) * sizeof(double);
+}
+
 int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st)
 {
     if (a.n <= 0) return KCIG_OK;
@@ -364,6 +481,14 @@ int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStrea
     k_leg_interp<<<grd, blk, 0, st>>>(a, out, work);
     KCIG_CUDA(cudaGetLastError());
     if (!a.angle) return KCIG_OK;
+    const size_t fsm = leg_grad_fused_smem(a.radius, a.smooth);
+    if (!a.use_grad && fsm <= 200 * 1024) {
+        KCIG_CUDA(cudaFuncSetAttribute(k_leg_grad_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+        const int tiles = ((a.nz + kGradTile - 1) / kGradTile) * ((a.nx + kGradTile - 1) / kGradTile);
+        k_leg_grad_fused<<<dim3(tiles, a.n), dim3(32, 8), fsm, st>>>(a, out);
+        KCIG_CUDA(cudaGetLastError());
+        return KCIG_OK;
+    }
     if (!a.use_grad) {
         k_leg_fd<<<grd, blk, 0, st>>>(a, out, work);
         KCIG_CUDA(cudaGetLastError());

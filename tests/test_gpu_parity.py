@@ -163,6 +163,28 @@ def test_leg_fields_vs_oracle(golden, is_source, pos):
     assert np.all((gw >= 0) & (gw <= 1))
 
 
+@pytest.mark.parametrize("radius,smooth", [(1, 0), (1, 1), (2, 2), (4, 6), (3, 9), (7, 11), (12, 20)])
+def test_leg_direction_radii_vs_oracle(golden, radius, smooth):
+    # the tiled gradient kernel (halo radius + 2 smooth) and, past its shared
+    # memory limit, the plane-by-plane passes; halos wider than the 41 x 81 grid
+    # check that the windows clamp to the grid and not to the tile
+    kp, geom, axis, op, _ = _cases.case_setup(golden, "base")
+    kp.angle_grad_radius = op.angle_grad_radius = radius
+    kp.angle_smooth = op.angle_smooth = smooth
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    for is_source, pos in ((1, 0.05), (0, 0.6133)):
+        pos = float(np.float32(pos))
+        _, _, gphi, _ = (x.cpu().numpy() for x in kd.leg_fields_device(plan, is_source, pos))
+        _, _, ogx, ogz = oracle.leg_fields(op, is_source, T, D, pos)
+        ok = np.hypot(ogx, ogz) > 1e-12
+        assert np.array_equal(np.isnan(gphi), ~ok)
+        dphi = np.abs(np.angle(np.exp(1j * (gphi[ok] - np.arctan2(ogz, ogx)[ok]))))
+        assert dphi.max() < 1e-9
+    plan.close()
+
+
 def test_cli_end_to_end(golden, o64, tmp_path):
     meta = golden.meta
     t = meta["table"]
