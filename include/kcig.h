@@ -178,6 +178,13 @@ int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, fl
                         int npos, float p0, float dp, float zsrc, int b1, int b2, int iterations,
                         float *time, float *deriv, void *stream);
 
+/* Self-test of the tensor-core operand layouts used by the traveltime
+ * surrogate (no counterpart in the reference, which has no surrogate): for
+ * two 128x128 BF16 row-major device matrices X and W writes, as FP32
+ * [3][128][128], X W^T, X W and X^T W computed by tcgen05 MMAs.  *status
+ * (device int) becomes 1 if the kernel gave up waiting for the tensor core. */
+int kcig_tc_selftest(const void *X, const void *W, float *D, int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

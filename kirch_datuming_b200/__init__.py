@@ -85,6 +85,7 @@ def lib():
         L.kcig_eikonal_tables.argtypes = [fp, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 4 + [
             ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             fp, fp, vp]
+        L.kcig_tc_selftest.argtypes = [vp, vp, fp, vp, vp]
         _lib = L
     return _lib
 
@@ -235,3 +236,20 @@ def eikonal_tables(vel, dz: float, dx: float, npos: int, p0: float, dp: float, z
                                      iterations, t.data_ptr(), d.data_ptr() if deriv else None,
                                      ctypes.c_void_p(st)))
     return t, d
+
+
+def tc_selftest(X, W):
+    """Tensor-core layout self-test: for 128x128 CUDA bfloat16 tensors X, W
+    returns the CUDA float32 tensor [3][128][128] of X W^T, X W and X^T W as
+    computed by the surrogate's tcgen05 operand views."""
+    import torch
+    for t in (X, W):
+        if not (t.is_cuda and t.dtype == torch.bfloat16 and t.shape == (128, 128) and t.is_contiguous()):
+            raise ValueError("X and W must be contiguous 128x128 CUDA bfloat16 tensors")
+    D = torch.empty((3, 128, 128), dtype=torch.float32, device=X.device)
+    status = torch.zeros(1, dtype=torch.int32, device=X.device)
+    st = torch.cuda.current_stream().cuda_stream
+    _check(lib().kcig_tc_selftest(X.data_ptr(), W.data_ptr(), D.data_ptr(), status.data_ptr(), ctypes.c_void_p(st)))
+    if int(status.item()) != 0:
+        raise KcigError(-6, "tensor-core self-test: the MMA did not complete")
+    return D
