@@ -185,6 +185,56 @@ int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, fl
  * (device int) becomes 1 if the kernel gave up waiting for the tensor core. */
 int kcig_tc_selftest(const void *X, const void *W, float *D, int *status, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Learned traveltime surrogate (no counterpart in the reference, which reads
+ * eikods2d tables).  A network T(xs, z, x) = T0 * tau(xs, z, x) with T0 the
+ * straight-ray time |(x, z) - (xs, zsrc)| / vref and tau a 4x128 SiLU MLP on
+ * 64-frequency Fourier features of the normalised inputs, BF16 tensor-core
+ * GEMMs with FP32 accumulation.  Trained on a table volume by the library's
+ * own forward and backward kernels (Adam, loss mean((1000 (T - T_table))^2)
+ * in ms^2); plugged into a plan it replaces the table interpolation and the
+ * finite-difference gradients of every leg. */
+typedef struct kcig_surrogate kcig_surrogate;
+typedef struct {
+    float lo[3], hi[3]; /* domain of (xs, z, x) in km, mapped to [-1, 1]      */
+    float fmax;         /* highest Fourier frequency (half-waves over the domain) */
+    float vref, zsrc;   /* background velocity (km/s) and source depth (km)    */
+} kcig_surrogate_config;
+
+int kcig_surrogate_nparams(void);
+/* Seeded initial parameters on the current device. */
+int kcig_surrogate_create(const kcig_surrogate_config *cfg, unsigned long long seed, kcig_surrogate **out);
+void kcig_surrogate_destroy(kcig_surrogate *s);
+/* Parameters as a host float vector of kcig_surrogate_nparams() entries:
+ * W1 [128][384], W2..W4 [128][128] (row = output), b1..b4 [128], wo [128], bo.
+ * set_params also resets the optimiser state. */
+int kcig_surrogate_set_params(kcig_surrogate *s, const float *params);
+int kcig_surrogate_get_params(const kcig_surrogate *s, float *params);
+/* T and its derivatives at n points (all device float arrays). */
+int kcig_surrogate_eval(kcig_surrogate *s, int n, const float *xs, const float *z, const float *x, float *T,
+                        float *dTdxs, float *dTdz, float *dTdx, void *stream);
+/* Diagnostics of the tensor-core evaluation: the FP32 accumulators of the
+ * first 128-point tile as device float [5][128][128] (row = point): layer 4
+ * before its bias, then d tau/d h_3, d tau/d h_2, d tau/d h_1 before the
+ * activation derivative, and d tau/d f of the xs features. */
+int kcig_surrogate_eval_stages(kcig_surrogate *s, int n, const float *xs, const float *z, const float *x,
+                               float *stages, void *stream);
+/* Loss of one batch (device float *loss) and its gradient with respect to
+ * the parameters (device float grad[nparams]); no update. */
+int kcig_surrogate_loss_grad(kcig_surrogate *s, int n, const float *xs, const float *z, const float *x,
+                             const float *Ttrue, float *loss, float *grad, void *stream);
+/* `steps` Adam steps on batches of `batch` (multiple of 128) points drawn
+ * uniformly from the device table volume [npos][nx][nz] (positions
+ * p0 + k*dp), learning rate decaying from lr to lr_final (cosine).  losses:
+ * host float[steps] or NULL. */
+int kcig_surrogate_train(kcig_surrogate *s, const float *table, int npos, float p0, float dp, int nz, int nx,
+                         float z0, float dz, float x0, float dx, int steps, int batch, float lr, float lr_final,
+                         unsigned long long seed, float *losses, void *stream);
+/* Leg fields of the plan's source (src) and receiver (rcv) legs from
+ * surrogates instead of tables (either may be NULL: that side uses its
+ * tables).  The surrogates must outlive the plan's migrations. */
+int kcig_plan_set_surrogate(kcig_plan *plan, kcig_surrogate *src, kcig_surrogate *rcv);
+
 #ifdef __cplusplus
 }
 #endif

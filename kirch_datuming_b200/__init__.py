@@ -32,6 +32,11 @@ class KcigError(RuntimeError):
         self.msg = msg
 
 
+class SurrogateConfig(ctypes.Structure):
+    _fields_ = [("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("fmax", ctypes.c_float),
+                ("vref", ctypes.c_float), ("zsrc", ctypes.c_float)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "adj", "cig", "cig_is_angle", "cmp", "half_angle", "isdiff", "interp_type", "angle_interp",
@@ -86,6 +91,20 @@ def lib():
             ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             fp, fp, vp]
         L.kcig_tc_selftest.argtypes = [vp, vp, fp, vp, vp]
+        SC = ctypes.POINTER(SurrogateConfig)
+        L.kcig_surrogate_create.argtypes = [SC, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+        L.kcig_surrogate_destroy.argtypes = [vp]
+        L.kcig_surrogate_destroy.restype = None
+        L.kcig_surrogate_set_params.argtypes = [vp, fp]
+        L.kcig_surrogate_get_params.argtypes = [vp, fp]
+        L.kcig_surrogate_eval.argtypes = [vp, ctypes.c_int] + [fp] * 7 + [vp]
+        L.kcig_surrogate_eval_stages.argtypes = [vp, ctypes.c_int] + [fp] * 4 + [vp]
+        L.kcig_surrogate_loss_grad.argtypes = [vp, ctypes.c_int] + [fp] * 6 + [vp]
+        L.kcig_surrogate_train.argtypes = ([vp, fp, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                            ctypes.c_int] + [ctypes.c_float] * 4 +
+                                           [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                            ctypes.c_ulonglong, fp, vp])
+        L.kcig_plan_set_surrogate.argtypes = [vp, vp, vp]
         _lib = L
     return _lib
 
@@ -161,6 +180,12 @@ class Plan:
         ptrs = [_ptr(x) for x in (sgradx, sgradz, rgradx, rgradz)]
         self._keep += [sgradx, sgradz, rgradx, rgradz]
         _check(lib().kcig_plan_set_gradients(self._h, *[p for p, _ in ptrs], ptrs[0][1]))
+
+    def set_surrogate(self, src=None, rcv=None):
+        """Leg fields of the source / receiver legs from Surrogate objects
+        instead of the tables (None: that side uses its tables)."""
+        self._keep += [src, rcv]
+        _check(lib().kcig_plan_set_surrogate(self._h, src.handle if src else None, rcv.handle if rcv else None))
 
     def migrate(self, data, image):
         (dp_, m1), (ip, m2) = _ptr(data), _ptr(image)
@@ -253,3 +278,109 @@ def tc_selftest(X, W):
     if int(status.item()) != 0:
         raise KcigError(-6, "tensor-core self-test: the MMA did not complete")
     return D
+
+
+class Surrogate:
+    """Learned traveltime surrogate T(xs, z, x) = T0 * tau (include/kcig.h,
+    kcig_surrogate_*): trained and evaluated by the library's tensor-core
+    kernels on the current CUDA device.  lo/hi: domain of (xs, z, x) in km."""
+
+    def __init__(self, lo, hi, fmax: float = 8.0, vref: float = 1.5, zsrc: float = 0.0, seed: int = 0):
+        c = SurrogateConfig()
+        for i in range(3):
+            c.lo[i], c.hi[i] = float(lo[i]), float(hi[i])
+        c.fmax, c.vref, c.zsrc = float(fmax), float(vref), float(zsrc)
+        self.config = c
+        h = ctypes.c_void_p()
+        _check(lib().kcig_surrogate_create(ctypes.byref(c), int(seed), ctypes.byref(h)))
+        self._h = h
+        self.nparams = int(lib().kcig_surrogate_nparams())
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_params(self):
+        import numpy as np
+        p = np.empty(self.nparams, np.float32)
+        _check(lib().kcig_surrogate_get_params(self._h, p.ctypes.data))
+        return p
+
+    def set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.nparams:
+            raise ValueError("expected %d parameters" % self.nparams)
+        _check(lib().kcig_surrogate_set_params(self._h, p.ctypes.data))
+
+    @staticmethod
+    def _dev(a, n=None):
+        import torch
+        t = torch.as_tensor(a, dtype=torch.float32).cuda().contiguous()
+        if n is not None and t.numel() != n:
+            raise ValueError("length mismatch")
+        return t
+
+    def eval(self, xs, z, x):
+        """(T, dT/dxs, dT/dz, dT/dx) at the points, as CUDA float32 tensors."""
+        import torch
+        xs = self._dev(xs)
+        n = xs.numel()
+        z, x = self._dev(z, n), self._dev(x, n)
+        out = [torch.empty(n, dtype=torch.float32, device=xs.device) for _ in range(4)]
+        st = torch.cuda.current_stream().cuda_stream
+        _check(lib().kcig_surrogate_eval(self._h, n, xs.data_ptr(), z.data_ptr(), x.data_ptr(),
+                                         *[o.data_ptr() for o in out], ctypes.c_void_p(st)))
+        return tuple(out)
+
+    def eval_stages(self, xs, z, x):
+        """FP32 accumulators of the first 128-point tile, [5][128][128]
+        (kcig_surrogate_eval_stages)."""
+        import torch
+        xs = self._dev(xs)
+        n = xs.numel()
+        z, x = self._dev(z, n), self._dev(x, n)
+        out = torch.zeros((8, 128, 128), dtype=torch.float32, device=xs.device)
+        st = torch.cuda.current_stream().cuda_stream
+        _check(lib().kcig_surrogate_eval_stages(self._h, n, xs.data_ptr(), z.data_ptr(), x.data_ptr(),
+                                                out.data_ptr(), ctypes.c_void_p(st)))
+        return out
+
+    def loss_grad(self, xs, z, x, Ttrue):
+        """Loss of the batch (ms^2) and its parameter gradient (CUDA tensor)."""
+        import torch
+        xs = self._dev(xs)
+        n = xs.numel()
+        z, x, Tt = self._dev(z, n), self._dev(x, n), self._dev(Ttrue, n)
+        loss = torch.empty(1, dtype=torch.float32, device=xs.device)
+        grad = torch.empty(self.nparams, dtype=torch.float32, device=xs.device)
+        st = torch.cuda.current_stream().cuda_stream
+        _check(lib().kcig_surrogate_loss_grad(self._h, n, xs.data_ptr(), z.data_ptr(), x.data_ptr(), Tt.data_ptr(),
+                                              loss.data_ptr(), grad.data_ptr(), ctypes.c_void_p(st)))
+        return float(loss.item()), grad
+
+    def train(self, table, p0: float, dp: float, z0: float, dz: float, x0: float, dx: float, steps: int,
+              batch: int = 16384, lr: float = 2e-3, lr_final: float = 2e-5, seed: int = 1):
+        """Adam on uniform samples of a CUDA table volume [npos][nx][nz];
+        returns the per-step losses (ms^2) as a numpy array."""
+        import numpy as np
+        import torch
+        if not (table.is_cuda and table.dtype == torch.float32 and table.is_contiguous() and table.dim() == 3):
+            raise ValueError("table must be a contiguous CUDA float32 tensor [npos][nx][nz]")
+        npos, nx, nz = table.shape
+        losses = np.zeros(max(steps, 1), np.float32)
+        st = torch.cuda.current_stream().cuda_stream
+        _check(lib().kcig_surrogate_train(self._h, table.data_ptr(), npos, p0, dp, nz, nx, z0, dz, x0, dx, steps,
+                                          batch, lr, lr_final, int(seed), losses.ctypes.data, ctypes.c_void_p(st)))
+        return losses[:steps]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().kcig_surrogate_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

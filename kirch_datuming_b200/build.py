@@ -21,7 +21,7 @@ LIB = os.path.join(PKG, "libkcig.so")
 CLI = os.path.join(PKG, "bin", "kirchmig2d_cig")
 
 SOURCES = ["kcig_kernels.cu", "kcig_plan.cu", "kcig_eikonal.cu", "kcig_mlp.cu", "kcig_params.cpp", "kcig_rsf.cpp", "kcig_cli.cpp"]
-HEADERS = ["kcig_common.h", "kcig_tc.h", "kcig_par.h", "kcig_rsf.h"]
+HEADERS = ["kcig_common.h", "kcig_tc.h", "kcig_aperture.h", "kcig_par.h", "kcig_rsf.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

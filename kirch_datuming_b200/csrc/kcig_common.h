@@ -66,6 +66,14 @@ struct FieldArgs {
 // Workspace for the gradient pipeline: 4 double planes per position.
 int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st);
 
+// Leg fields from a traveltime surrogate (kcig_mlp.cu): one launch for all
+// `nlegs` legs (only .pos and .scale of each are read).  The surrogate's
+// status flag is cleared by sg_reset_status and read by sg_check_status.
+int launch_surrogate_fields(kcig_surrogate *s, const LegInterp *legs, int nlegs, const kcig_geometry &g,
+                            const kcig_params &p, LegFields out, cudaStream_t st);
+int sg_reset_status(kcig_surrogate *s, cudaStream_t st);
+int sg_check_status(kcig_surrogate *s, cudaStream_t st);
+
 struct PreludeArgs {
     const float *data;      // [ns][nh][nt] whole data cube on the device
     double2 *D;             // [ntr][nt] {D[i], D[i+1]}, ntr = nshots * nhc

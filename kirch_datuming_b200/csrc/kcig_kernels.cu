@@ -16,6 +16,7 @@
 #include <math.h>
 #include <stdio.h>
 
+#include "kcig_aperture.h"
 #include "kcig_common.h"
 
 namespace kcig {
@@ -187,33 +188,6 @@ int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdi
 }
 
 // ============================================================ K2 leg fields ==
-// kirchmig2d_cig.cpp:226-269: raised-cosine aperture legs, max-combined with
-// the shallow floor disk.  Evaluated once per (position, image point) instead
-// of once per pair: the value depends only on this leg.
-__device__ double leg_cone(double leg, double aper, double band)
-{
-    if (!isfinite(leg)) return 0.0;
-    if (band <= 0.0) return (leg <= aper) ? 1.0 : 0.0;
-    const double inner = aper - band;
-    if (leg <= inner) return 1.0;
-    if (leg >= aper) return 0.0;
-    return 0.5 * (1.0 + cos(kPi * ((leg - inner) / band)));
-}
-
-__device__ double leg_floor(double d, double rmin, double rt)
-{
-    if (rmin <= 0.0) return 0.0;
-    if (rt <= 0.0) return (d <= rmin) ? 1.0 : 0.0;
-    const double inner = rmin - rt;
-    if (inner <= 0.0) {
-        if (d >= rmin) return 0.0;
-        return 0.5 * (1.0 + cos(kPi * (d / rmin)));
-    }
-    if (d <= inner) return 1.0;
-    if (d >= rmin) return 0.0;
-    return 0.5 * (1.0 + cos(kPi * ((d - inner) / rt)));
-}
-
 // Table interpolation (tinterpsr.cpp:37-188) in double, aperture weight, and
 // the input-gradient interpolation (kirchmig2d_cig.cpp:294-322).
 __global__ void k_leg_interp(FieldArgs a, LegFields out, double *work)
@@ -268,12 +242,7 @@ __global__ void k_leg_interp(FieldArgs a, LegFields out, double *work)
         Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
     }
     const int iz = i % a.nz, ix = i / a.nz;
-    const double dz = a.dz;
-    const double zdist = fmax(fabs((double)iz * dz), fmax(1.0e-12, 1.0e-6 * fabs(dz)));
-    const double ximg = (double)a.x0 + (double)ix * (double)a.dx;
-    const double d = fabs(L.pos - ximg);
-    const double legdeg = atan(d / zdist) * 180.0 / kPi;
-    const double w = fmax(leg_cone(legdeg, a.aper, a.aper_taper), leg_floor(d, a.rmin, a.rtaper));
+    const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin, a.rtaper);
     out.TP[base + i] = make_double2(T, 0.0);
     // reference: stablex[i]*ds, an FP32 product of the FP32 table derivative
     out.XW[base + i] = make_float2((float)Tx * L.scale, (float)w);

@@ -59,6 +59,7 @@ struct kcig_plan {
     DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
     int sum_launches = 0, all_launches = 0;
     float sum_ms = 0.f;
+    kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
 };
 
 namespace {
@@ -157,6 +158,16 @@ int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &le
     const kcig_geometry &g = P->g;
     const size_t nzx = (size_t)g.nz * g.nx;
     const int angle = P->p.cig && P->p.cig_is_angle;
+    if (kcig_surrogate *sgt = is_source ? P->sg_src : P->sg_rcv) {
+        KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
+        if (legs.empty()) return KCIG_OK;
+        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
+                                  P->st));
+        KCIG_TRY(launch_surrogate_fields(sgt, P->d_legs.as<LegInterp>(), (int)legs.size(), g, P->p,
+                                         LegFields{TP, XW}, P->st));
+        P->all_launches += 1;
+        return KCIG_OK;
+    }
     const int FB = std::max(1, std::min<int>((int)legs.size(), (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
     if (angle) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
     KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
@@ -315,7 +326,8 @@ extern "C" int kcig_plan_last_stats(const kcig_plan *P, int *sum_launches, float
 extern "C" int kcig_leg_fields_device(kcig_plan *P, int is_source, double pos, double *T, float *Tx, double *phi,
                                       float *w)
 {
-    if (!P || !P->stab) return set_error(KCIG_ERR_ARG, "kcig_leg_fields_device: plan without tables");
+    if (!P || !(is_source ? (P->sg_src || P->stab) : (P->sg_rcv || P->rtab)))
+        return set_error(KCIG_ERR_ARG, "kcig_leg_fields_device: plan without tables");
     const size_t nzx = (size_t)P->g.nz * P->g.nx;
     std::vector<LegInterp> legs(1);
     leg_interp(P, is_source, (float)pos, pos, &legs[0]);
@@ -323,7 +335,10 @@ extern "C" int kcig_leg_fields_device(kcig_plan *P, int is_source, double pos, d
     DevBuf tp, xw;
     int rc = tp.ensure(nzx * sizeof(double2));
     if (!rc) rc = xw.ensure(nzx * sizeof(float2));
+    kcig_surrogate *sgt = is_source ? P->sg_src : P->sg_rcv;
+    if (!rc && sgt) rc = sg_reset_status(sgt, P->st);
     if (!rc) rc = compute_fields(P, is_source, legs, tp.as<double2>(), xw.as<float2>());
+    if (!rc && sgt) rc = sg_check_status(sgt, P->st);
     // unpack {T, phi} and {Tx, w} into the caller's planes
     struct Cp { void *dst; const char *src; size_t el, pitch; } cps[4] = {
         {T, tp.as<char>(), sizeof(double), sizeof(double2)},
@@ -352,7 +367,10 @@ extern "C" int kcig_doubint_device(const float *in, double *out, int ntr, int nt
 extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int memory)
 {
     if (!P || !data || !image) return set_error(KCIG_ERR_ARG, "kcig_migrate: null argument");
-    if (!P->stab) return set_error(KCIG_ERR_ARG, "kcig_migrate: tables not set");
+    if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab))
+        return set_error(KCIG_ERR_ARG, "kcig_migrate: tables not set");
+    for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
+        if (s) KCIG_TRY(sg_reset_status(s, P->st));
     const kcig_params &p = P->p;
     const kcig_geometry &g = P->g;
     const size_t nzx = (size_t)g.nz * g.nx;
@@ -626,7 +644,17 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
         cudaEventDestroy(evs[i]);
         cudaEventDestroy(evs[i + 1]);
     }
+    for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
+        if (s && rc == KCIG_OK) rc = sg_check_status(s, st);
     return rc;
+}
+
+extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_surrogate *rcv)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_surrogate: null plan");
+    P->sg_src = src;
+    P->sg_rcv = rcv;
+    return KCIG_OK;
 }
 
 // ------------------------------------------------- allocation-free variant --

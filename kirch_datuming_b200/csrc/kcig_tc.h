@@ -64,7 +64,8 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
 // all tcgen05 operations issued so far by this thread arrive on `bar` when done
@@ -86,6 +87,8 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 }
 
 // waits for the phase with parity `parity` to complete; false if it gave up
+// (each try suspends the thread for up to a hardware time limit, so the
+// bound is generous in time but finite)
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
     const uint32_t a = smem_u32(bar);
@@ -93,14 +96,42 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(a), "r"(parity)
+            : "r"(a), "r"(parity), "r"(0x989680u)
             : "memory");
         if (done) return true;
     }
     return false;
+}
+
+// non-blocking probe: has the phase with parity `parity` completed?
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// one lane of a converged warp (elect.sync): the issuer of MMAs and commits
+__device__ __forceinline__ bool elect_one()
+{
+    uint32_t pred = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t.reg .b32 r;\n\t"
+        "elect.sync r|p, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(pred)
+        :
+        : "memory");
+    return pred != 0;
 }
 
 // TMEM allocation by one whole warp; the base address is written to *slot
@@ -121,6 +152,7 @@ __device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols)
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 {
     uint32_t r[32];
+    __syncwarp();  // the load is warp-collective (.sync.aligned)
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
@@ -128,11 +160,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
+        : "r"(taddr)
+        : "memory");
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
+
+// Ordering contract used by the kernels: the MMAs of one step and the commit
+// that tracks them are issued by one elected lane of a converged warp 0, in
+// one block (every tcgen05 asm carries a memory clobber, so the commit cannot
+// move above the MMAs it must track); all threads then wait on the mbarrier,
+// fence::after_thread_sync, and only then read TMEM, warp by warp.
 
 // one GEMM D[M=128][N] (+)= sum over K of A x B^T, K a multiple of 16, issued
 // by the calling (single) thread; a/b are the tiles' shared addresses at K=0
