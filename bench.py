@@ -239,6 +239,102 @@ def cpu_sample(threads: int, tables=None):
 
 
 # -------------------------------------------------------------------- main ---
+# ------------------------------------------------------- surrogate section ---
+SG_FLOPS_EVAL = 2 * 128 * (256 + 3 * 128 + 3 * 128 + 256)  # tensor FLOPs per (leg, point) in k_sg_fields
+SG_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m, 64 shots x 201 receivers (cmp=0, 10 m), nt=1001 dt=2ms, 61 angle bins, "
+               "3 flat reflectors, 20 Hz; network trained on the 401-position GPU eikonal tables")
+
+
+def surrogate_section(train_steps: int, steps: int, warmup: int):
+    """Table path vs learned-surrogate path on the same config-1 gathers:
+    throughput of each (device time per migration), the surrogate's training
+    time and traveltime error on the tables, and the image error of the
+    surrogate path (and of the straight-ray background alone, the method
+    without the network) against the table path."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import synth
+    vel, T1, D1, data1, g = synth.config1_workload(seed=4)
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    geom = kd.geometry(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds),
+                       nz=g.nz, nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0,
+                       sdy=f(g.dp), rny=g.npos, ry0=0.0, rdy=f(g.dp))
+    kp = kd.params(*TOKENS)
+    pairs = g.nz * g.nx * g.ns * g.nh
+    st = torch.cuda.current_stream()
+
+    def run(src=None, rcv=None):
+        plan = kd.Plan(kp, geom, stream=st.cuda_stream)
+        plan.set_tables(T1, D1, T1, D1)
+        if src is not None:
+            plan.set_surrogate(src, rcv)
+        img = torch.zeros((plan.ng, g.nx, g.nz), dtype=torch.float32, device="cuda")
+        for _ in range(warmup):
+            plan.migrate(data1, img)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fields, summ = [], []
+        e0.record(st)
+        for _ in range(steps):
+            plan.migrate(data1, img)
+            t = plan.timing()
+            fields.append(t["fields_ms"])
+            summ.append(t["sum_ms"])
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        plan.close()
+        return img.cpu().double().numpy(), ms, statistics.median(fields), statistics.median(summ)
+
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    img_t, ms_t, fl_t, sm_t = run()
+    net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, train_steps, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    n = 200000
+    ip, iz, ix = rng.integers(0, g.npos, n), rng.integers(0, g.nz, n), rng.integers(0, g.nx, n)
+    Tt = T1[torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), torch.from_numpy(iz).cuda()].cpu().numpy()
+    Tg = net.eval((ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32),
+                  (ix * g.dx).astype(np.float32))[0].cpu().numpy()
+    err_ms = 1000.0 * np.abs(Tg - Tt)
+    img_s, ms_s, fl_s, sm_s = run(net, net)
+    background = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    p = background.get_params()
+    p[-129:] = 0.0  # output weights and bias: tau = 1, T = straight-ray time
+    background.set_params(p)
+    img_b, _, _, _ = run(background, background)
+    evals = (g.ns + g.nh) * g.nz * g.nx  # legs x points per migration
+    achieved = evals * SG_FLOPS_EVAL / (fl_s / 1e3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak, peak_src = float(json.load(fh)["bf16_tflops"]), "of measured"
+    except Exception:
+        peak, peak_src = 1590.0, "of fallback"
+    net.close()
+    background.close()
+    return {
+        "workload": SG_WORKLOAD, "pairs_per_step": pairs,
+        "table_path": {"value": pairs / (ms_t / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_t,
+                       "fields_ms": fl_t, "k_sum_ms": sm_t},
+        "surrogate_path": {"value": pairs / (ms_s / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_s,
+                           "fields_ms": fl_s, "k_sum_ms": sm_s},
+        "image_rel_l2_vs_table_path": rel(img_s, img_t),
+        "image_rel_l2_background_only_vs_table_path": rel(img_b, img_t),
+        "meets_rel_l2_1e-3": rel(img_s, img_t) <= 1e-3,
+        "training": {"steps": train_steps, "batch": 16384, "seconds": train_s,
+                     "samples_per_s": train_steps * 16384 / train_s, "final_loss_ms2": float(np.mean(losses[-50:])),
+                     "traveltime_err_ms": {"rms": float(np.sqrt(np.mean(err_ms ** 2))),
+                                           "p99": float(np.percentile(err_ms, 99)), "max": float(err_ms.max())}},
+        "roofline": {"bound": "tensor", "kernel": "k_sg_fields", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src,
+                     "flops_per_eval": SG_FLOPS_EVAL, "evals_per_step": evals},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,6 +343,8 @@ def main():
     ap.add_argument("--impl", default="kcig", choices=["kcig", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--surrogate-steps", type=int, default=40000,
+                    help="training steps of the traveltime surrogate (0: skip the surrogate section)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES),
                     help="small: 64 shots x 64 receivers every 240 m on the same grid (ncu captures)")
     args = ap.parse_args()
@@ -380,6 +478,8 @@ def main():
             line["cpu_baseline"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()))
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(e)[:300]}
+    if dist is None and args.surrogate_steps > 0:
+        line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -230,6 +230,10 @@ int kcig_surrogate_loss_grad(kcig_surrogate *s, int n, const float *xs, const fl
 int kcig_surrogate_train(kcig_surrogate *s, const float *table, int npos, float p0, float dp, int nz, int nx,
                          float z0, float dz, float x0, float dx, int steps, int batch, float lr, float lr_final,
                          unsigned long long seed, float *losses, void *stream);
+/* Device time of the last kcig_migrate spent in leg-field computation (tables
+ * or surrogate) and in the summation kernel, from CUDA events on the plan's
+ * stream (ms). */
+int kcig_plan_last_timing(const kcig_plan *plan, float *fields_ms, float *sum_ms);
 /* Leg fields of the plan's source (src) and receiver (rcv) legs from
  * surrogates instead of tables (either may be NULL: that side uses its
  * tables).  The surrogates must outlive the plan's migrations. */

@@ -105,6 +105,7 @@ def lib():
                                            [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_ulonglong, fp, vp])
         L.kcig_plan_set_surrogate.argtypes = [vp, vp, vp]
+        L.kcig_plan_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         _lib = L
     return _lib
 
@@ -193,6 +194,12 @@ class Plan:
             raise ValueError("data and image must both be host or both be device arrays")
         _check(lib().kcig_migrate(self._h, dp_, ip, m1))
         return image
+
+    def timing(self):
+        """Device ms of the last migration in leg fields and in the summation."""
+        f, m = ctypes.c_float(), ctypes.c_float()
+        _check(lib().kcig_plan_last_timing(self._h, ctypes.byref(f), ctypes.byref(m)))
+        return {"fields_ms": f.value, "sum_ms": m.value}
 
     def stats(self):
         a, b, c = ctypes.c_int(), ctypes.c_float(), ctypes.c_int()

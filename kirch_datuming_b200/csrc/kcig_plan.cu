@@ -58,7 +58,7 @@ struct kcig_plan {
     DevBuf own_stab, own_sder, own_rtab, own_rder, own_sgx, own_sgz, own_rgx, own_rgz;
     DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
     int sum_launches = 0, all_launches = 0;
-    float sum_ms = 0.f;
+    float sum_ms = 0.f, fields_ms = 0.f;
     kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
 };
 
@@ -484,7 +484,19 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     int *d_rfi = (int *)(d_trw + trn);
     int *d_igo = d_rfi + trn;
 
-    std::vector<cudaEvent_t> evs;
+    std::vector<cudaEvent_t> evs, fevs;
+    // leg fields of one batch, bracketed by events (the plan's fields time)
+    auto fields = [&](int is_source, const std::vector<LegInterp> &legs, double2 *TP, float2 *XW) {
+        cudaEvent_t f0, f1;
+        cudaEventCreate(&f0);
+        cudaEventCreate(&f1);
+        fevs.push_back(f0);
+        fevs.push_back(f1);
+        cudaEventRecord(f0, st);
+        const int r = compute_fields(P, is_source, legs, TP, XW);
+        cudaEventRecord(f1, st);
+        return r;
+    };
     bool first = true;
     std::vector<float> h_trw(trn);
     std::vector<int> h_rfi(trn), h_igo(trn);
@@ -499,13 +511,13 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
                 leg_interp(P, 0, hxf[r0 + r], hx[r0 + r], &rl[r]);
                 rl[r].scale = (float)dh;
             }
-            rc = compute_fields(P, 0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+            rc = fields(0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
             if (rc) break;
         }
         for (int s0 = 0; s0 < g.ns && rc == KCIG_OK; s0 += nsb) {
             const int nsh = std::min(nsb, g.ns - s0);
             std::vector<LegInterp> sl(slegs.begin() + s0, slegs.begin() + s0 + nsh);
-            rc = compute_fields(P, 1, sl, P->d_sT.as<double2>(), P->d_sF.as<float2>());
+            rc = fields(1, sl, P->d_sT.as<double2>(), P->d_sF.as<float2>());
             if (rc) break;
             // per-trace arrays of this (shot batch, receiver chunk)
             std::vector<LegInterp> rl;
@@ -534,7 +546,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
                     }
                 }
             if (!shared_r) {
-                rc = compute_fields(P, 0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+                rc = fields(0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
                 if (rc) break;
             }
             const size_t nb = (size_t)nsh * nhb;
@@ -644,9 +656,24 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
         cudaEventDestroy(evs[i]);
         cudaEventDestroy(evs[i + 1]);
     }
+    P->fields_ms = 0.f;
+    for (size_t i = 0; i + 1 < fevs.size(); i += 2) {
+        float ms = 0.f;
+        if (rc == KCIG_OK && cudaEventElapsedTime(&ms, fevs[i], fevs[i + 1]) == cudaSuccess) P->fields_ms += ms;
+        cudaEventDestroy(fevs[i]);
+        cudaEventDestroy(fevs[i + 1]);
+    }
     for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
         if (s && rc == KCIG_OK) rc = sg_check_status(s, st);
     return rc;
+}
+
+extern "C" int kcig_plan_last_timing(const kcig_plan *P, float *fields_ms, float *sum_ms)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_last_timing: null plan");
+    if (fields_ms) *fields_ms = P->fields_ms;
+    if (sum_ms) *sum_ms = P->sum_ms;
+    return KCIG_OK;
 }
 
 extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_surrogate *rcv)

@@ -163,3 +163,22 @@ def reflectivities(n: int, seed: int) -> list:
     mag = rng.uniform(0.05, 0.2, size=n)
     sign = np.where(rng.random(n) < 0.5, -1.0, 1.0)
     return [float(s * m) for s, m in zip(sign, mag)]
+
+
+def config1_workload(seed: int = 4, device: str = "cuda"):
+    """The CPU-runnable benchmark configuration: v(z) = 1.5 + 0.6 z km/s on a
+    201 x 401 grid of 10 m; flat reflectors at 0.6 / 1.2 / 1.7 km with
+    reflectivity +-U(0.05, 0.2); 64 shots evenly spaced over 0..4 km, 201
+    receivers every 10 m from 1.0 to 3.0 km (cmp=0); nt=1001, dt=2 ms; 20 Hz
+    Ricker; traveltime tables from the GPU eikonal solver at the 401 grid
+    columns.  Returns (vel, tables, deriv, data, geometry)."""
+    import kirch_datuming_b200 as kd
+    nz, nx, dz = 201, 401, 0.01
+    vel = torch.from_numpy(velocity_linear_vz(nz, nx, dz)).to(device)
+    T, D = kd.eikonal_tables(vel, dz, dz, nx, 0.0, dz, iterations=3)
+    g = Geometry(nz=nz, nx=nx, dz=dz, dx=dz, z0=0.0, x0=0.0, ns=64, s0=0.0, ds=4.0 / 63, nh=201, h0=1.0, dh=dz,
+                 cmp=0, nt=1001, dt=0.002, t0=0.0, npos=nx, p0=0.0, dp=dz)
+    amps = reflectivities(3, seed)
+    refl = [(np.full(nx, int(round(zr / dz))), a) for zr, a in zip((0.6, 1.2, 1.7), amps)]
+    data = shot_gathers(T, g, refl, 20.0, seed=seed)
+    return vel, T, D, data, g

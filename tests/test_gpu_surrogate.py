@@ -119,3 +119,105 @@ def test_surrogate_eval_stages_vs_oracle():
             bad.append(nm)
     s.close()
     assert not bad, bad
+
+
+import _cases  # noqa: E402
+
+
+def test_surrogate_leg_fields_match_eval(golden):
+    # the persistent leg-field kernel (resident weights, per-leg xs features)
+    # against the general evaluation kernel at the same points, and the
+    # aperture weight against the table path's
+    kp, geom, axis, op, _ = _cases.case_setup(golden, "base")
+    T, Dt = golden.tables()
+    nz, nx, dz = geom["nz"], geom["nx"], geom["dz"]
+    lo, hi = (0.0, 0.0, 0.0), (0.8, 0.4, 0.8)
+    s = kd.Surrogate(lo, hi, fmax=4.0, vref=1.5, zsrc=0.0, seed=9)
+    p = s.get_params()
+    p[sgo.OFF_WO:sgo.OFF_BO] *= 30.0
+    s.set_params(p)
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, Dt, T, Dt)
+    ref_plan = kd.Plan(kp, kd.geometry(**geom))
+    ref_plan.set_tables(T, Dt, T, Dt)
+    plan.set_surrogate(s, s)
+    zz, xx = np.meshgrid(np.arange(nz) * dz, np.arange(nx) * dz)  # [nx][nz]
+    for is_source, pos in ((1, 0.05), (0, 0.4133), (1, 0.7)):
+        pos = float(np.float32(pos))
+        gT, gTx, gphi, gw = (t.cpu().numpy() for t in kd.leg_fields_device(plan, is_source, pos))
+        eT, exs, ez, ex = (t.cpu().double().numpy().reshape(nx, nz) for t in
+                           s.eval(np.full(nx * nz, pos, np.float32), zz.ravel().astype(np.float32),
+                                  xx.ravel().astype(np.float32)))
+        gT, gTx, gphi, gw = (a.reshape(nx, nz) for a in (gT, gTx, gphi, gw))
+        # the leg kernel folds the xs features into a per-leg bias (an FP32
+        # GEMV) where the evaluation kernel runs them through the MMA: the two
+        # agree except for BF16 rounding flips (tau off by <~1e-2, see above)
+        scale = np.sqrt(np.mean(exs ** 2))
+        T0 = np.maximum(np.hypot(xx - pos, zz) / 1.5, 1e-3)
+        eT0 = np.abs(gT - eT) / T0
+        assert np.median(eT0) < 1e-6 and np.percentile(eT0, 99) < 2e-3 and eT0.max() < 2e-2
+        assert np.median(np.abs(gTx - exs)) < 1e-4 * scale and np.percentile(np.abs(gTx - exs), 99) < 1e-2 * scale
+        # phi is NaN where the gradient vanishes (the source point itself)
+        nan = np.isnan(gphi)
+        assert np.all(np.hypot(ez, ex)[nan] < 1e-6)
+        dphi = np.abs(np.angle(np.exp(1j * (gphi[~nan] - np.arctan2(ez, ex)[~nan]))))
+        assert np.median(dphi) < 1e-5 and np.percentile(dphi, 99) < 1e-2
+        _, _, _, rw = (t.cpu().numpy().reshape(nx, nz) for t in kd.leg_fields_device(ref_plan, is_source, pos))
+        assert np.array_equal(gw, rw)
+    plan.close()
+    ref_plan.close()
+    s.close()
+
+
+def test_surrogate_training_gain_and_migration():
+    # train on the config-1 tables (GPU eikonal, 401 positions), then migrate
+    # the config-1 gathers with the surrogate's leg fields.  What the network
+    # gains over the method without it (the straight-ray background T0 alone):
+    # traveltime error on the tables and image error against the table path.
+    import torch
+    from kirch_datuming_b200 import synth
+    vel, T1, D1, data1, g = synth.config1_workload(seed=4)
+    net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, 6000, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
+    assert np.all(np.isfinite(losses)) and losses[-50:].mean() < 1e-3 * losses[:50].mean()
+    rng = np.random.default_rng(1)
+    n = 50000
+    ip, iz, ix = rng.integers(0, g.npos, n), rng.integers(0, g.nz, n), rng.integers(0, g.nx, n)
+    Tt = T1[torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), torch.from_numpy(iz).cuda()].cpu().numpy()
+    xs, z, x = (ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32), (ix * g.dx).astype(np.float32)
+    Tg = net.eval(xs, z, x)[0].cpu().numpy()
+    rms_net = 1000 * np.sqrt(np.mean((Tg - Tt) ** 2))
+    rms_bg = 1000 * np.sqrt(np.mean((np.hypot(x - xs, z) / 1.5 - Tt) ** 2))
+    print("traveltime rms: network %.3f ms, straight-ray background %.1f ms" % (rms_net, rms_bg))
+    assert rms_net < 0.6 and rms_net < 0.01 * rms_bg
+
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    geom = kd.geometry(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds),
+                       nz=g.nz, nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0,
+                       sdy=f(g.dp), rny=g.npos, ry0=0.0, rdy=f(g.dp))
+    kp = kd.params("cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60", "angle_step=1", "angle_n=61",
+                   "direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05")
+    bg = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    p = bg.get_params()
+    p[sgo.OFF_WO:] = 0.0
+    bg.set_params(p)
+    imgs = []
+    for sur in (None, net, bg):
+        plan = kd.Plan(kp, geom)
+        plan.set_tables(T1, D1, T1, D1)
+        if sur is not None:
+            plan.set_surrogate(sur, sur)
+        img = torch.zeros((plan.ng, g.nx, g.nz), device="cuda")
+        plan.migrate(data1, img)
+        imgs.append(img.cpu().double().numpy())
+        plan.close()
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)  # noqa: E731
+    r_net, r_bg = rel(imgs[1], imgs[0]), rel(imgs[2], imgs[0])
+    print("image relL2 vs table path: network %.3f, background %.3f" % (r_net, r_bg))
+    assert r_net < 0.35 and r_net < 0.5 * r_bg
+    # the reflectors stay where the table path puts them
+    prof = [np.abs(im).sum(axis=(0, 1)) for im in imgs[:2]]
+    for zr in (60, 120, 170):
+        assert abs(int(np.argmax(prof[1][zr - 8:zr + 9])) - int(np.argmax(prof[0][zr - 8:zr + 9]))) <= 1
+    net.close()
+    bg.close()
