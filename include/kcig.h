@@ -186,6 +186,49 @@ int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, fl
 int kcig_tc_selftest(const void *X, const void *W, float *D, int *status, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Shots of uneven receiver count and trace length (the recursive-layer
+ * workflow's windows, run_salt_adcig.sh:131-149, migrate such gathers one
+ * file at a time).  Each shot is migrated as kirchmig2d_cig migrates a
+ * one-shot file (ns = 1, so the source term of the antialias width uses
+ * ds = 0): the image is the sum of those per-shot images.  The plan's
+ * geometry supplies the image grid, the table axes, t0, dt and the largest
+ * nt; its ns/nh/s0/ds/h0/dh are not used here. */
+typedef struct {
+    float sx;           /* source position (km)                                   */
+    int nh;             /* receivers of this shot                                 */
+    float h0, dh;       /* receiver axis h0 + k*dh: offsets (cmp=1) or positions   */
+    int nt;             /* samples per trace of this shot, <= the plan's nt        */
+    const float *data;  /* [nh][nt], host or device as `memory` says               */
+} kcig_shot;
+
+/* Uploads the shots and every per-batch table to the device (batches sized
+ * to the plan's scratch budget; receivers at the same position and spacing
+ * share one leg within a batch). */
+int kcig_shots_prepare(kcig_plan *plan, int nshots, const kcig_shot *shots, int memory);
+/* Migrates the prepared shots into image [ng][nx][nz] (host or device).  The
+ * launch sequence needs no host work; with kcig_plan_set_graph(plan, 1) it
+ * is captured once into a CUDA graph (per image buffer) and replayed. */
+int kcig_migrate_prepared(kcig_plan *plan, float *image, int memory);
+int kcig_migrate_shots(kcig_plan *plan, int nshots, const kcig_shot *shots, float *image, int memory);
+int kcig_plan_set_graph(kcig_plan *plan, int enable);
+/* Image points x traces of the prepared shots (the throughput unit). */
+long long kcig_shots_pairs(const kcig_plan *plan);
+/* Times the summation kernel's tile variants (tile shape, shots per block)
+ * on the first batch of the prepared shots and keeps the fastest for this
+ * plan.  choice: the variant kept; ms: float[5], [0] the kept variant's
+ * time, [1..4] each variant's (either may be NULL). */
+int kcig_plan_autotune(kcig_plan *plan, int *choice, float *ms);
+/* One CUDA graph over several prepared plans (e.g. the five depth windows of
+ * the recursive workflow, each with its own tables, mute and image): create
+ * runs every plan once directly, then captures the same sequence; launch
+ * replays it asynchronously on `stream` (the caller synchronises).  The
+ * plans, their prepared shots and the images must outlive the graph. */
+typedef struct kcig_graph kcig_graph;
+int kcig_graph_create(int nplans, kcig_plan *const *plans, float *const *images, kcig_graph **out);
+int kcig_graph_launch(kcig_graph *graph, void *stream);
+void kcig_graph_destroy(kcig_graph *graph);
+
+/* ---------------------------------------------------------------------------
  * Learned traveltime surrogate (no counterpart in the reference, which reads
  * eikods2d tables).  A network T(xs, z, x) = T0 * tau(xs, z, x) with T0 the
  * straight-ray time |(x, z) - (xs, zsrc)| / vref and tau a 4x128 SiLU MLP on

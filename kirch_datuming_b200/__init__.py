@@ -37,6 +37,11 @@ class SurrogateConfig(ctypes.Structure):
                 ("vref", ctypes.c_float), ("zsrc", ctypes.c_float)]
 
 
+class Shot(ctypes.Structure):
+    _fields_ = [("sx", ctypes.c_float), ("nh", ctypes.c_int), ("h0", ctypes.c_float), ("dh", ctypes.c_float),
+                ("nt", ctypes.c_int), ("data", ctypes.c_void_p)]
+
+
 class Params(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "adj", "cig", "cig_is_angle", "cmp", "half_angle", "isdiff", "interp_type", "angle_interp",
@@ -105,6 +110,17 @@ def lib():
                                            [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_ulonglong, fp, vp])
         L.kcig_plan_set_surrogate.argtypes = [vp, vp, vp]
+        L.kcig_shots_prepare.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Shot), ctypes.c_int]
+        L.kcig_migrate_prepared.argtypes = [vp, fp, ctypes.c_int]
+        L.kcig_migrate_shots.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Shot), fp, ctypes.c_int]
+        L.kcig_plan_set_graph.argtypes = [vp, ctypes.c_int]
+        L.kcig_plan_autotune.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]
+        L.kcig_graph_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]
+        L.kcig_graph_launch.argtypes = [vp, vp]
+        L.kcig_graph_destroy.argtypes = [vp]
+        L.kcig_graph_destroy.restype = None
+        L.kcig_shots_pairs.argtypes = [vp]
+        L.kcig_shots_pairs.restype = ctypes.c_longlong
         L.kcig_plan_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         _lib = L
     return _lib
@@ -187,6 +203,46 @@ class Plan:
         instead of the tables (None: that side uses its tables)."""
         self._keep += [src, rcv]
         _check(lib().kcig_plan_set_surrogate(self._h, src.handle if src else None, rcv.handle if rcv else None))
+
+    def prepare_shots(self, shots):
+        """Upload ragged shots (include/kcig.h kcig_shot): a list of dicts with
+        sx, h0, dh and data [nh][nt] (numpy float32 or CUDA float32 tensor)."""
+        arr = (Shot * max(1, len(shots)))()
+        mems = set()
+        keep = []
+        for i, s in enumerate(shots):
+            d = s["data"]
+            if hasattr(d, "is_cuda"):
+                d = d.contiguous()
+            else:
+                import numpy as np
+                d = np.ascontiguousarray(d, dtype=np.float32)
+            keep.append(d)
+            p, m = _ptr(d)
+            mems.add(m)
+            nh, nt = d.shape
+            arr[i] = Shot(float(s["sx"]), int(nh), float(s.get("h0", 0.0)), float(s.get("dh", 0.0)), int(nt),
+                          ctypes.c_void_p(p))
+        if len(mems) > 1:
+            raise ValueError("shots must all be host or all be device arrays")
+        _check(lib().kcig_shots_prepare(self._h, len(shots), arr, mems.pop() if mems else 0))
+        return int(lib().kcig_shots_pairs(self._h))
+
+    def migrate_prepared(self, image):
+        ip, m = _ptr(image)
+        _check(lib().kcig_migrate_prepared(self._h, ip, m))
+        return image
+
+    def autotune(self):
+        """Pick the summation's tile variant for the prepared shots; returns
+        (variant, {variant: ms})."""
+        c = ctypes.c_int()
+        ms = (ctypes.c_float * 5)()
+        _check(lib().kcig_plan_autotune(self._h, ctypes.byref(c), ms))
+        return c.value, {i: ms[i] for i in range(1, 5)}
+
+    def set_graph(self, enable=True):
+        _check(lib().kcig_plan_set_graph(self._h, 1 if enable else 0))
 
     def migrate(self, data, image):
         (dp_, m1), (ip, m2) = _ptr(data), _ptr(image)
@@ -384,6 +440,35 @@ class Surrogate:
     def close(self):
         if getattr(self, "_h", None):
             lib().kcig_surrogate_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """One CUDA graph over several prepared plans (kcig_graph_*): replaying it
+    migrates every plan's prepared shots into that plan's device image."""
+
+    def __init__(self, plans, images):
+        n = len(plans)
+        ps = (ctypes.c_void_p * n)(*[p._h.value for p in plans])
+        ims = (ctypes.c_void_p * n)(*[_ptr(im)[0] for im in images])
+        self._keep = (list(plans), list(images))
+        self._h = ctypes.c_void_p()
+        _check(lib().kcig_graph_create(n, ps, ims, ctypes.byref(self._h)))
+
+    def launch(self, stream=None):
+        import torch
+        st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+        _check(lib().kcig_graph_launch(self._h, ctypes.c_void_p(st)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().kcig_graph_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -13,6 +13,10 @@ namespace kcig {
 
 // ------------------------------------------------------------------ errors --
 int set_error(int code, const char *fmt, ...);
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device, calling the runtime only when the limit must grow (so a
+// launch sequence under stream capture makes no attribute calls once warm).
+int set_dyn_smem(const void *fn, int bytes);
 int cuda_error(cudaError_t e, const char *what);
 
 #define KCIG_CUDA(call)                                               \
@@ -64,7 +68,7 @@ struct FieldArgs {
 };
 
 // Workspace for the gradient pipeline: 4 double planes per position.
-int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st);
+int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches = nullptr);
 
 // Leg fields from a traveltime surrogate (kcig_mlp.cu): one launch for all
 // `nlegs` legs (only .pos and .scale of each are read).  The surrogate's
@@ -82,6 +86,11 @@ struct PreludeArgs {
     int ntr, nt, isdiff, invert;
     int nh, nhc, shot0, rcv0;  // batch = shots shot0.., receivers rcv0..rcv0+nhc-1
     double t0, dt, slope, intercept, taper;
+    // ragged shots (null for the regular cube): per batch trace, the offset
+    // of its samples in `data` (-1: padding, written as zeros) and its
+    // sample count (<= nt, the row stride of D)
+    const long long *toff;
+    const int *tnt;
 };
 int launch_prelude(const PreludeArgs &a, cudaStream_t st);
 int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdiff, double dt,
@@ -96,6 +105,8 @@ struct SumArgs {
     const float *trw;      // [nsb*nh] trace weight, 0 = skip
     const int *rfi;        // [nsb*nh] receiver field index
     const int *igo;        // [nsb*nh] offset-mode bin
+    const float *stop;     // [nsb] last usable sample (nt_shot - 1) of ragged shots, or null
+    int tile;              // tile variant (kSumTiles), 0 = the default rule
     float *image;          // [ng][nzx]
     int zero_init;
     int nz, nx, nt, nsb, nh, ng;
@@ -111,5 +122,9 @@ struct SumArgs {
     int gchunk0, gchunk1;  // bin range handled by this launch
 };
 int launch_sum(const SumArgs &a, cudaStream_t st, int *launches);
+// Tile variants the summation can be launched with (the autotuner's choices):
+// {TZ, TX, shots per block on the receiver-shared path}.
+constexpr int kSumTiles = 5;
+extern const int kSumTileShape[kSumTiles][3];
 
 }  // namespace kcig

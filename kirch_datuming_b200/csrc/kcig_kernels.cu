@@ -16,6 +16,10 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "kcig_aperture.h"
 #include "kcig_common.h"
 
@@ -108,13 +112,25 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
     double *s = smem_d + (size_t)warp * a.nt;
     const int k = tr / a.nhc, r = tr % a.nhc;
     const float *x = a.data + ((size_t)(a.shot0 + k) * a.nh + (a.rcv0 + r)) * a.nt;
+    int nt = a.nt;
+    if (a.toff) {  // ragged shots: own samples, own length
+        const long long off = a.toff[tr];
+        double2 *out = a.D + (size_t)tr * a.nt;
+        if (off < 0) {
+            for (int i = lane; i < a.nt; i += 32) out[i] = make_double2(0.0, 0.0);
+            return;
+        }
+        x = a.data + off;
+        nt = a.tnt[tr];
+        for (int i = nt + lane; i < a.nt; i += 32) out[i] = make_double2(0.0, 0.0);
+    }
     double boundary = 0.0;
     const bool mute = a.mute_sx != nullptr;
     if (mute) {
         const double off = a.slope * fabs(a.mute_rx[tr] - a.mute_sx[tr]);
         boundary = a.invert ? a.intercept - off : a.intercept + off;
     }
-    for (int i = lane; i < a.nt; i += 32) {
+    for (int i = lane; i < nt; i += 32) {
         double v = (double)x[i];
         if (mute) {
             const double t = a.t0 + (double)i * a.dt;
@@ -126,13 +142,13 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
         s[i] = v;
     }
     __syncwarp();
-    doubint_warp(s, a.nt);
-    if (a.isdiff == 1) diff2_warp(s, a.nt, a.dt);
+    doubint_warp(s, nt);
+    if (a.isdiff == 1) diff2_warp(s, nt, a.dt);
     double2 *out = a.D + (size_t)tr * a.nt;
-    for (int i = lane; i < a.nt; i += 32) {
+    for (int i = lane; i < nt; i += 32) {
         double2 e;
         e.x = s[i];
-        e.y = (i + 1 < a.nt) ? s[i + 1] - s[i] : 0.0;
+        e.y = (i + 1 < nt) ? s[i + 1] - s[i] : 0.0;
         out[i] = e;
     }
 }
@@ -152,6 +168,20 @@ __global__ void __launch_bounds__(64) k_doubint_plain(const float *in, double *o
     for (int i = lane; i < nt; i += 32) out[(size_t)tr * nt + i] = s[i];
 }
 
+int set_dyn_smem(const void *fn, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> done;
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    int &have = done[std::make_pair(dev, fn)];
+    if (bytes <= have) return KCIG_OK;
+    KCIG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    have = bytes;
+    return KCIG_OK;
+}
+
 static int prelude_block(int nt, int *warps)
 {
     const size_t per = (size_t)nt * sizeof(double);
@@ -167,7 +197,7 @@ int launch_prelude(const PreludeArgs &a, cudaStream_t st)
     if (prelude_block(a.nt, &warps))
         return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", a.nt);
     const size_t sm = (size_t)warps * a.nt * sizeof(double);
-    KCIG_CUDA(cudaFuncSetAttribute(k_prelude, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    KCIG_TRY(set_dyn_smem((const void *)k_prelude, (int)sm));
     k_prelude<<<(a.ntr + warps - 1) / warps, 32 * warps, sm, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
@@ -181,7 +211,7 @@ int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdi
     if (prelude_block(nt, &warps))
         return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", nt);
     const size_t sm = (size_t)warps * nt * sizeof(double);
-    KCIG_CUDA(cudaFuncSetAttribute(k_doubint_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    KCIG_TRY(set_dyn_smem((const void *)k_doubint_plain, (int)sm));
     k_doubint_plain<<<(ntr + warps - 1) / warps, 32 * warps, sm, st>>>(in, out, ntr, nt, isdiff, dt);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
@@ -442,24 +472,33 @@ size_t leg_grad_fused_smem(int radius, int smooth)
     return (4 * (size_t)W * W + 2 * smooth + 1 + 2 * (2 * r + 1)) * sizeof(double);
 }
 
-int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st)
+int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
 {
+    int nl = 0;
+    struct Count {
+        int *dst;
+        int &n;
+        ~Count() { if (dst) *dst = n; }
+    } count{launches, nl};
     if (a.n <= 0) return KCIG_OK;
     const int nzx = a.nz * a.nx;
     const dim3 blk(256), grd((nzx + 255) / 256, a.n);
     k_leg_interp<<<grd, blk, 0, st>>>(a, out, work);
+    nl++;
     KCIG_CUDA(cudaGetLastError());
     if (!a.angle) return KCIG_OK;
     const size_t fsm = leg_grad_fused_smem(a.radius, a.smooth);
     if (!a.use_grad && fsm <= 200 * 1024) {
-        KCIG_CUDA(cudaFuncSetAttribute(k_leg_grad_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+        KCIG_TRY(set_dyn_smem((const void *)k_leg_grad_fused, (int)fsm));
         const int tiles = ((a.nz + kGradTile - 1) / kGradTile) * ((a.nx + kGradTile - 1) / kGradTile);
         k_leg_grad_fused<<<dim3(tiles, a.n), dim3(32, 8), fsm, st>>>(a, out);
+        nl++;
         KCIG_CUDA(cudaGetLastError());
         return KCIG_OK;
     }
     if (!a.use_grad) {
         k_leg_fd<<<grd, blk, 0, st>>>(a, out, work);
+        nl++;
         KCIG_CUDA(cudaGetLastError());
     }
     if (a.smooth > 0) {
@@ -469,10 +508,12 @@ int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStrea
         for (int pass = 0; pass < 2; pass++) {
             k_box<<<g3, blk, 0, st>>>(a.nz, a.nx, a.smooth, 0, 0, 2, work);
             k_box<<<g3, blk, 0, st>>>(a.nz, a.nx, a.smooth, 1, 2, 0, work);
+            nl += 2;
         }
         KCIG_CUDA(cudaGetLastError());
     }
     k_leg_pack<<<grd, blk, 0, st>>>(a, out, work);
+    nl++;
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
@@ -547,6 +588,9 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     const double top = (double)(a.nt - 1);
 
     for (int sb = 0; sb < a.nsb; sb += KB) {
+        // last usable sample of this shot's traces: ragged shots (receivers
+        // never shared, one shot per block) carry their own
+        const double topk = (!SHARED_R && a.stop) ? (double)__ldg(a.stop + sb) : top;
         double2 sTP[KB];
         float2 sXW[KB];
 #pragma unroll
@@ -630,7 +674,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 const double sh = fma((double)(fmaxf(fabsf(sXW[k].x), fabsf(rXW.x)) * a.aal), a.inv_dt, 1.0);
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
                 const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
-                if (!(fl0 >= 0.0 && fl0 < top && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < top)) continue;
+                if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
                 const double2 *Dk = a.D + (size_t)trc * a.nt;
                 const double2 q0 = __ldg(Dk + (int)fl0);
                 const double2 qm = __ldg(Dk + (int)flm);
@@ -653,7 +697,7 @@ static int launch_sum_t(const SumArgs &a, int nb, cudaStream_t st)
     constexpr int P = TZ * TX;
     const size_t sm = (size_t)nb * P * sizeof(float);
     auto kern = k_sum<TZ, TX, KB, SR, MODE>;
-    KCIG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    KCIG_TRY(set_dyn_smem((const void *)kern, (int)sm));
     const int tiles = ((a.nz + TZ - 1) / TZ) * ((a.nx + TX - 1) / TX);
     kern<<<tiles, P, sm, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
@@ -688,6 +732,8 @@ static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
 // Shared memory holds [bins][points] FP32 accumulators: TZ x TX-point tiles
 // while a launch's bins fit in 200 KB, 8x8 tiles beyond, and launches of at
 // most 384 bins.
+const int kSumTileShape[kSumTiles][3] = {{0, 0, 0}, {16, 8, 4}, {8, 8, 4}, {8, 16, 4}, {16, 8, 2}};
+
 int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
 {
     const int maxb = 384;
@@ -697,7 +743,12 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
         a.gchunk1 = min(a0.ng, g + maxb);
         const int nb = a.gchunk1 - a.gchunk0;
         int rc;
-        if ((size_t)nb * KCIG_TZ * KCIG_TX * 4 <= 200 * 1024) rc = launch_sum_mode<KCIG_TZ, KCIG_TX, KCIG_KB>(a, nb, st);
+        const bool fits128 = (size_t)nb * 128 * 4 <= 200 * 1024;  // every variant but 8x8 holds 128 points
+        if (a.tile == 1 && fits128) rc = launch_sum_mode<16, 8, 4>(a, nb, st);
+        else if (a.tile == 2) rc = launch_sum_mode<8, 8, 4>(a, nb, st);
+        else if (a.tile == 3 && fits128) rc = launch_sum_mode<8, 16, 4>(a, nb, st);
+        else if (a.tile == 4 && fits128) rc = launch_sum_mode<16, 8, 2>(a, nb, st);
+        else if ((size_t)nb * KCIG_TZ * KCIG_TX * 4 <= 200 * 1024) rc = launch_sum_mode<KCIG_TZ, KCIG_TX, KCIG_KB>(a, nb, st);
         else rc = launch_sum_mode<8, 8, KCIG_KB>(a, nb, st);
         if (rc) return rc;
         if (launches) (*launches)++;

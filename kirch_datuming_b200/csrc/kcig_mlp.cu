@@ -832,7 +832,7 @@ static int launch_sg_fields(const SgNet &net, const LegInterp *legs, int nlegs, 
     a.status = status;
     const long long items = (long long)nlegs * ((g.nz * g.nx + 127) / 128);
     const int grid = (int)std::min<long long>(sms, items);
-    KCIG_CUDA(cudaFuncSetAttribute(k_sg_fields, cudaFuncAttributeMaxDynamicSharedMemorySize, kSgFieldSmem));
+    KCIG_TRY(set_dyn_smem((const void *)k_sg_fields, kSgFieldSmem));
     k_sg_fields<<<grid, 256, kSgFieldSmem, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
@@ -940,10 +940,10 @@ int sg_launch_tile(kcig_surrogate *s, int mode, const float *xs, const float *z,
     a.status = s->status;
     const int tiles = (n + 127) / 128;
     if (mode == SG_TRAIN) {
-        KCIG_CUDA(cudaFuncSetAttribute(k_sg_tile<SG_TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSgTileSmem));
+        KCIG_TRY(set_dyn_smem((const void *)k_sg_tile<SG_TRAIN>, kSgTileSmem));
         k_sg_tile<SG_TRAIN><<<tiles, 256, kSgTileSmem, st>>>(a);
     } else {
-        KCIG_CUDA(cudaFuncSetAttribute(k_sg_tile<SG_EVAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSgTileSmem));
+        KCIG_TRY(set_dyn_smem((const void *)k_sg_tile<SG_EVAL>, kSgTileSmem));
         k_sg_tile<SG_EVAL><<<tiles, 256, kSgTileSmem, st>>>(a);
     }
     KCIG_CUDA(cudaGetLastError());

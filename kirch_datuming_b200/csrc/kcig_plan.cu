@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <vector>
 
@@ -60,7 +61,44 @@ struct kcig_plan {
     int sum_launches = 0, all_launches = 0;
     float sum_ms = 0.f, fields_ms = 0.f;
     kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
+    struct ShotsPrepared *shots = nullptr;                 // ragged shots uploaded by kcig_shots_prepare
+    int use_graph = 0;                                     // replay kcig_migrate_prepared as a CUDA graph
+    int tile = 0;                                          // summation tile variant (kcig_plan_autotune)
+    cudaStream_t own_st = nullptr;                         // capture stream when the plan's is the legacy one
 };
+
+// Ragged shots on the device, batched (kcig_shots_prepare); the launch
+// sequence that migrates them needs no host work, so it can be captured.
+struct ShotBatch {
+    int ns = 0, nhb = 0, nrl = 0;  // shots, padded receivers per shot, receiver legs
+    size_t sleg0 = 0, rleg0 = 0;   // first source / receiver leg in `legs`
+    size_t tr0 = 0, shot0 = 0;     // first padded trace, first shot
+    int unit_tw = 0;
+};
+struct ShotsPrepared {
+    std::vector<ShotBatch> batches;
+    int nshots = 0, ntmax = 0;
+    size_t ntr = 0;
+    long long pairs = 0;
+    DevBuf data, legs, trf, stop;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float *graph_image = nullptr;
+};
+
+static void release_shots(kcig_plan *P)
+{
+    if (!P->shots) return;
+    ShotsPrepared *S = P->shots;
+    if (S->exec) cudaGraphExecDestroy(S->exec);
+    if (S->graph) cudaGraphDestroy(S->graph);
+    S->data.release();
+    S->legs.release();
+    S->trf.release();
+    S->stop.release();
+    delete S;
+    P->shots = nullptr;
+}
 
 namespace {
 
@@ -153,35 +191,35 @@ int leg_interp(const kcig_plan *P, int is_source, float posf, double pos, LegInt
     return ret;
 }
 
-int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &legs, double2 *TP, float2 *XW)
+// Legs per field launch and the FP64 work planes they need (4 per leg).
+int field_batch(const kcig_plan *P, size_t nlegs)
+{
+    const size_t nzx = (size_t)P->g.nz * P->g.nx;
+    return std::max(1, std::min<int>((int)nlegs, (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
+}
+
+// Leg fields of n legs whose LegInterp records are already on the device.
+int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int n, double2 *TP, float2 *XW)
 {
     const kcig_geometry &g = P->g;
     const size_t nzx = (size_t)g.nz * g.nx;
-    const int angle = P->p.cig && P->p.cig_is_angle;
+    if (n <= 0) return KCIG_OK;
     if (kcig_surrogate *sgt = is_source ? P->sg_src : P->sg_rcv) {
-        KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
-        if (legs.empty()) return KCIG_OK;
-        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
-                                  P->st));
-        KCIG_TRY(launch_surrogate_fields(sgt, P->d_legs.as<LegInterp>(), (int)legs.size(), g, P->p,
-                                         LegFields{TP, XW}, P->st));
+        KCIG_TRY(launch_surrogate_fields(sgt, d_legs, n, g, P->p, LegFields{TP, XW}, P->st));
         P->all_launches += 1;
         return KCIG_OK;
     }
-    const int FB = std::max(1, std::min<int>((int)legs.size(), (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
+    const int angle = P->p.cig && P->p.cig_is_angle;
+    const int FB = field_batch(P, (size_t)n);
     if (angle) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
-    KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
-    if (!legs.empty())
-        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
-                                  P->st));
-    for (size_t j0 = 0; j0 < legs.size(); j0 += FB) {
+    for (int j0 = 0; j0 < n; j0 += FB) {
         FieldArgs a;
         a.tab = is_source ? P->stab : P->rtab;
         a.der = is_source ? P->sder : P->rder;
         a.gxv = is_source ? P->sgx : P->rgx;
         a.gzv = is_source ? P->sgz : P->rgz;
-        a.legs = P->d_legs.as<LegInterp>() + j0;
-        a.n = (int)std::min<size_t>(FB, legs.size() - j0);
+        a.legs = d_legs + j0;
+        a.n = std::min(FB, n - j0);
         a.nz = g.nz;
         a.nx = g.nx;
         a.dz = g.dz;
@@ -195,11 +233,21 @@ int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &le
         a.aper_taper = P->p.aperture_taper;
         a.rmin = P->p.aperture_rmin;
         a.rtaper = P->p.aperture_rtaper;
-        LegFields out{TP + j0 * nzx, XW + j0 * nzx};
-        KCIG_TRY(launch_leg_fields(a, out, P->d_work.as<double>(), P->st));
-        P->all_launches += 1 + (angle ? (a.use_grad ? 0 : 1) + (a.smooth > 0 ? 4 : 0) + 1 : 0);
+        LegFields out{TP + (size_t)j0 * nzx, XW + (size_t)j0 * nzx};
+        int nl = 0;
+        KCIG_TRY(launch_leg_fields(a, out, P->d_work.as<double>(), P->st, &nl));
+        P->all_launches += nl;
     }
     return KCIG_OK;
+}
+
+int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &legs, double2 *TP, float2 *XW)
+{
+    KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
+    if (legs.empty()) return KCIG_OK;
+    KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
+                              P->st));
+    return compute_fields_dev(P, is_source, P->d_legs.as<LegInterp>(), (int)legs.size(), TP, XW);
 }
 
 }  // namespace
@@ -251,6 +299,8 @@ extern "C" int kcig_plan_destroy(kcig_plan *P)
                       &P->own_rgx,  &P->own_rgz,  &P->d_data,   &P->d_image,  &P->d_rT,   &P->d_rF,
                       &P->d_sT,     &P->d_sF,   &P->d_work,   &P->d_D,      &P->d_legs, &P->d_tr};
     for (DevBuf *b : bufs) b->release();
+    release_shots(P);
+    if (P->own_st) cudaStreamDestroy(P->own_st);
     delete P;
     return KCIG_OK;
 }
@@ -561,6 +611,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
                 if (rc) break;
             }
             PreludeArgs pa;
+            memset(&pa, 0, sizeof pa);
             pa.data = d_data;
             pa.D = P->d_D.as<double2>();
             pa.mute_sx = p.direct_mute ? d_msx : nullptr;
@@ -603,6 +654,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
             // a uniform flag spares the pair loop a dependent load per pair
             sa.unit_tw = std::all_of(h_trw.begin(), h_trw.begin() + nb, [](float v) { return v == 1.0f; }) ? 1 : 0;
+            sa.tile = P->tile;
             sa.shared_r = shared_r ? 1 : 0;
             sa.half = p.half_angle;
             sa.t0 = g.t0;
@@ -682,6 +734,554 @@ extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_s
     P->sg_src = src;
     P->sg_rcv = rcv;
     return KCIG_OK;
+}
+
+// ------------------------------------------------------------ ragged shots --
+// Each shot is migrated as the reference migrates a one-shot file (ns = 1:
+// the source leg's antialias term uses ds = 0; the receiver leg's uses the
+// shot's own dh, 0 for one receiver), so the image equals the sum of the
+// per-shot runs.  Shots keep their own receiver positions and trace length.
+namespace {
+
+// The trace tables of a prepared batch (views into the per-trace buffer).
+struct TraceViews {
+    const double *msx, *mrx;
+    const long long *toff;
+    const float *trw;
+    const int *rfi, *igo, *tnt;
+};
+
+TraceViews trace_views(const ShotsPrepared *S)
+{
+    const size_t ntr = S->ntr;
+    TraceViews v;
+    v.msx = S->trf.as<double>();
+    v.mrx = v.msx + ntr;
+    v.toff = (const long long *)(v.mrx + ntr);
+    v.trw = (const float *)(v.toff + ntr);
+    v.rfi = (const int *)(v.trw + ntr);
+    v.igo = v.rfi + ntr;
+    v.tnt = v.igo + ntr;
+    return v;
+}
+
+// leg fields and integrated traces of batch b (everything k_sum reads)
+int batch_inputs(kcig_plan *P, size_t b, cudaStream_t st)
+{
+    const ShotsPrepared *S = P->shots;
+    const ShotBatch &B = S->batches[b];
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    const TraceViews v = trace_views(S);
+    const LegInterp *legs = S->legs.as<LegInterp>();
+    cudaStream_t saved = P->st;
+    P->st = st;
+    int rc = compute_fields_dev(P, 1, legs + B.sleg0, B.ns, P->d_sT.as<double2>(), P->d_sF.as<float2>());
+    if (!rc) rc = compute_fields_dev(P, 0, legs + B.rleg0, B.nrl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+    P->st = saved;
+    if (rc) return rc;
+    PreludeArgs pa;
+    memset(&pa, 0, sizeof pa);
+    pa.data = S->data.as<float>();
+    pa.D = P->d_D.as<double2>();
+    pa.mute_sx = p.direct_mute ? v.msx + B.tr0 : nullptr;
+    pa.mute_rx = v.mrx + B.tr0;
+    pa.ntr = B.ns * B.nhb;
+    pa.nt = S->ntmax;
+    pa.isdiff = p.isdiff;
+    pa.invert = p.direct_mute_invert;
+    pa.nh = B.nhb;
+    pa.nhc = B.nhb;
+    pa.t0 = g.t0;
+    pa.dt = g.dt;
+    pa.slope = p.direct_mute_slope;
+    pa.intercept = p.direct_mute_intercept;
+    pa.taper = p.direct_mute_taper;
+    pa.toff = v.toff + B.tr0;
+    pa.tnt = v.tnt + B.tr0;
+    KCIG_TRY(launch_prelude(pa, st));
+    P->all_launches++;
+    return KCIG_OK;
+}
+
+SumArgs batch_sum_args(const kcig_plan *P, size_t b, float *d_img)
+{
+    const ShotsPrepared *S = P->shots;
+    const ShotBatch &B = S->batches[b];
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    const TraceViews v = trace_views(S);
+    const int angle = p.cig && p.cig_is_angle;
+    SumArgs sa;
+    memset(&sa, 0, sizeof sa);
+    sa.STP = P->d_sT.as<double2>();
+    sa.SXW = P->d_sF.as<float2>();
+    sa.RTP = P->d_rT.as<double2>();
+    sa.RXW = P->d_rF.as<float2>();
+    sa.D = P->d_D.as<double2>();
+    sa.trw = v.trw + B.tr0;
+    sa.rfi = v.rfi + B.tr0;
+    sa.igo = v.igo + B.tr0;
+    sa.stop = S->stop.as<float>() + B.shot0;
+    sa.tile = P->tile;
+    sa.image = d_img;
+    sa.zero_init = b == 0 ? 1 : 0;
+    sa.nz = g.nz;
+    sa.nx = g.nx;
+    sa.nt = S->ntmax;
+    sa.nsb = B.ns;
+    sa.nh = B.nhb;
+    sa.ng = P->ng;
+    sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
+    sa.unit_tw = B.unit_tw;
+    sa.shared_r = 0;
+    sa.half = p.half_angle;
+    sa.t0 = g.t0;
+    sa.dt = g.dt;
+    sa.inv_dt = 1.0 / (double)g.dt;
+    sa.tau = p.tau;
+    sa.deg = (p.half_angle ? 90.0 : 180.0) / M_PI;
+    sa.ug0 = P->g0;
+    sa.uinv = 1.0 / (double)P->dg;
+    sa.dtf = g.dt;
+    sa.aal = p.antialias;
+    sa.g0 = P->g0;
+    sa.dg = P->dg;
+    sa.oazmin = p.oazmin;
+    sa.oazmax = p.oazmax;
+    sa.oaztaper = p.oaztaper;
+    sa.ats = p.angle_taper_start;
+    sa.ate = p.angle_taper_end;
+    return sa;
+}
+
+int run_prepared(kcig_plan *P, float *d_img, cudaStream_t st)
+{
+    ShotsPrepared *S = P->shots;
+    for (size_t b = 0; b < S->batches.size(); b++) {
+        KCIG_TRY(batch_inputs(P, b, st));
+        const SumArgs sa = batch_sum_args(P, b, d_img);
+        int nl = 0;
+        KCIG_TRY(launch_sum(sa, st, &nl));
+        P->sum_launches += nl;
+        P->all_launches += nl;
+    }
+    if (S->batches.empty()) {
+        const size_t nzx = (size_t)P->g.nz * P->g.nx;
+        KCIG_CUDA(cudaMemsetAsync(d_img, 0, (size_t)P->ng * nzx * sizeof(float), st));
+    }
+    return KCIG_OK;
+}
+
+}  // namespace
+
+extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *shots, int memory)
+{
+    if (!P || nshots < 0 || (nshots > 0 && !shots)) return set_error(KCIG_ERR_ARG, "kcig_shots_prepare: bad arguments");
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab))
+        return set_error(KCIG_ERR_ARG, "kcig_shots_prepare: tables not set");
+    const size_t nzx = (size_t)g.nz * g.nx;
+    const int angle = p.cig && p.cig_is_angle;
+    int ntmax = 1;
+    size_t nsamp = 0;
+    for (int i = 0; i < nshots; i++) {
+        const kcig_shot &sh = shots[i];
+        if (sh.nh < 1 || sh.nt < 1 || !sh.data || !std::isfinite(sh.sx))
+            return set_error(KCIG_ERR_ARG, "kcig_shots_prepare: shot %d: need nh >= 1, nt >= 1, data", i);
+        if (sh.nt > g.nt) return set_error(KCIG_ERR_ARG, "kcig_shots_prepare: shot %d: nt=%d exceeds the plan's nt=%d", i, sh.nt, g.nt);
+        ntmax = std::max(ntmax, sh.nt);
+        nsamp += (size_t)sh.nh * sh.nt;
+    }
+    release_shots(P);
+    ShotsPrepared *S = new ShotsPrepared();
+    P->shots = S;
+    S->nshots = nshots;
+    S->ntmax = ntmax;
+    cudaStream_t st = P->st;
+
+    // all samples in one device buffer, shot after shot
+    std::vector<size_t> base(nshots);
+    int rc = S->data.ensure(std::max<size_t>(nsamp, 1) * sizeof(float));
+    size_t at = 0;
+    for (int i = 0; i < nshots && rc == KCIG_OK; i++) {
+        base[i] = at;
+        const size_t n = (size_t)shots[i].nh * shots[i].nt;
+        cudaError_t e = cudaMemcpyAsync(S->data.as<float>() + at, shots[i].data, n * sizeof(float),
+                                        memory == KCIG_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(shot data)");
+        at += n;
+    }
+    if (rc) { release_shots(P); return rc; }
+
+    // batches: as many shots as the scratch budget holds, receivers shared
+    // within a batch when position and spacing agree
+    const size_t leg_bytes = nzx * (sizeof(double2) + sizeof(float2));
+    const unsigned long long budget = P->budget;
+    const size_t work_bytes = angle ? (size_t)field_batch(P, 64) * 4 * nzx * 8 : 0;
+    std::vector<LegInterp> hlegs;
+    std::vector<double> h_msx, h_mrx;
+    std::vector<long long> h_toff;
+    std::vector<float> h_trw, h_stop;
+    std::vector<int> h_rfi, h_igo, h_tnt;
+    size_t max_s = 0, max_r = 0, max_d = 0;
+    int i0 = 0;
+    while (i0 < nshots) {
+        // grow the batch
+        std::map<std::tuple<double, float, float>, int> seen;
+        int nhb = 0, i1 = i0;
+        for (; i1 < nshots; i1++) {
+            const kcig_shot &sh = shots[i1];
+            const float dhf = sh.nh == 1 ? 0.0f : sh.dh;
+            std::map<std::tuple<double, float, float>, int> add;
+            for (int k = 0; k < sh.nh; k++) {
+                const double hx = (double)sh.h0 + (double)k * (double)dhf;
+                const float hxf = sh.h0 + (float)k * dhf;
+                const double rpos = p.cmp ? (double)sh.sx + hx : hx;
+                const float rposf = p.cmp ? sh.sx + hxf : hxf;
+                const auto key = std::make_tuple(rpos, rposf, dhf);
+                if (!seen.count(key)) add.emplace(key, 0);
+            }
+            const int ns1 = i1 - i0 + 1, nh1 = std::max(nhb, sh.nh);
+            const size_t need = (size_t)(ns1 + seen.size() + add.size()) * leg_bytes +
+                                (size_t)ns1 * nh1 * ((size_t)ntmax * sizeof(double2) + 48) + work_bytes;
+            if (i1 > i0 && need > budget) break;
+            for (auto &kv : add) seen.emplace(kv.first, 0);
+            nhb = nh1;
+        }
+        ShotBatch B;
+        B.ns = i1 - i0;
+        B.nhb = nhb;
+        B.sleg0 = hlegs.size();
+        B.tr0 = h_trw.size();
+        B.shot0 = h_stop.size();
+        std::vector<int> ist(B.ns);
+        for (int k = 0; k < B.ns; k++) {
+            const kcig_shot &sh = shots[i0 + k];
+            LegInterp L;
+            ist[k] = leg_interp(P, 1, sh.sx, (double)sh.sx, &L);
+            L.scale = 0.0f;  // one-shot file: ds = 0
+            hlegs.push_back(L);
+            h_stop.push_back((float)(sh.nt - 1));
+        }
+        B.rleg0 = hlegs.size();
+        std::map<std::tuple<double, float, float>, int> index;
+        bool unit = true;
+        for (int k = 0; k < B.ns; k++) {
+            const kcig_shot &sh = shots[i0 + k];
+            const float dhf = sh.nh == 1 ? 0.0f : sh.dh;
+            for (int r = 0; r < B.nhb; r++) {
+                if (r >= sh.nh) {  // padding: no samples, weight 0
+                    h_msx.push_back(0.0);
+                    h_mrx.push_back(0.0);
+                    h_toff.push_back(-1);
+                    h_trw.push_back(0.0f);
+                    h_rfi.push_back(0);
+                    h_igo.push_back(0);
+                    h_tnt.push_back(0);
+                    unit = false;
+                    continue;
+                }
+                const double hx = (double)sh.h0 + (double)r * (double)dhf;
+                const float hxf = sh.h0 + (float)r * dhf;
+                const double rpos = p.cmp ? (double)sh.sx + hx : hx;
+                const float rposf = p.cmp ? sh.sx + hxf : hxf;
+                const auto key = std::make_tuple(rpos, rposf, dhf);
+                auto it = index.find(key);
+                if (it == index.end()) {
+                    LegInterp L;
+                    leg_interp(P, 0, rposf, rpos, &L);
+                    L.scale = dhf;
+                    it = index.emplace(key, (int)index.size()).first;
+                    hlegs.push_back(L);
+                }
+                // trace aperture (:1082-1099) and offset bin (:35-41), as the regular path
+                float rf = 0.0f;
+                if (g.rny > 1 && g.rdy != 0.0f) rf = (rposf - g.ry0) / g.rdy;
+                const int iht = (g.rny > 1 && g.rdy != 0.0f) ? (int)floorf(rf) : 0;
+                double w = 1.0;
+                if (p.aperture_trace != -1) {
+                    const double ad = fabs((double)(iht - ist[k]));
+                    if (ad >= (double)p.aperture_trace) w = 0.0;
+                    else if (p.aperture_trace_taper > 0) {
+                        const double tb = std::max(0.0, (double)(p.aperture_trace - p.aperture_trace_taper));
+                        if (ad > tb) {
+                            const double den = (double)p.aperture_trace - tb;
+                            if (den > 0.0) w = 0.5 * (1.0 + cos(M_PI * ((ad - tb) / den)));
+                        }
+                    }
+                }
+                int ig = 0;
+                if (p.cig && !p.cig_is_angle) {
+                    int b = -1;
+                    if (P->ng > 0 && P->dg > 0.0f && std::isfinite(hxf)) {
+                        b = (int)floorf((hxf - P->g0) / P->dg + 0.5f);
+                        if (b < 0 || b >= P->ng) b = -1;
+                    }
+                    if (b < 0) w = 0.0;
+                    ig = b < 0 ? 0 : b;
+                }
+                if (w != 1.0) unit = false;
+                h_msx.push_back((double)sh.sx);
+                h_mrx.push_back(rpos);
+                h_toff.push_back((long long)(base[i0 + k] + (size_t)r * sh.nt));
+                h_trw.push_back((float)w);
+                h_rfi.push_back(it->second);
+                h_igo.push_back(ig);
+                h_tnt.push_back(sh.nt);
+                S->pairs += (long long)nzx;
+            }
+        }
+        B.nrl = (int)index.size();
+        B.unit_tw = unit ? 1 : 0;
+        max_s = std::max<size_t>(max_s, B.ns);
+        max_r = std::max<size_t>(max_r, B.nrl);
+        max_d = std::max<size_t>(max_d, (size_t)B.ns * B.nhb);
+        S->batches.push_back(B);
+        i0 = i1;
+    }
+    const size_t ntr = h_trw.size();
+    S->ntr = ntr;
+    rc = S->legs.ensure(std::max<size_t>(hlegs.size(), 1) * sizeof(LegInterp));
+    if (!rc) rc = S->trf.ensure(std::max<size_t>(ntr, 1) * (3 * 8 + 4 * 4));
+    if (!rc) rc = S->stop.ensure(std::max<size_t>(h_stop.size(), 1) * sizeof(float));
+    if (!rc) rc = P->d_sT.ensure(std::max<size_t>(max_s, 1) * nzx * sizeof(double2));
+    if (!rc) rc = P->d_sF.ensure(std::max<size_t>(max_s, 1) * nzx * sizeof(float2));
+    if (!rc) rc = P->d_rT.ensure(std::max<size_t>(max_r, 1) * nzx * sizeof(double2));
+    if (!rc) rc = P->d_rF.ensure(std::max<size_t>(max_r, 1) * nzx * sizeof(float2));
+    if (!rc) rc = P->d_D.ensure(std::max<size_t>(max_d, 1) * (size_t)ntmax * sizeof(double2));
+    if (!rc && angle && !(P->sg_src && P->sg_rcv))
+        rc = P->d_work.ensure((size_t)field_batch(P, std::max(max_s, max_r)) * 4 * nzx * sizeof(double));
+    struct Cp { void *dst; const void *src; size_t bytes; } cps[] = {
+        {S->legs.p, hlegs.data(), hlegs.size() * sizeof(LegInterp)},
+        {S->trf.as<double>(), h_msx.data(), ntr * 8},
+        {S->trf.as<double>() + ntr, h_mrx.data(), ntr * 8},
+        {S->trf.as<double>() + 2 * ntr, h_toff.data(), ntr * 8},
+        {S->trf.as<char>() + 24 * ntr, h_trw.data(), ntr * 4},
+        {S->trf.as<char>() + 28 * ntr, h_rfi.data(), ntr * 4},
+        {S->trf.as<char>() + 32 * ntr, h_igo.data(), ntr * 4},
+        {S->trf.as<char>() + 36 * ntr, h_tnt.data(), ntr * 4},
+        {S->stop.p, h_stop.data(), h_stop.size() * 4}};
+    for (auto &c : cps) {
+        if (rc || c.bytes == 0) continue;
+        cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(shot tables)");
+    }
+    cudaError_t e = cudaStreamSynchronize(st);  // the host vectors go out of scope
+    if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(shots)");
+    if (rc) release_shots(P);
+    return rc;
+}
+
+extern "C" int kcig_plan_set_graph(kcig_plan *P, int enable)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_graph: null plan");
+    P->use_graph = enable ? 1 : 0;
+    if (P->shots && P->shots->exec) {
+        cudaGraphExecDestroy(P->shots->exec);
+        cudaGraphDestroy(P->shots->graph);
+        P->shots->exec = nullptr;
+        P->shots->graph = nullptr;
+        P->shots->graph_image = nullptr;
+    }
+    return KCIG_OK;
+}
+
+extern "C" int kcig_migrate_prepared(kcig_plan *P, float *image, int memory)
+{
+    if (!P || !image) return set_error(KCIG_ERR_ARG, "kcig_migrate_prepared: null argument");
+    ShotsPrepared *S = P->shots;
+    if (!S) return set_error(KCIG_ERR_ARG, "kcig_migrate_prepared: no shots prepared (kcig_shots_prepare)");
+    const size_t nzx = (size_t)P->g.nz * P->g.nx;
+    const size_t img_bytes = (size_t)P->ng * nzx * sizeof(float);
+    P->sum_launches = 0;
+    P->all_launches = 0;
+    P->sum_ms = 0.f;
+    P->fields_ms = 0.f;
+    for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
+        if (s) KCIG_TRY(sg_reset_status(s, P->st));
+    float *d_img = image;
+    if (memory == KCIG_MEM_HOST) {
+        KCIG_TRY(P->d_image.ensure(img_bytes));
+        d_img = P->d_image.as<float>();
+    }
+    cudaStream_t st = P->st;
+    int rc = KCIG_OK;
+    if (P->use_graph) {
+        if (!st) {  // the legacy stream cannot be captured
+            if (!P->own_st) KCIG_CUDA(cudaStreamCreateWithFlags(&P->own_st, cudaStreamNonBlocking));
+            st = P->own_st;
+            KCIG_CUDA(cudaDeviceSynchronize());  // order against work on the legacy stream
+        }
+        if (S->exec && S->graph_image == d_img) {
+            KCIG_CUDA(cudaGraphLaunch(S->exec, st));
+            P->sum_launches = -1;  // inside the graph
+        } else {
+            // one direct run (it also raises every kernel's shared-memory
+            // limit), then capture the same sequence for the next calls
+            rc = run_prepared(P, d_img, st);
+            if (!rc) {
+                if (S->exec) {
+                    cudaGraphExecDestroy(S->exec);
+                    cudaGraphDestroy(S->graph);
+                    S->exec = nullptr;
+                    S->graph = nullptr;
+                }
+                const int sl = P->sum_launches, al = P->all_launches;
+                cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamBeginCapture");
+                if (!rc) {
+                    const int rc2 = run_prepared(P, d_img, st);
+                    cudaGraph_t gr = nullptr;
+                    e = cudaStreamEndCapture(st, &gr);
+                    if (rc2) rc = rc2;
+                    else if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamEndCapture");
+                    if (!rc) {
+                        e = cudaGraphInstantiate(&S->exec, gr, 0);
+                        if (e != cudaSuccess) {
+                            rc = cuda_error(e, "cudaGraphInstantiate");
+                            cudaGraphDestroy(gr);
+                        } else {
+                            S->graph = gr;
+                            S->graph_image = d_img;
+                        }
+                    } else if (gr) {
+                        cudaGraphDestroy(gr);
+                    }
+                }
+                P->sum_launches = sl;
+                P->all_launches = al;
+            }
+        }
+    } else {
+        rc = run_prepared(P, d_img, st);
+    }
+    if (!rc && memory == KCIG_MEM_HOST) {
+        cudaError_t e = cudaMemcpyAsync(image, d_img, img_bytes, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(image)");
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(prepared)");
+    for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
+        if (s && rc == KCIG_OK) rc = sg_check_status(s, st);
+    return rc;
+}
+
+extern "C" int kcig_plan_autotune(kcig_plan *P, int *choice, float *ms)
+{
+    if (!P || !P->shots || P->shots->batches.empty())
+        return set_error(KCIG_ERR_ARG, "kcig_plan_autotune: no shots prepared (kcig_shots_prepare)");
+    const size_t nzx = (size_t)P->g.nz * P->g.nx;
+    KCIG_TRY(P->d_image.ensure((size_t)P->ng * nzx * sizeof(float)));
+    cudaStream_t st = P->st;
+    KCIG_TRY(batch_inputs(P, 0, st));
+    SumArgs sa = batch_sum_args(P, 0, P->d_image.as<float>());
+    cudaEvent_t e0, e1;
+    KCIG_CUDA(cudaEventCreate(&e0));
+    KCIG_CUDA(cudaEventCreate(&e1));
+    int best = 0, rc = KCIG_OK;
+    float best_ms = 0.f;
+    for (int t = 1; t < kSumTiles && rc == KCIG_OK; t++) {
+        sa.tile = t;
+        rc = launch_sum(sa, st, nullptr);  // warm-up (shared-memory limit, caches)
+        float tms = 0.f;
+        for (int rep = 0; rep < 3 && rc == KCIG_OK; rep++) {
+            cudaEventRecord(e0, st);
+            rc = launch_sum(sa, st, nullptr);
+            cudaEventRecord(e1, st);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaEventSynchronize(autotune)");
+            float x = 0.f;
+            cudaEventElapsedTime(&x, e0, e1);
+            tms = rep == 0 ? x : std::min(tms, x);
+        }
+        if (ms) ms[t] = tms;
+        if (!rc && (best == 0 || tms < best_ms)) {
+            best = t;
+            best_ms = tms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (ms) ms[0] = best_ms;
+    P->tile = best;
+    if (choice) *choice = best;
+    kcig_plan_set_graph(P, P->use_graph);  // a captured graph used the old tile
+    return KCIG_OK;
+}
+
+// Several prepared plans (the depth windows of the recursive workflow) in one
+// CUDA graph: one replay migrates every plan's shots into its image.
+struct kcig_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int kcig_graph_create(int n, kcig_plan *const *plans, float *const *images, kcig_graph **out)
+{
+    if (n < 1 || !plans || !images || !out) return set_error(KCIG_ERR_ARG, "kcig_graph_create: bad arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; i++)
+        if (!plans[i] || !plans[i]->shots || !images[i])
+            return set_error(KCIG_ERR_ARG, "kcig_graph_create: plan %d has no prepared shots or image", i);
+    cudaStream_t st;
+    KCIG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int rc = KCIG_OK;
+    // one direct pass first: kernels' shared-memory limits are raised outside the capture
+    for (int i = 0; i < n && rc == KCIG_OK; i++) rc = run_prepared(plans[i], images[i], st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(graph warm-up)");
+    kcig_graph *G = new kcig_graph();
+    if (!rc) {
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamBeginCapture");
+        if (!rc) {
+            int rc2 = KCIG_OK;
+            for (int i = 0; i < n && rc2 == KCIG_OK; i++) rc2 = run_prepared(plans[i], images[i], st);
+            e = cudaStreamEndCapture(st, &G->graph);
+            if (rc2) rc = rc2;
+            else if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamEndCapture");
+        }
+        if (!rc) {
+            e = cudaGraphInstantiate(&G->exec, G->graph, 0);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaGraphInstantiate");
+        }
+    }
+    cudaStreamDestroy(st);
+    if (rc) {
+        kcig_graph_destroy(G);
+        return rc;
+    }
+    *out = G;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_graph_launch(kcig_graph *G, void *stream)
+{
+    if (!G || !G->exec) return set_error(KCIG_ERR_ARG, "kcig_graph_launch: no graph");
+    KCIG_CUDA(cudaGraphLaunch(G->exec, (cudaStream_t)stream));
+    return KCIG_OK;
+}
+
+extern "C" void kcig_graph_destroy(kcig_graph *G)
+{
+    if (!G) return;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    delete G;
+}
+
+extern "C" int kcig_migrate_shots(kcig_plan *P, int nshots, const kcig_shot *shots, float *image, int memory)
+{
+    KCIG_TRY(kcig_shots_prepare(P, nshots, shots, memory));
+    return kcig_migrate_prepared(P, image, memory);
+}
+
+extern "C" long long kcig_shots_pairs(const kcig_plan *P)
+{
+    return (P && P->shots) ? P->shots->pairs : 0;
 }
 
 // ------------------------------------------------- allocation-free variant --
