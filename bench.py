@@ -335,6 +335,88 @@ def surrogate_section(train_steps: int, steps: int, warmup: int):
     }
 
 
+# --------------------------------------------------------- batched section ---
+BATCH_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m in five 0.4 km depth windows (own tables from the window top, own "
+                  "mute: slopes 50/40/30/20/10 s/km, tapers 0.05-0.10 s); 512 shots over 0-4 km, receivers "
+                  "~U{96..480} every 8 m around the source, nt ~U{1501..4001} at 1 ms; 61 angle bins")
+MUTE_SLOPES = (50.0, 40.0, 30.0, 20.0, 10.0)
+MUTE_TAPERS = (0.05, 0.06, 0.07, 0.08, 0.10)
+
+
+def batched_section(steps: int, warmup: int, seed: int = 21):
+    """The uneven-workload configuration: every depth window is a plan of its
+    own with ragged shots prepared on the device, the summation tile is
+    autotuned per window, and one CUDA graph replays all five windows."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import synth
+    nz_all, nx, dz, nshot, dh, nrg, nt_max = 201, 401, 0.01, 512, 0.008, 501, 4001
+    rng = np.random.default_rng(seed)
+    nh = rng.integers(96, 481, nshot)
+    nts = rng.integers(1501, 4002, nshot)
+    sx = (np.arange(nshot) * (4.0 / (nshot - 1))).astype(np.float32)
+    i0 = np.clip(np.round((sx - nh * dh / 2) / dh).astype(int), 0, nrg - nh)
+    vel = synth.velocity_linear_vz(nz_all, nx, dz)
+    amps = synth.reflectivities(5, seed)
+    rows = [(0, 40), (40, 80), (80, 120), (120, 160), (160, 201)]
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    plans, images, tuned, pairs = [], [], [], 0
+    for w, (r0, r1) in enumerate(rows):
+        nzw = r1 - r0
+        vw = torch.from_numpy(np.ascontiguousarray(vel[:, r0:r1])).cuda()
+        T, D = kd.eikonal_tables(vw, dz, dz, nx, 0.0, dz, iterations=3)
+        g = synth.Geometry(nz=nzw, nx=nx, dz=dz, dx=dz, z0=0.0, x0=0.0, ns=nshot, s0=0.0, ds=4.0 / (nshot - 1),
+                           nh=nrg, h0=0.0, dh=dh, cmp=0, nt=nt_max, dt=0.001, t0=0.0, npos=nx, p0=0.0, dp=dz)
+        cube = synth.shot_gathers(T, g, [(np.full(nx, 20), amps[w])], 20.0, seed=seed + w, noise_on_device=True)
+        grid = (np.arange(nrg) * dh).astype(np.float32)  # receiver stations shared by every shot
+        shots = [dict(sx=float(sx[s]), dh=dh, h=grid[i0[s]:i0[s] + nh[s]],
+                      data=cube[s, i0[s]:i0[s] + nh[s], :nts[s]].contiguous()) for s in range(nshot)]
+        del cube
+        kp = kd.params(*(TOKENS[:7] + ["direct_mute=1", "direct_mute_slope=%g" % MUTE_SLOPES[w],
+                                      "direct_mute_intercept=0", "direct_mute_taper=%g" % MUTE_TAPERS[w]]))
+        geom = kd.geometry(nt=nt_max, nh=1, ns=1, t0=0.0, dt=f(0.001), h0=0.0, dh=f(dh), s0=0.0, ds=0.0, nz=nzw,
+                           nx=nx, z0=0.0, dz=f(dz), x0=0.0, dx=f(dz), sny=nx, sy0=0.0, sdy=f(dz), rny=nx, ry0=0.0,
+                           rdy=f(dz))
+        plan = kd.Plan(kp, geom)
+        plan.set_tables(T, D, T, D)
+        pairs += plan.prepare_shots(shots)
+        del shots
+        choice, ms = plan.autotune()
+        tuned.append({"window": w, "tile": choice, "ms": ms})
+        plans.append(plan)
+        images.append(torch.zeros((plan.ng, nx, nzw), dtype=torch.float32, device="cuda"))
+        torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+
+    def timed(step_fn):
+        for _ in range(warmup):
+            step_fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            step_fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_direct = timed(lambda: [p.migrate_prepared(im) for p, im in zip(plans, images)])
+    stages = [p.timing() for p in plans]  # of the last direct run
+    ref = [im.clone() for im in images]
+    graph = kd.Graph(plans, images)
+    ms_graph = timed(lambda: graph.launch(st.cuda_stream))
+    same = all(torch.equal(a, b) for a, b in zip(images, ref))
+    graph.close()
+    for p in plans:
+        p.close()
+    return {"workload": BATCH_WORKLOAD, "pairs_per_step": pairs,
+            "value": pairs / (ms_graph / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_graph,
+            "direct": {"value": pairs / (ms_direct / 1e3) / 1e9, "ms_per_step": ms_direct,
+                       "stage_ms_per_window": stages},
+            "graph_equals_direct": same, "autotune": tuned,
+            "launch": "one CUDA graph replaying the five window plans (kcig_graph_launch)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,6 +425,9 @@ def main():
     ap.add_argument("--impl", default="kcig", choices=["kcig", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run only the uneven five-window workload and print its object (profiling)")
     ap.add_argument("--surrogate-steps", type=int, default=40000,
                     help="training steps of the traveltime surrogate (0: skip the surrogate section)")
     ap.add_argument("--size", default="full", choices=sorted(SIZES),
@@ -389,6 +474,9 @@ def main():
     import torch
     import kirch_datuming_b200 as kd
     torch.cuda.set_device(local)
+    if args.only_batched:
+        print(json.dumps({"batched": batched_section(args.steps, args.warmup)}), flush=True)
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -480,12 +568,18 @@ def main():
             line["cpu_baseline"] = {"value": None, "error": str(e)[:300]}
     if dist is None and args.surrogate_steps > 0:
         line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup)
+    if dist is None and not args.no_batched:
+        plan.close()
+        del T, D, data, image
+        torch.cuda.empty_cache()
+        line["batched"] = batched_section(args.steps, args.warmup)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
+    if dist is not None or args.no_batched:
+        plan.close()
     return 0
 
 

@@ -199,6 +199,11 @@ typedef struct {
     float h0, dh;       /* receiver axis h0 + k*dh: offsets (cmp=1) or positions   */
     int nt;             /* samples per trace of this shot, <= the plan's nt        */
     const float *data;  /* [nh][nt], host or device as `memory` says               */
+    const float *h;     /* optional host array [nh]: the receiver axis values (in
+                           place of h0 + k*dh), e.g. positions on a survey grid;
+                           receivers with equal values then share one leg.  The
+                           values are used as given (FP32), where h0 + k*dh is
+                           rebuilt in FP64 for the continuous quantities      */
 } kcig_shot;
 
 /* Uploads the shots and every per-batch table to the device (batches sized
@@ -277,6 +282,9 @@ int kcig_surrogate_train(kcig_surrogate *s, const float *table, int npos, float 
  * or surrogate) and in the summation kernel, from CUDA events on the plan's
  * stream (ms). */
 int kcig_plan_last_timing(const kcig_plan *plan, float *fields_ms, float *sum_ms);
+/* Device ms of the trace prelude (mute, integration) in the last uncaptured
+ * kcig_migrate_prepared. */
+float kcig_plan_last_prelude_ms(const kcig_plan *plan);
 /* Leg fields of the plan's source (src) and receiver (rcv) legs from
  * surrogates instead of tables (either may be NULL: that side uses its
  * tables).  The surrogates must outlive the plan's migrations. */

@@ -39,7 +39,7 @@ class SurrogateConfig(ctypes.Structure):
 
 class Shot(ctypes.Structure):
     _fields_ = [("sx", ctypes.c_float), ("nh", ctypes.c_int), ("h0", ctypes.c_float), ("dh", ctypes.c_float),
-                ("nt", ctypes.c_int), ("data", ctypes.c_void_p)]
+                ("nt", ctypes.c_int), ("data", ctypes.c_void_p), ("h", ctypes.c_void_p)]
 
 
 class Params(ctypes.Structure):
@@ -122,6 +122,8 @@ def lib():
         L.kcig_shots_pairs.argtypes = [vp]
         L.kcig_shots_pairs.restype = ctypes.c_longlong
         L.kcig_plan_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
+        L.kcig_plan_last_prelude_ms.argtypes = [vp]
+        L.kcig_plan_last_prelude_ms.restype = ctypes.c_float
         _lib = L
     return _lib
 
@@ -206,7 +208,8 @@ class Plan:
 
     def prepare_shots(self, shots):
         """Upload ragged shots (include/kcig.h kcig_shot): a list of dicts with
-        sx, h0, dh and data [nh][nt] (numpy float32 or CUDA float32 tensor)."""
+        sx, h0, dh (or h: the receiver axis values) and data [nh][nt] (numpy
+        float32 or CUDA float32 tensor)."""
         arr = (Shot * max(1, len(shots)))()
         mems = set()
         keep = []
@@ -221,8 +224,16 @@ class Plan:
             p, m = _ptr(d)
             mems.add(m)
             nh, nt = d.shape
+            hp = None
+            if s.get("h") is not None:
+                import numpy as np
+                hv = np.ascontiguousarray(s["h"], dtype=np.float32)
+                if hv.size != nh:
+                    raise ValueError("shot %d: h has %d values for %d receivers" % (i, hv.size, nh))
+                keep.append(hv)
+                hp = hv.ctypes.data
             arr[i] = Shot(float(s["sx"]), int(nh), float(s.get("h0", 0.0)), float(s.get("dh", 0.0)), int(nt),
-                          ctypes.c_void_p(p))
+                          ctypes.c_void_p(p), ctypes.c_void_p(hp))
         if len(mems) > 1:
             raise ValueError("shots must all be host or all be device arrays")
         _check(lib().kcig_shots_prepare(self._h, len(shots), arr, mems.pop() if mems else 0))
@@ -255,7 +266,7 @@ class Plan:
         """Device ms of the last migration in leg fields and in the summation."""
         f, m = ctypes.c_float(), ctypes.c_float()
         _check(lib().kcig_plan_last_timing(self._h, ctypes.byref(f), ctypes.byref(m)))
-        return {"fields_ms": f.value, "sum_ms": m.value}
+        return {"fields_ms": f.value, "sum_ms": m.value, "prelude_ms": float(lib().kcig_plan_last_prelude_ms(self._h))}
 
     def stats(self):
         a, b, c = ctypes.c_int(), ctypes.c_float(), ctypes.c_int()

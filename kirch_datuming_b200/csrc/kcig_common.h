@@ -106,7 +106,13 @@ struct SumArgs {
     const int *rfi;        // [nsb*nh] receiver field index
     const int *igo;        // [nsb*nh] offset-mode bin
     const float *stop;     // [nsb] last usable sample (nt_shot - 1) of ragged shots, or null
+    const int *snh;        // [nsb] receivers of each ragged shot (<= nh), or null
     int tile;              // tile variant (kSumTiles), 0 = the default rule
+    // the shots of a launch split over `nsplit` CTA rows (grids too small to
+    // fill the GPU): row y sums its share into partial[y][ng][nzx], then a
+    // fixed-order reduction adds the rows into the image.  nsplit 1: direct.
+    int nsplit;
+    float *partial;
     float *image;          // [ng][nzx]
     int zero_init;
     int nz, nx, nt, nsb, nh, ng;
@@ -124,6 +130,9 @@ struct SumArgs {
 int launch_sum(const SumArgs &a, cudaStream_t st, int *launches);
 // Tile variants the summation can be launched with (the autotuner's choices):
 // {TZ, TX, shots per block on the receiver-shared path}.
+// How many shot splits a summation over nsb shots on an nz x nx image needs
+// to give the GPU at least two waves of CTAs (1: none).
+int sum_nsplit(int nz, int nx, int nsb, bool shared_r);
 constexpr int kSumTiles = 5;
 extern const int kSumTileShape[kSumTiles][3];
 

@@ -16,6 +16,7 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -113,16 +114,12 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
     const int k = tr / a.nhc, r = tr % a.nhc;
     const float *x = a.data + ((size_t)(a.shot0 + k) * a.nh + (a.rcv0 + r)) * a.nt;
     int nt = a.nt;
-    if (a.toff) {  // ragged shots: own samples, own length
+    if (a.toff) {  // ragged shots: own samples, own length (k_sum reads no
+                   // padding trace and no sample past a trace's own end)
         const long long off = a.toff[tr];
-        double2 *out = a.D + (size_t)tr * a.nt;
-        if (off < 0) {
-            for (int i = lane; i < a.nt; i += 32) out[i] = make_double2(0.0, 0.0);
-            return;
-        }
+        if (off < 0) return;
         x = a.data + off;
         nt = a.tnt[tr];
-        for (int i = nt + lane; i < a.nt; i += 32) out[i] = make_double2(0.0, 0.0);
     }
     double boundary = 0.0;
     const bool mute = a.mute_sx != nullptr;
@@ -575,9 +572,19 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     const int nzx = a.nz * a.nx;
     const int i = valid ? ix * a.nz + iz : 0;
     const int gc0 = a.gchunk0, nb = a.gchunk1 - a.gchunk0;
+    // this CTA row's share of the shots (whole blocks of KB)
+    int s_lo = 0, s_hi = a.nsb;
+    float *out = a.image;
+    if (a.nsplit > 1) {
+        const int nblk = (a.nsb + KB - 1) / KB;
+        s_lo = (int)((long long)nblk * blockIdx.y / a.nsplit) * KB;
+        s_hi = min(a.nsb, (int)((long long)nblk * (blockIdx.y + 1) / a.nsplit) * KB);
+        out = a.partial + (size_t)blockIdx.y * a.ng * nzx;
+    }
+    const bool fresh = a.zero_init || a.nsplit > 1;
 
     for (int b = 0; b < nb; b++)
-        acc[b * P + tid] = (a.zero_init || !valid) ? 0.0f : a.image[(size_t)(gc0 + b) * nzx + i];
+        acc[b * P + tid] = (fresh || !valid) ? 0.0f : a.image[(size_t)(gc0 + b) * nzx + i];
     if (!valid) return;  // no block-wide synchronisation follows
 
     // cutoff of angle_depth_mute_weight (:200-211) depends only on depth
@@ -587,7 +594,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;  // u = th*uk - ub
     const double top = (double)(a.nt - 1);
 
-    for (int sb = 0; sb < a.nsb; sb += KB) {
+    for (int sb = s_lo; sb < s_hi; sb += KB) {
         // last usable sample of this shot's traces: ragged shots (receivers
         // never shared, one shot per block) carry their own
         const double topk = (!SHARED_R && a.stop) ? (double)__ldg(a.stop + sb) : top;
@@ -595,7 +602,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
         float2 sXW[KB];
 #pragma unroll
         for (int k = 0; k < KB; k++) {
-            if (sb + k < a.nsb) {
+            if (sb + k < s_hi) {
                 sTP[k] = __ldg(a.STP + (size_t)(sb + k) * nzx + i);
                 sXW[k] = __ldg(a.SXW + (size_t)(sb + k) * nzx + i);
             } else {
@@ -603,30 +610,31 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 sXW[k] = make_float2(0.f, 0.f);
             }
         }
+        // receivers of this block: all nh, or (ragged shots, one shot per
+        // block) the shot's own count; their fields are loaded one receiver
+        // ahead of use (through the trace's field index when not shared)
+        const int nr = (!SHARED_R && a.snh) ? __ldg(a.snh + sb) : a.nh;
         double2 nTP = make_double2(0.0, 0.0);
         float2 nXW = make_float2(0.f, 0.f);
-        if (SHARED_R) {
-            nTP = __ldg(a.RTP + i);
-            nXW = __ldg(a.RXW + i);
+        if (nr > 0) {
+            const size_t f0 = SHARED_R ? 0 : (size_t)__ldg(a.rfi + (size_t)sb * a.nh);
+            nTP = __ldg(a.RTP + f0 * nzx + i);
+            nXW = __ldg(a.RXW + f0 * nzx + i);
         }
-        for (int r = 0; r < a.nh; r++) {
+        for (int r = 0; r < nr; r++) {
             double2 rTP = nTP;
             float2 rXW = nXW;
-            if (SHARED_R && r + 1 < a.nh) {  // next receiver, one ahead of use
-                nTP = __ldg(a.RTP + (size_t)(r + 1) * nzx + i);
-                nXW = __ldg(a.RXW + (size_t)(r + 1) * nzx + i);
+            if (r + 1 < nr) {  // next receiver, one ahead of use
+                const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)__ldg(a.rfi + (size_t)sb * a.nh + r + 1);
+                nTP = __ldg(a.RTP + f1 * nzx + i);
+                nXW = __ldg(a.RXW + f1 * nzx + i);
             }
 #pragma unroll
             for (int k = 0; k < KB; k++) {
-                if (sb + k >= a.nsb) break;
+                if (sb + k >= s_hi) break;
                 const int trc = (sb + k) * a.nh + r;
                 const float tw = a.unit_tw ? 1.0f : __ldg(a.trw + trc);
                 if (tw == 0.0f) continue;  // trace removed by aperture_trace / offset bin
-                if (!SHARED_R) {
-                    const int ri = __ldg(a.rfi + trc);
-                    rTP = __ldg(a.RTP + (size_t)ri * nzx + i);
-                    rXW = __ldg(a.RXW + (size_t)ri * nzx + i);
-                }
                 const float apw = sXW[k].y * rXW.y;
                 if (!(apw > 0.0f)) continue;
                 int b0 = 0;
@@ -688,7 +696,17 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
             }
         }
     }
-    for (int b = 0; b < nb; b++) a.image[(size_t)(gc0 + b) * nzx + i] = acc[b * P + tid];
+    for (int b = 0; b < nb; b++) out[(size_t)(gc0 + b) * nzx + i] = acc[b * P + tid];
+}
+
+// image (+)= the split rows' partial images, rows in order (deterministic)
+__global__ void k_sum_reduce(float *image, const float *partial, int nsplit, size_t n, int zero_init)
+{
+    const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float v = zero_init ? 0.0f : image[j];
+    for (int y = 0; y < nsplit; y++) v += partial[(size_t)y * n + j];
+    image[j] = v;
 }
 
 template <int TZ, int TX, int KB, bool SR, int MODE>
@@ -699,7 +717,7 @@ static int launch_sum_t(const SumArgs &a, int nb, cudaStream_t st)
     auto kern = k_sum<TZ, TX, KB, SR, MODE>;
     KCIG_TRY(set_dyn_smem((const void *)kern, (int)sm));
     const int tiles = ((a.nz + TZ - 1) / TZ) * ((a.nx + TX - 1) / TX);
-    kern<<<tiles, P, sm, st>>>(a);
+    kern<<<dim3(tiles, a.nsplit > 1 ? a.nsplit : 1), P, sm, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
@@ -753,7 +771,29 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
         if (rc) return rc;
         if (launches) (*launches)++;
     }
+    if (a0.nsplit > 1) {
+        const size_t n = (size_t)a0.ng * a0.nz * a0.nx;
+        k_sum_reduce<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a0.image, a0.partial, a0.nsplit, n, a0.zero_init);
+        KCIG_CUDA(cudaGetLastError());  // (counted by the caller: `launches` counts k_sum launches)
+    }
     return KCIG_OK;
+}
+
+int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+    }
+    const long long tiles = (long long)((nz + 15) / 16) * ((nx + 7) / 8);
+    const long long want = 2LL * sms * KCIG_SUM_MINB;  // two waves of resident CTAs
+    if (tiles >= want) return 1;
+    const int blocks = shared_r ? (nsb + KCIG_KB - 1) / KCIG_KB : nsb;
+    long long ns = (want + tiles - 1) / tiles;
+    ns = std::min<long long>(ns, std::min(blocks, 64));
+    return (int)std::max<long long>(1, ns);
 }
 
 }  // namespace kcig

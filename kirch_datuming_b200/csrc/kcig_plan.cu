@@ -58,8 +58,9 @@ struct kcig_plan {
     const float *sgx = nullptr, *sgz = nullptr, *rgx = nullptr, *rgz = nullptr;
     DevBuf own_stab, own_sder, own_rtab, own_rder, own_sgx, own_sgz, own_rgx, own_rgz;
     DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
+    DevBuf d_part;  // partial images of a split summation (small grids)
     int sum_launches = 0, all_launches = 0;
-    float sum_ms = 0.f, fields_ms = 0.f;
+    float sum_ms = 0.f, fields_ms = 0.f, prelude_ms = 0.f;
     kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
     struct ShotsPrepared *shots = nullptr;                 // ragged shots uploaded by kcig_shots_prepare
     int use_graph = 0;                                     // replay kcig_migrate_prepared as a CUDA graph
@@ -80,7 +81,7 @@ struct ShotsPrepared {
     int nshots = 0, ntmax = 0;
     size_t ntr = 0;
     long long pairs = 0;
-    DevBuf data, legs, trf, stop;
+    DevBuf data, legs, trf, stop, snh;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     float *graph_image = nullptr;
@@ -96,6 +97,7 @@ static void release_shots(kcig_plan *P)
     S->legs.release();
     S->trf.release();
     S->stop.release();
+    S->snh.release();
     delete S;
     P->shots = nullptr;
 }
@@ -297,7 +299,8 @@ extern "C" int kcig_plan_destroy(kcig_plan *P)
     if (!P) return KCIG_OK;
     DevBuf *bufs[] = {&P->own_stab, &P->own_sder, &P->own_rtab, &P->own_rder, &P->own_sgx, &P->own_sgz,
                       &P->own_rgx,  &P->own_rgz,  &P->d_data,   &P->d_image,  &P->d_rT,   &P->d_rF,
-                      &P->d_sT,     &P->d_sF,   &P->d_work,   &P->d_D,      &P->d_legs, &P->d_tr};
+                      &P->d_sT,     &P->d_sF,   &P->d_work,   &P->d_D,      &P->d_legs, &P->d_tr,
+                      &P->d_part};
     for (DevBuf *b : bufs) b->release();
     release_shots(P);
     if (P->own_st) cudaStreamDestroy(P->own_st);
@@ -655,6 +658,12 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             // a uniform flag spares the pair loop a dependent load per pair
             sa.unit_tw = std::all_of(h_trw.begin(), h_trw.begin() + nb, [](float v) { return v == 1.0f; }) ? 1 : 0;
             sa.tile = P->tile;
+            sa.nsplit = sum_nsplit(g.nz, g.nx, nsh, shared_r);
+            if (sa.nsplit > 1) {
+                rc = P->d_part.ensure((size_t)sa.nsplit * P->ng * nzx * sizeof(float));
+                if (rc) break;
+                sa.partial = P->d_part.as<float>();
+            }
             sa.shared_r = shared_r ? 1 : 0;
             sa.half = p.half_angle;
             sa.t0 = g.t0;
@@ -684,7 +693,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             cudaEventRecord(e1, st);
             if (rc) break;
             P->sum_launches += nl;
-            P->all_launches += nl;
+            P->all_launches += nl + (sa.nsplit > 1 ? 1 : 0);
             first = false;
             // the host-side arrays are reused by the next batch
             if (s0 + nsb < g.ns || r0 + nhc < g.nh) {
@@ -728,6 +737,8 @@ extern "C" int kcig_plan_last_timing(const kcig_plan *P, float *fields_ms, float
     return KCIG_OK;
 }
 
+extern "C" float kcig_plan_last_prelude_ms(const kcig_plan *P) { return P ? P->prelude_ms : 0.f; }
+
 extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_surrogate *rcv)
 {
     if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_surrogate: null plan");
@@ -765,21 +776,28 @@ TraceViews trace_views(const ShotsPrepared *S)
     return v;
 }
 
-// leg fields and integrated traces of batch b (everything k_sum reads)
-int batch_inputs(kcig_plan *P, size_t b, cudaStream_t st)
+// leg fields of batch b
+int batch_fields(kcig_plan *P, size_t b, cudaStream_t st)
 {
     const ShotsPrepared *S = P->shots;
     const ShotBatch &B = S->batches[b];
-    const kcig_params &p = P->p;
-    const kcig_geometry &g = P->g;
-    const TraceViews v = trace_views(S);
     const LegInterp *legs = S->legs.as<LegInterp>();
     cudaStream_t saved = P->st;
     P->st = st;
     int rc = compute_fields_dev(P, 1, legs + B.sleg0, B.ns, P->d_sT.as<double2>(), P->d_sF.as<float2>());
     if (!rc) rc = compute_fields_dev(P, 0, legs + B.rleg0, B.nrl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
     P->st = saved;
-    if (rc) return rc;
+    return rc;
+}
+
+// integrated traces of batch b
+int batch_prelude(kcig_plan *P, size_t b, cudaStream_t st)
+{
+    const ShotsPrepared *S = P->shots;
+    const ShotBatch &B = S->batches[b];
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    const TraceViews v = trace_views(S);
     PreludeArgs pa;
     memset(&pa, 0, sizeof pa);
     pa.data = S->data.as<float>();
@@ -823,7 +841,10 @@ SumArgs batch_sum_args(const kcig_plan *P, size_t b, float *d_img)
     sa.rfi = v.rfi + B.tr0;
     sa.igo = v.igo + B.tr0;
     sa.stop = S->stop.as<float>() + B.shot0;
+    sa.snh = S->snh.as<int>() + B.shot0;
     sa.tile = P->tile;
+    sa.nsplit = sum_nsplit(g.nz, g.nx, B.ns, false);
+    if (sa.nsplit > 1) sa.partial = P->d_part.as<float>();  // sized by kcig_shots_prepare
     sa.image = d_img;
     sa.zero_init = b == 0 ? 1 : 0;
     sa.nz = g.nz;
@@ -855,16 +876,30 @@ SumArgs batch_sum_args(const kcig_plan *P, size_t b, float *d_img)
     return sa;
 }
 
-int run_prepared(kcig_plan *P, float *d_img, cudaStream_t st)
+int batch_inputs(kcig_plan *P, size_t b, cudaStream_t st)
+{
+    KCIG_TRY(batch_fields(P, b, st));
+    return batch_prelude(P, b, st);
+}
+
+// `ev` (4 events per batch, or null): before the fields, after the fields,
+// after the prelude, after the summation -- for the stage times of a direct
+// (uncaptured) run
+int run_prepared(kcig_plan *P, float *d_img, cudaStream_t st, cudaEvent_t *ev = nullptr)
 {
     ShotsPrepared *S = P->shots;
     for (size_t b = 0; b < S->batches.size(); b++) {
-        KCIG_TRY(batch_inputs(P, b, st));
+        if (ev) cudaEventRecord(ev[4 * b], st);
+        KCIG_TRY(batch_fields(P, b, st));
+        if (ev) cudaEventRecord(ev[4 * b + 1], st);
+        KCIG_TRY(batch_prelude(P, b, st));
+        if (ev) cudaEventRecord(ev[4 * b + 2], st);
         const SumArgs sa = batch_sum_args(P, b, d_img);
         int nl = 0;
         KCIG_TRY(launch_sum(sa, st, &nl));
+        if (ev) cudaEventRecord(ev[4 * b + 3], st);
         P->sum_launches += nl;
-        P->all_launches += nl;
+        P->all_launches += nl + (sa.nsplit > 1 ? 1 : 0);
     }
     if (S->batches.empty()) {
         const size_t nzx = (size_t)P->g.nz * P->g.nx;
@@ -924,6 +959,7 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
     std::vector<double> h_msx, h_mrx;
     std::vector<long long> h_toff;
     std::vector<float> h_trw, h_stop;
+    std::vector<int> h_snh;
     std::vector<int> h_rfi, h_igo, h_tnt;
     size_t max_s = 0, max_r = 0, max_d = 0;
     int i0 = 0;
@@ -936,8 +972,8 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
             const float dhf = sh.nh == 1 ? 0.0f : sh.dh;
             std::map<std::tuple<double, float, float>, int> add;
             for (int k = 0; k < sh.nh; k++) {
-                const double hx = (double)sh.h0 + (double)k * (double)dhf;
-                const float hxf = sh.h0 + (float)k * dhf;
+                const double hx = sh.h ? (double)sh.h[k] : (double)sh.h0 + (double)k * (double)dhf;
+                const float hxf = sh.h ? sh.h[k] : sh.h0 + (float)k * dhf;
                 const double rpos = p.cmp ? (double)sh.sx + hx : hx;
                 const float rposf = p.cmp ? sh.sx + hxf : hxf;
                 const auto key = std::make_tuple(rpos, rposf, dhf);
@@ -964,6 +1000,7 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
             L.scale = 0.0f;  // one-shot file: ds = 0
             hlegs.push_back(L);
             h_stop.push_back((float)(sh.nt - 1));
+            h_snh.push_back(sh.nh);
         }
         B.rleg0 = hlegs.size();
         std::map<std::tuple<double, float, float>, int> index;
@@ -983,8 +1020,8 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
                     unit = false;
                     continue;
                 }
-                const double hx = (double)sh.h0 + (double)r * (double)dhf;
-                const float hxf = sh.h0 + (float)r * dhf;
+                const double hx = sh.h ? (double)sh.h[r] : (double)sh.h0 + (double)r * (double)dhf;
+                const float hxf = sh.h ? sh.h[r] : sh.h0 + (float)r * dhf;
                 const double rpos = p.cmp ? (double)sh.sx + hx : hx;
                 const float rposf = p.cmp ? sh.sx + hxf : hxf;
                 const auto key = std::make_tuple(rpos, rposf, dhf);
@@ -1046,6 +1083,7 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
     rc = S->legs.ensure(std::max<size_t>(hlegs.size(), 1) * sizeof(LegInterp));
     if (!rc) rc = S->trf.ensure(std::max<size_t>(ntr, 1) * (3 * 8 + 4 * 4));
     if (!rc) rc = S->stop.ensure(std::max<size_t>(h_stop.size(), 1) * sizeof(float));
+    if (!rc) rc = S->snh.ensure(std::max<size_t>(h_snh.size(), 1) * sizeof(int));
     if (!rc) rc = P->d_sT.ensure(std::max<size_t>(max_s, 1) * nzx * sizeof(double2));
     if (!rc) rc = P->d_sF.ensure(std::max<size_t>(max_s, 1) * nzx * sizeof(float2));
     if (!rc) rc = P->d_rT.ensure(std::max<size_t>(max_r, 1) * nzx * sizeof(double2));
@@ -1053,6 +1091,9 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
     if (!rc) rc = P->d_D.ensure(std::max<size_t>(max_d, 1) * (size_t)ntmax * sizeof(double2));
     if (!rc && angle && !(P->sg_src && P->sg_rcv))
         rc = P->d_work.ensure((size_t)field_batch(P, std::max(max_s, max_r)) * 4 * nzx * sizeof(double));
+    int max_split = 1;
+    for (const ShotBatch &B : S->batches) max_split = std::max(max_split, sum_nsplit(g.nz, g.nx, B.ns, false));
+    if (!rc && max_split > 1) rc = P->d_part.ensure((size_t)max_split * P->ng * nzx * sizeof(float));
     struct Cp { void *dst; const void *src; size_t bytes; } cps[] = {
         {S->legs.p, hlegs.data(), hlegs.size() * sizeof(LegInterp)},
         {S->trf.as<double>(), h_msx.data(), ntr * 8},
@@ -1062,7 +1103,8 @@ extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *sho
         {S->trf.as<char>() + 28 * ntr, h_rfi.data(), ntr * 4},
         {S->trf.as<char>() + 32 * ntr, h_igo.data(), ntr * 4},
         {S->trf.as<char>() + 36 * ntr, h_tnt.data(), ntr * 4},
-        {S->stop.p, h_stop.data(), h_stop.size() * 4}};
+        {S->stop.p, h_stop.data(), h_stop.size() * 4},
+        {S->snh.p, h_snh.data(), h_snh.size() * 4}};
     for (auto &c : cps) {
         if (rc || c.bytes == 0) continue;
         cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st);
@@ -1155,7 +1197,24 @@ extern "C" int kcig_migrate_prepared(kcig_plan *P, float *image, int memory)
             }
         }
     } else {
-        rc = run_prepared(P, d_img, st);
+        std::vector<cudaEvent_t> ev(4 * S->batches.size());
+        for (auto &x : ev) cudaEventCreate(&x);
+        rc = run_prepared(P, d_img, st, ev.data());
+        if (!rc) {
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(prepared)");
+        }
+        P->prelude_ms = 0.f;
+        for (size_t b = 0; b < S->batches.size() && !rc; b++) {
+            float f = 0.f, q = 0.f, m = 0.f;
+            cudaEventElapsedTime(&f, ev[4 * b], ev[4 * b + 1]);
+            cudaEventElapsedTime(&q, ev[4 * b + 1], ev[4 * b + 2]);
+            cudaEventElapsedTime(&m, ev[4 * b + 2], ev[4 * b + 3]);
+            P->fields_ms += f;
+            P->prelude_ms += q;
+            P->sum_ms += m;
+        }
+        for (auto &x : ev) cudaEventDestroy(x);
     }
     if (!rc && memory == KCIG_MEM_HOST) {
         cudaError_t e = cudaMemcpyAsync(image, d_img, img_bytes, cudaMemcpyDeviceToHost, st);

@@ -126,11 +126,13 @@ def _rows_at(tables: torch.Tensor, g: Geometry, xs: np.ndarray, rows: torch.Tens
 
 
 def shot_gathers(tables: torch.Tensor, g: Geometry, reflectors: list, freq: float,
-                 seed: int, snr_amp: float = 10.0, shot_chunk: int = 8) -> torch.Tensor:
+                 seed: int, snr_amp: float = 10.0, shot_chunk: int = 8, noise_on_device: bool = False) -> torch.Tensor:
     """FP32 gathers [ns][nh][nt] on tables.device.
 
     tables: [npos][nx][nz] source/receiver traveltime table (shared).
     reflectors: list of (depth index per column [nx], reflectivity).
+    noise_on_device: draw the noise with a device generator (fast for
+    multi-GB cubes; a different seeded realisation than the host draw).
     """
     dev = tables.device
     gen = torch.Generator(device="cpu").manual_seed(seed)
@@ -153,8 +155,12 @@ def shot_gathers(tables: torch.Tensor, g: Geometry, reflectors: list, freq: floa
             tref = (ts[:, None, :] + tr).amin(dim=2)  # [chunk][nh]
             out[a:b] += refl * ricker(t[None, None, :] - tref[:, :, None], freq)
     rms = out.square().mean().sqrt()
-    noise = torch.randn(out.shape, generator=gen, dtype=torch.float32).to(dev)
-    out += noise * (rms / snr_amp)
+    if noise_on_device:
+        dgen = torch.Generator(device=dev).manual_seed(seed)
+        out += torch.randn(out.shape, generator=dgen, dtype=torch.float32, device=dev) * (rms / snr_amp)
+    else:
+        noise = torch.randn(out.shape, generator=gen, dtype=torch.float32).to(dev)
+        out += noise * (rms / snr_amp)
     return out
 
 

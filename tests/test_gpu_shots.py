@@ -138,3 +138,29 @@ def test_autotune_and_multi_plan_graph(golden):
     g.close()
     for p in plans:
         p.close()
+
+
+def test_receiver_stations_given_explicitly(golden):
+    # receivers given as an explicit axis (kcig_shot.h): equal values share a
+    # leg across shots.  The values are taken as given (FP32), where h0 + k*dh
+    # is rebuilt in FP64 for the continuous quantities: the images agree to
+    # that rounding (~1e-8 km in position)
+    kp, geom, axis, op, _ = _cases.case_setup(golden, "base")
+    T, D = golden.tables()
+    shots = _ragged(golden, "base")
+    f32 = np.float32
+    explicit = []
+    for s in shots:
+        nh = s["data"].shape[0]
+        h = f32(s["h0"]) + np.arange(nh, dtype=f32) * f32(s["dh"])
+        explicit.append(dict(sx=s["sx"], dh=s["dh"], h=h, data=s["data"]))
+    imgs = []
+    for ss in (shots, explicit):
+        plan = kd.Plan(kp, kd.geometry(**geom))
+        plan.set_tables(T, D, T, D)
+        im = np.zeros((axis[0], geom["nx"], geom["nz"]), np.float32)
+        plan.prepare_shots(ss)
+        plan.migrate_prepared(im)
+        plan.close()
+        imgs.append(im)
+    assert np.linalg.norm(imgs[1] - imgs[0]) <= 1e-5 * np.linalg.norm(imgs[0])
