@@ -185,6 +185,14 @@ int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, fl
  * (device int) becomes 1 if the kernel gave up waiting for the tensor core. */
 int kcig_tc_selftest(const void *X, const void *W, float *D, int *status, void *stream);
 
+/* Forward modelling (kirchmig2d_cig adj=0, src/kirchmig2d_cig.cpp:1300-1351,
+ * SERECKIRCH/src/kirmig.cpp:59-68): data [ns][nh][nt] from image
+ * [ng][nx][nz] with the plan's geometry and parameters (host or device, as
+ * `memory`).  The exact adjoint of kcig_migrate when direct_mute = 0 and
+ * diff = 0 (the reference's forward branch applies neither; direct_mute=1
+ * is rejected with the reference's message). */
+int kcig_model(kcig_plan *plan, const float *image, float *data, int memory);
+
 /* ---------------------------------------------------------------------------
  * Shots of uneven receiver count and trace length (the recursive-layer
  * workflow's windows, run_salt_adcig.sh:131-149, migrate such gathers one

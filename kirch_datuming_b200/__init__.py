@@ -87,6 +87,7 @@ def lib():
         L.kcig_plan_set_tables.argtypes = [vp, fp, fp, fp, fp, ctypes.c_int]
         L.kcig_plan_set_gradients.argtypes = [vp, fp, fp, fp, fp, ctypes.c_int]
         L.kcig_migrate.argtypes = [vp, fp, fp, ctypes.c_int]
+        L.kcig_model.argtypes = [vp, fp, fp, ctypes.c_int]
         L.kcig_plan_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
                                            ctypes.POINTER(ctypes.c_int)]
         L.kcig_run_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
@@ -254,6 +255,14 @@ class Plan:
 
     def set_graph(self, enable=True):
         _check(lib().kcig_plan_set_graph(self._h, 1 if enable else 0))
+
+    def model(self, image, data):
+        """Forward modelling (adj=0): data [ns][nh][nt] from image [ng][nx][nz]."""
+        (ip, m1), (dp_, m2) = _ptr(image), _ptr(data)
+        if m1 != m2:
+            raise ValueError("image and data must both be host or both be device arrays")
+        _check(lib().kcig_model(self._h, ip, dp_, m1))
+        return data
 
     def migrate(self, data, image):
         (dp_, m1), (ip, m2) = _ptr(data), _ptr(image)

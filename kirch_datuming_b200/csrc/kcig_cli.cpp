@@ -1,4 +1,4 @@
-// kcig_run_cli: the drop-in kirchmig2d_cig (adj=1).  Same argv keys, files,
+// kcig_run_cli: the drop-in kirchmig2d_cig (adj=1 migration, adj=0 forward modelling).  Same argv keys, files,
 // defaults, ERROR texts, output header and exit status as
 // src/kirchmig2d_cig.cpp:494-1401; the migration itself runs on the GPU.
 #include <cuda_runtime.h>
@@ -82,7 +82,7 @@ extern "C" int kcig_run_cli(int argc, char **argv)
         if (!m.have(k[0])) return fail(set_error(KCIG_ERR_ARG, "%s", k[1]));
     rc = params_from_map(m, &p);
     if (rc) return fail(rc);
-    if (!p.adj) return fail(set_error(KCIG_ERR_UNSUPPORTED, "adj=0 (forward modelling) is not built; only adj=1 is."));
+    const bool fwd = !p.adj;  // adj=0: migration= is read, seismic_data= written (:643-701)
     const bool angle = p.cig && p.cig_is_angle;
     int use_grad = 0;
     if (angle) {
@@ -94,17 +94,45 @@ extern "C" int kcig_run_cli(int argc, char **argv)
         use_grad = hg == 4;
     }
     RsfFile dat, stim, sder, rtim, rder;
-    if ((rc = open3(m, "seismic_data", &dat, "Need 3D data volume for seismic_data= (t,h/r,s)"))) return fail(rc);
     kcig_geometry g;
-    g.nt = dat.n[0];
-    g.nh = dat.n[1];
-    g.ns = dat.n[2];
-    g.t0 = (float)dat.o[0];
-    g.dt = (float)dat.d[0];
-    g.h0 = (float)dat.o[1];
-    g.dh = (float)dat.d[1];
-    g.s0 = (float)dat.o[2];
-    g.ds = (float)dat.d[2];
+    if (!fwd) {
+        if ((rc = open3(m, "seismic_data", &dat, "Need 3D data volume for seismic_data= (t,h/r,s)"))) return fail(rc);
+        g.nt = dat.n[0];
+        g.nh = dat.n[1];
+        g.ns = dat.n[2];
+        g.t0 = (float)dat.o[0];
+        g.dt = (float)dat.d[0];
+        g.h0 = (float)dat.o[1];
+        g.dh = (float)dat.d[1];
+        g.s0 = (float)dat.o[2];
+        g.ds = (float)dat.d[2];
+    } else {
+        // the data geometry comes from the parameters (:663-701)
+        struct { const char *k; int *v; int def; const char *need; } ints[3] = {
+            {"nt", &g.nt, 0, "Need nt="}, {"nh", &g.nh, 1, nullptr}, {"ns", &g.ns, 1, nullptr}};
+        for (auto &q : ints) {
+            if (!m.have(q.k)) {
+                if (q.need) return fail(set_error(KCIG_ERR_ARG, "%s", q.need));
+                *q.v = q.def;
+            } else if ((rc = m.get_int(q.k, q.v))) {
+                return fail(rc);
+            }
+        }
+        struct { const char *k; float *v; const char *need; } fls[5] = {
+            {"t0", &g.t0, nullptr}, {"dt", &g.dt, "Need dt="}, {"h0", &g.h0, nullptr}, {"dh", &g.dh, "Need dh="},
+            {"s0", &g.s0, nullptr}};
+        for (auto &q : fls) {
+            if (!m.have(q.k)) {
+                if (q.need) return fail(set_error(KCIG_ERR_ARG, "%s", q.need));
+                *q.v = 0.0f;
+            } else if ((rc = m.get_float(q.k, q.v))) {
+                return fail(rc);
+            }
+        }
+        if (!m.have("ds")) return fail(set_error(KCIG_ERR_ARG, "Need ds="));
+        if ((rc = m.get_float("ds", &g.ds))) return fail(rc);
+        if (g.nt < 1 || g.nh < 1 || g.ns < 1) return fail(set_error(KCIG_ERR_ARG, "Need 3D data volume for seismic_data= (t,h/r,s)"));
+    }
     if (g.nh == 1) g.dh = 0.0f;
     if (g.ns == 1) g.ds = 0.0f;
     if (p.direct_mute && p.direct_mute_qc_shot >= g.ns)
@@ -157,7 +185,7 @@ extern "C" int kcig_run_cli(int argc, char **argv)
     const size_t nzx = (size_t)g.nz * g.nx;
     std::vector<float> data((size_t)g.nt * g.nh * g.ns);
     std::vector<float> st(nzx * g.sny), sd(nzx * g.sny);
-    if ((rc = rsf_read(dat, 0, (long long)data.size(), data.data()))) return fail(rc);
+    if (!fwd && (rc = rsf_read(dat, 0, (long long)data.size(), data.data()))) return fail(rc);
     if ((rc = rsf_read(stim, 0, (long long)st.size(), st.data()))) return fail(rc);
     if ((rc = rsf_read(sder, 0, (long long)sd.size(), sd.data()))) return fail(rc);
     const bool same_r = (rtim.binary == stim.binary && rder.binary == sder.binary && g.rny == g.sny);
@@ -208,13 +236,32 @@ extern "C" int kcig_run_cli(int argc, char **argv)
                               KCIG_MEM_HOST);
     if (!rc && use_grad)
         rc = kcig_plan_set_gradients(plan, gvol[0].data(), gvol[1].data(), gvol[2].data(), gvol[3].data(), KCIG_MEM_HOST);
-    if (!rc) rc = kcig_migrate(plan, data.data(), img.data(), KCIG_MEM_HOST);
+    if (fwd) {
+        // the model: nzx * ng floats of migration= (:966), whatever its header says
+        RsfFile mig;
+        if (!rc) rc = rsf_open(m.str("migration"), &mig);
+        if (!rc) rc = rsf_read(mig, 0, (long long)img.size(), img.data());
+        if (!rc) rc = kcig_model(plan, img.data(), data.data(), KCIG_MEM_HOST);
+    } else if (!rc) {
+        rc = kcig_migrate(plan, data.data(), img.data(), KCIG_MEM_HOST);
+    }
     kcig_plan_destroy(plan);
     if (rc) return fail(rc);
     const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     log_line("INFO", "FINISH.");
     snprintf(msg, sizeof msg, "Done. Elapsed time: %.3f s.", el);
     log_line("INFO", msg);
+    if (fwd) {
+        // the data header of :906-920, with its three axes
+        const int n3[3] = {g.nt, g.nh, g.ns};
+        const double o3[3] = {g.t0, g.h0, g.s0};
+        const double d3[3] = {g.dt, g.dh, g.ds};
+        std::vector<std::pair<std::string, std::string>> keys = {
+            {"label1", "Time"}, {"unit1", "s"}, {"label2", p.cmp ? "Offset" : "Receiver"}, {"label3", "Shot"}};
+        if ((rc = rsf_write(m.str("seismic_data"), 3, n3, o3, d3, keys, data.data(), (long long)data.size())))
+            return fail(rc);
+        return KCIG_OK;
+    }
     // output header (:876-905)
     const int n3[3] = {g.nz, g.nx, p.cig ? ng : 1};
     const double o3[3] = {g.z0, g.x0, p.cig ? (double)g0 : 0.0};

@@ -130,6 +130,26 @@ struct SumArgs {
 int launch_sum(const SumArgs &a, cudaStream_t st, int *launches);
 // Tile variants the summation can be launched with (the autotuner's choices):
 // {TZ, TX, shots per block on the receiver-shared path}.
+// Forward modelling (adj=0): the picks of k_sum run backwards, each image
+// value sprayed onto the six trace samples of its pick.
+struct SprayArgs {
+    const double2 *STP;    // [nsb][nzx] source {T, phi}
+    const float2 *SXW;     // [nsb][nzx] source {Tx*ds, w}
+    const double2 *RTP;    // [nrf][nzx] receiver {T, phi}
+    const float2 *RXW;     // [nrf][nzx] receiver {Tx*dh, w}
+    const float *trw;      // [nsb*nh] trace weight, 0 = the trace stays zero
+    const int *rfi;        // [nsb*nh] receiver field index
+    const int *igo;        // [nsb*nh] offset-mode bin
+    const float *image;    // [ng][nzx] model
+    double *raw;           // [nsb*nh][nt] sprayed traces, before doubint
+    int nz, nx, nt, nsb, nh, ng;
+    int mode;              // 0 angle two-bin, 1 angle nearest, 2 single bin
+    double t0, inv_dt, tau, deg, ug0, uinv;
+    float aal, oazmin, oazmax, oaztaper, ats, ate;
+};
+int launch_spray(const SprayArgs &a, cudaStream_t st);
+int launch_doubint_f32(const double *in, float *out, int ntr, int nt, cudaStream_t st);
+
 // How many shot splits a summation over nsb shots on an nz x nx image needs
 // to give the GPU at least two waves of CTAs (1: none).
 int sum_nsplit(int nz, int nx, int nsb, bool shared_r);

@@ -150,7 +150,8 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
     }
 }
 
-__global__ void __launch_bounds__(64) k_doubint_plain(const float *in, double *out, int ntr, int nt,
+template <typename IN, typename OUT>
+__global__ void __launch_bounds__(64) k_doubint_plain(const IN *in, OUT *out, int ntr, int nt,
                                                       int isdiff, double dt)
 {
     extern __shared__ double smem_d[];
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(64) k_doubint_plain(const float *in, double *o
     __syncwarp();
     doubint_warp(s, nt);
     if (isdiff == 1) diff2_warp(s, nt, dt);
-    for (int i = lane; i < nt; i += 32) out[(size_t)tr * nt + i] = s[i];
+    for (int i = lane; i < nt; i += 32) out[(size_t)tr * nt + i] = (OUT)s[i];
 }
 
 int set_dyn_smem(const void *fn, int bytes)
@@ -200,6 +201,19 @@ int launch_prelude(const PreludeArgs &a, cudaStream_t st)
     return KCIG_OK;
 }
 
+int launch_doubint_f32(const double *in, float *out, int ntr, int nt, cudaStream_t st)
+{
+    if (ntr <= 0) return KCIG_OK;
+    int warps;
+    if (prelude_block(nt, &warps))
+        return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", nt);
+    const size_t sm = (size_t)warps * nt * sizeof(double);
+    KCIG_TRY(set_dyn_smem((const void *)k_doubint_plain<double, float>, (int)sm));
+    k_doubint_plain<double, float><<<(ntr + warps - 1) / warps, 32 * warps, sm, st>>>(in, out, ntr, nt, 0, 1.0);
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
 int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdiff, double dt,
                          cudaStream_t st)
 {
@@ -208,8 +222,8 @@ int launch_doubint_plain(const float *in, double *out, int ntr, int nt, int isdi
     if (prelude_block(nt, &warps))
         return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", nt);
     const size_t sm = (size_t)warps * nt * sizeof(double);
-    KCIG_TRY(set_dyn_smem((const void *)k_doubint_plain, (int)sm));
-    k_doubint_plain<<<(ntr + warps - 1) / warps, 32 * warps, sm, st>>>(in, out, ntr, nt, isdiff, dt);
+    KCIG_TRY(set_dyn_smem((const void *)k_doubint_plain<float, double>, (int)sm));
+    k_doubint_plain<float, double><<<(ntr + warps - 1) / warps, 32 * warps, sm, st>>>(in, out, ntr, nt, isdiff, dt);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
@@ -697,6 +711,129 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
         }
     }
     for (int b = 0; b < nb; b++) out[(size_t)(gc0 + b) * nzx + i] = acc[b * P + tid];
+}
+
+// ------------------------------------------------------- forward modelling --
+// kirchmig2d_cig adj=0 (:1300-1312, kirmig.cpp:59-68): one CTA per shot and
+// block of RB receivers, the RB traces accumulated in shared memory in FP64
+// (the trace is integrated twice afterwards, which would amplify FP32
+// accumulation error; threads sweep the image points, and neighbouring points
+// land on different samples), the same gates, weights and pick positions as
+// k_sum.
+template <int MODE, int RB>
+__global__ void __launch_bounds__(256) k_spray(const __grid_constant__ SprayArgs a)
+{
+    constexpr double kPiD = 3.141592653589793238463, kTwoPi = 6.283185307179586476925;
+    extern __shared__ double tr[];  // [RB][nt]
+    const int nrb = (a.nh + RB - 1) / RB;
+    const int k = blockIdx.x / nrb, r0 = (blockIdx.x % nrb) * RB;
+    const int nr = min(RB, a.nh - r0);
+    for (int q = threadIdx.x; q < RB * a.nt; q += blockDim.x) tr[q] = 0.0;
+    float tw[RB];
+    int ri[RB], ig[RB];
+#pragma unroll
+    for (int j = 0; j < RB; j++) {
+        const int trc = k * a.nh + r0 + j;
+        tw[j] = j < nr ? __ldg(a.trw + trc) : 0.0f;
+        ri[j] = j < nr ? __ldg(a.rfi + trc) : 0;
+        ig[j] = j < nr ? __ldg(a.igo + trc) : 0;
+    }
+    __syncthreads();
+    const int nzx = a.nz * a.nx;
+    const double top = (double)(a.nt - 1);
+    const double ulo = -1.0e-5, uhi = (double)(a.ng - 1) + 1.0e-5;
+    const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;
+    for (int i = threadIdx.x; i < nzx; i += blockDim.x) {
+        const double2 sTP = __ldg(a.STP + (size_t)k * nzx + i);
+        const float2 sXW = __ldg(a.SXW + (size_t)k * nzx + i);
+        if (!(sXW.y > 0.0f)) continue;
+        const int iz = i % a.nz;
+        const float zf = (a.nz > 1) ? (float)iz / (float)(a.nz - 1) : 0.0f;
+        const float cutoff = a.oazmin + zf * (a.oazmax - a.oazmin);
+#pragma unroll
+        for (int j = 0; j < RB; j++) {
+            if (tw[j] == 0.0f) continue;
+            const double2 rTP = __ldg(a.RTP + (size_t)ri[j] * nzx + i);
+            const float2 rXW = __ldg(a.RXW + (size_t)ri[j] * nzx + i);
+            const float apw = sXW.y * rXW.y;
+            if (!(apw > 0.0f)) continue;
+            int b0 = 0;
+            float w0 = 1.0f, w1 = 0.0f, aw;
+            if (MODE == 2) {
+                b0 = ig[j];
+                aw = tw[j] * apw;
+            } else {
+                double th = fabs(sTP.y - rTP.y);
+                th = (th > kPiD) ? kTwoPi - th : th;
+                const double u = fma(th, uk, -ub);
+                double fl;
+                if (MODE == 0) {
+                    if (!(u >= ulo && u <= uhi)) continue;
+                    fl = floor(u);
+                } else {
+                    fl = floor(u + 0.5);
+                    if (!(fl >= 0.0 && fl < (double)a.ng)) continue;
+                }
+                const float ang = (float)(th * a.deg);
+                aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw[j] * apw;
+                if (!(aw > 0.0f)) continue;
+                if (MODE == 0) {
+                    if (u <= 0.0) { b0 = 0; w0 = 1.0f; w1 = 0.0f; }
+                    else if (u >= (double)(a.ng - 1)) { b0 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
+                    else {
+                        b0 = (int)fl;
+                        const double f1 = u - fl;
+                        w1 = (float)f1;
+                        w0 = (float)(1.0 - f1);
+                    }
+                } else {
+                    b0 = (int)fl;
+                }
+            }
+            const double ft0 = (sTP.x + rTP.x + a.tau - a.t0) * a.inv_dt;
+            const double sh = fma((double)(fmaxf(fabsf(sXW.x), fabsf(rXW.x)) * a.aal), a.inv_dt, 1.0);
+            const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
+            const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
+            if (!(fl0 >= 0.0 && fl0 < top && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < top)) continue;
+            float val = w0 * __ldg(a.image + (size_t)b0 * nzx + i);
+            if (MODE == 0 && w1 > 0.0f) val += w1 * __ldg(a.image + (size_t)(b0 + 1) * nzx + i);
+            const float r1 = 1.0f / (1.0f + 2.0f * (float)sh);  // dt / (dt + tp - tm)
+            const double sv = (double)(r1 * r1 * (aw * val));
+            double *t = tr + j * a.nt;
+            const double f0 = ft0 - fl0, fm = ftm0 - flm, fp = ftp0 - flp;
+            atomicAdd(t + (int)fl0, 2.0 * (1.0 - f0) * sv);
+            atomicAdd(t + (int)fl0 + 1, 2.0 * f0 * sv);
+            atomicAdd(t + (int)flm, -(1.0 - fm) * sv);
+            atomicAdd(t + (int)flm + 1, -fm * sv);
+            atomicAdd(t + (int)flp, -(1.0 - fp) * sv);
+            atomicAdd(t + (int)flp + 1, -fp * sv);
+        }
+    }
+    __syncthreads();
+    for (int j = 0; j < nr; j++)
+        for (int q = threadIdx.x; q < a.nt; q += blockDim.x)
+            a.raw[((size_t)k * a.nh + r0 + j) * a.nt + q] = tr[j * a.nt + q];
+}
+
+int launch_spray(const SprayArgs &a, cudaStream_t st)
+{
+    if (a.nsb <= 0 || a.nh <= 0) return KCIG_OK;
+    constexpr int RB = 4;
+    const size_t sm = (size_t)RB * a.nt * sizeof(double);
+    if (sm > 200 * 1024) return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d too long for forward modelling", a.nt);
+    const int grid = a.nsb * ((a.nh + RB - 1) / RB);
+    if (a.mode == 0) {
+        KCIG_TRY(set_dyn_smem((const void *)k_spray<0, RB>, (int)sm));
+        k_spray<0, RB><<<grid, 256, sm, st>>>(a);
+    } else if (a.mode == 1) {
+        KCIG_TRY(set_dyn_smem((const void *)k_spray<1, RB>, (int)sm));
+        k_spray<1, RB><<<grid, 256, sm, st>>>(a);
+    } else {
+        KCIG_TRY(set_dyn_smem((const void *)k_spray<2, RB>, (int)sm));
+        k_spray<2, RB><<<grid, 256, sm, st>>>(a);
+    }
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
 }
 
 // image (+)= the split rows' partial images, rows in order (deterministic)

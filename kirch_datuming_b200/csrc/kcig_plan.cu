@@ -260,7 +260,6 @@ extern "C" int kcig_plan_create(const kcig_params *p, const kcig_geometry *g, un
 {
     if (!p || !g || !out) return set_error(KCIG_ERR_ARG, "kcig_plan_create: null argument");
     *out = nullptr;
-    if (!p->adj) return set_error(KCIG_ERR_UNSUPPORTED, "adj=0 (forward modelling) is not built; only adj=1 is.");
     if (g->nt < 1 || g->nh < 1 || g->ns < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for seismic_data= (t,h/r,s)");
     if (g->nz < 1 || g->nx < 1 || g->sny < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for stable= (z,x,s)");
     if (g->rny < 1) return set_error(KCIG_ERR_ARG, "Need 3D data volume for rtable= (z,x,r)");
@@ -745,6 +744,170 @@ extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_s
     P->sg_src = src;
     P->sg_rcv = rcv;
     return KCIG_OK;
+}
+
+// ------------------------------------------------------- forward modelling --
+// kirchmig2d_cig adj=0: data [ns][nh][nt] from an image [ng][nx][nz] with the
+// plan's geometry, the exact adjoint of kcig_migrate without the direct mute
+// and diff2 (the reference's forward branch applies neither and rejects
+// direct_mute=1).  Same per-trace gates as the migration.
+extern "C" int kcig_model(kcig_plan *P, const float *image, float *data, int memory)
+{
+    if (!P || !image || !data) return set_error(KCIG_ERR_ARG, "kcig_model: null argument");
+    if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab)) return set_error(KCIG_ERR_ARG, "kcig_model: tables not set");
+    const kcig_params &p = P->p;
+    const kcig_geometry &g = P->g;
+    if (p.direct_mute) return set_error(KCIG_ERR_ARG, "direct_mute=1 is an input-data preprocessing option and requires adj=1.");
+    const size_t nzx = (size_t)g.nz * g.nx;
+    const int angle = p.cig && p.cig_is_angle;
+    cudaStream_t st = P->st;
+    P->sum_launches = 0;
+    P->all_launches = 0;
+    const float *d_img = image;
+    float *d_dat = data;
+    const size_t img_bytes = (size_t)P->ng * nzx * sizeof(float);
+    const size_t dat_bytes = (size_t)g.ns * g.nh * g.nt * sizeof(float);
+    if (memory == KCIG_MEM_HOST) {
+        KCIG_TRY(upload(P->d_image, image, img_bytes, st));
+        d_img = P->d_image.as<float>();
+        KCIG_TRY(P->d_data.ensure(dat_bytes));
+        d_dat = P->d_data.as<float>();
+    }
+    const double ds = g.ns == 1 ? 0.0 : (double)g.ds, dh = g.nh == 1 ? 0.0 : (double)g.dh;
+    std::vector<double> sx(g.ns), hx(g.nh);
+    std::vector<float> sxf(g.ns), hxf(g.nh);
+    for (int is = 0; is < g.ns; is++) {
+        sx[is] = (double)g.s0 + (double)is * ds;
+        sxf[is] = g.s0 + (float)is * (float)ds;
+    }
+    for (int ih = 0; ih < g.nh; ih++) {
+        hx[ih] = (double)g.h0 + (double)ih * dh;
+        hxf[ih] = g.h0 + (float)ih * (float)dh;
+    }
+    // batches of shots: source and receiver legs, raw traces
+    const size_t leg_bytes = nzx * (sizeof(double2) + sizeof(float2));
+    const size_t per_shot = leg_bytes * (1 + (size_t)g.nh) + (size_t)g.nh * g.nt * sizeof(double) + (size_t)g.nh * 16;
+    int nsb = (int)std::max<long long>(1, (long long)(P->budget / 2) / (long long)per_shot);
+    nsb = std::min(nsb, g.ns);
+    int rc = P->d_sT.ensure((size_t)nsb * nzx * sizeof(double2));
+    if (!rc) rc = P->d_sF.ensure((size_t)nsb * nzx * sizeof(float2));
+    if (!rc) rc = P->d_rT.ensure((size_t)nsb * g.nh * nzx * sizeof(double2));
+    if (!rc) rc = P->d_rF.ensure((size_t)nsb * g.nh * nzx * sizeof(float2));
+    if (!rc) rc = P->d_D.ensure((size_t)nsb * g.nh * g.nt * sizeof(double));  // raw traces
+    if (!rc) rc = P->d_tr.ensure((size_t)nsb * g.nh * (sizeof(float) + 2 * sizeof(int)));
+    if (rc) return rc;
+    float *d_trw = P->d_tr.as<float>();
+    int *d_rfi = (int *)(d_trw + (size_t)nsb * g.nh);
+    int *d_igo = d_rfi + (size_t)nsb * g.nh;
+    std::vector<float> h_trw((size_t)nsb * g.nh);
+    std::vector<int> h_rfi(h_trw.size()), h_igo(h_trw.size());
+    for (int s0 = 0; s0 < g.ns && rc == KCIG_OK; s0 += nsb) {
+        const int nsh = std::min(nsb, g.ns - s0);
+        std::vector<LegInterp> sl(nsh), rl;
+        std::map<std::pair<double, float>, int> seen;
+        for (int k = 0; k < nsh; k++) {
+            const int is = s0 + k;
+            const int ist = leg_interp(P, 1, sxf[is], sx[is], &sl[k]);
+            sl[k].scale = (float)ds;
+            for (int ih = 0; ih < g.nh; ih++) {
+                const size_t b = (size_t)k * g.nh + ih;
+                const double rpos = p.cmp ? sx[is] + hx[ih] : hx[ih];
+                const float rposf = p.cmp ? sxf[is] + hxf[ih] : hxf[ih];
+                const std::pair<double, float> key(rpos, rposf);
+                auto it = seen.find(key);
+                if (it == seen.end()) {
+                    LegInterp L;
+                    leg_interp(P, 0, rposf, rpos, &L);
+                    L.scale = (float)dh;
+                    it = seen.emplace(key, (int)rl.size()).first;
+                    rl.push_back(L);
+                }
+                h_rfi[b] = it->second;
+                float rf = 0.0f;
+                if (g.rny > 1 && g.rdy != 0.0f) rf = (rposf - g.ry0) / g.rdy;
+                const int iht = (g.rny > 1 && g.rdy != 0.0f) ? (int)floorf(rf) : 0;
+                double w = 1.0;
+                if (p.aperture_trace != -1) {
+                    const double ad = fabs((double)(iht - ist));
+                    if (ad >= (double)p.aperture_trace) w = 0.0;
+                    else if (p.aperture_trace_taper > 0) {
+                        const double tb = std::max(0.0, (double)(p.aperture_trace - p.aperture_trace_taper));
+                        if (ad > tb) {
+                            const double den = (double)p.aperture_trace - tb;
+                            if (den > 0.0) w = 0.5 * (1.0 + cos(M_PI * ((ad - tb) / den)));
+                        }
+                    }
+                }
+                int bin = 0;
+                if (p.cig && !p.cig_is_angle) {
+                    int b2 = -1;
+                    if (P->ng > 0 && P->dg > 0.0f && std::isfinite(hxf[ih])) {
+                        b2 = (int)floorf((hxf[ih] - P->g0) / P->dg + 0.5f);
+                        if (b2 < 0 || b2 >= P->ng) b2 = -1;
+                    }
+                    if (b2 < 0) w = 0.0;
+                    bin = b2 < 0 ? 0 : b2;
+                }
+                h_trw[b] = (float)w;
+                h_igo[b] = bin;
+            }
+        }
+        rc = compute_fields(P, 1, sl, P->d_sT.as<double2>(), P->d_sF.as<float2>());
+        if (!rc) rc = compute_fields(P, 0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
+        const size_t nb = (size_t)nsh * g.nh;
+        const void *srcs[3] = {h_trw.data(), h_rfi.data(), h_igo.data()};
+        void *dsts[3] = {d_trw, d_rfi, d_igo};
+        for (int q = 0; q < 3 && rc == KCIG_OK; q++) {
+            cudaError_t e = cudaMemcpyAsync(dsts[q], srcs[q], nb * 4, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(trace tables)");
+        }
+        if (rc) break;
+        SprayArgs sa;
+        memset(&sa, 0, sizeof sa);
+        sa.STP = P->d_sT.as<double2>();
+        sa.SXW = P->d_sF.as<float2>();
+        sa.RTP = P->d_rT.as<double2>();
+        sa.RXW = P->d_rF.as<float2>();
+        sa.trw = d_trw;
+        sa.rfi = d_rfi;
+        sa.igo = d_igo;
+        sa.image = d_img;
+        sa.raw = P->d_D.as<double>();
+        sa.nz = g.nz;
+        sa.nx = g.nx;
+        sa.nt = g.nt;
+        sa.nsb = nsh;
+        sa.nh = g.nh;
+        sa.ng = P->ng;
+        sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
+        sa.t0 = g.t0;
+        sa.inv_dt = 1.0 / (double)g.dt;
+        sa.tau = p.tau;
+        sa.deg = (p.half_angle ? 90.0 : 180.0) / M_PI;
+        sa.ug0 = P->g0;
+        sa.uinv = 1.0 / (double)P->dg;
+        sa.aal = p.antialias;
+        sa.oazmin = p.oazmin;
+        sa.oazmax = p.oazmax;
+        sa.oaztaper = p.oaztaper;
+        sa.ats = p.angle_taper_start;
+        sa.ate = p.angle_taper_end;
+        rc = launch_spray(sa, st);
+        if (!rc) rc = launch_doubint_f32(P->d_D.as<double>(), d_dat + (size_t)s0 * g.nh * g.nt, (int)nb, g.nt, st);
+        P->all_launches += 2;
+        P->sum_launches += 1;
+        if (!rc) {  // the host tables are reused by the next batch
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(model)");
+        }
+    }
+    if (!rc && memory == KCIG_MEM_HOST) {
+        cudaError_t e = cudaMemcpyAsync(data, d_dat, dat_bytes, cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(data)");
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(model)");
+    return rc;
 }
 
 // ------------------------------------------------------------ ragged shots --

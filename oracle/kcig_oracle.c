@@ -258,6 +258,45 @@ static R kirmig_pick(R ti, R deltat, const R *trace, int nt, R dt, R t0)
 #endif
 }
 
+/* SERECKIRCH/src/kirmig.cpp:59-68 (the forward branch): the sample, scaled
+ * by imp, is spread over the same six trace samples with the same weights
+ * (the reference's s = imp*sample is a float product; the six updates are
+ * evaluated in double and rounded into the float trace). */
+static void kirmig_spray(R ti, R deltat, R sample, R *trace, int nt, R dt, R t0)
+{
+    int it, itm, itp;
+    R ft, tm, tp, ftm, ftp, imp, sv;
+    ft = (ti - t0) / dt; it = (int)R_FLOOR(ft); ft -= (R)it;
+    if (it < 0 || it >= nt - 1) return;
+    tm = ti - deltat - dt;
+    ftm = (tm - t0) / dt; itm = (int)R_FLOOR(ftm); ftm -= (R)itm;
+    if (itm < 0) return;
+    tp = ti + deltat + dt;
+    ftp = (tp - t0) / dt; itp = (int)R_FLOOR(ftp); ftp -= (R)itp;
+    if (itp >= nt - 1) return;
+    imp = dt / (dt + tp - tm);
+    imp *= imp;
+    sv = imp * sample;
+#if KCIG_ORACLE_FP64
+    trace[it] += 2. * (1. - ft) * sv;
+    trace[it + 1] += 2. * ft * sv;
+    trace[itm] -= (1. - ftm) * sv;
+    trace[itm + 1] -= ftm * sv;
+    trace[itp] -= (1. - ftp) * sv;
+    trace[itp + 1] -= ftp * sv;
+#else
+    /* the reference's operand types: a double literal promotes the update
+     * to double before it is added to the float sample; ftm*s and ftp*s are
+     * float products subtracted in float */
+    trace[it] = (float)((double)trace[it] + 2. * (1. - ft) * sv);
+    trace[it + 1] = (float)((double)trace[it + 1] + 2. * ft * sv);
+    trace[itm] = (float)((double)trace[itm] - (1. - ftm) * sv);
+    trace[itm + 1] = trace[itm + 1] - ftm * sv;
+    trace[itp] = (float)((double)trace[itp] - (1. - ftp) * sv);
+    trace[itp + 1] = trace[itp + 1] - ftp * sv;
+#endif
+}
+
 /* SERECKIRCH/src/tinterpsr.cpp:37-70, 142-188, 72-140.  Writes the value
  * field p and the position-derivative field dp between slices (p0,m0) and
  * (p1,m1) at in-interval coordinate x of a position axis with spacing dxp. */
@@ -673,5 +712,129 @@ int oracle_migrate_adj(const oracle_params *P, const float *data, const float *s
     free(buf);
     free(trace);
     free(out);
+    return 0;
+}
+
+/* kirchmig2d_cig.cpp adj=0 (:1110-1147, :1300-1312, :1340-1351): forward
+ * modelling of data [ns][nh][nt] from an image [ng][nx][nz] with the weights
+ * of the adjoint path; each trace is the sum of the sprayed picks, then
+ * doubint (its own adjoint).  No direct mute and no diff2 are applied, as in
+ * the reference's forward branch.  Serial (the trace is the scatter target). */
+int oracle_model_fwd(const oracle_params *P, const float *image, const float *stab, const float *sder,
+                     const float *rtab, const float *rder, const float *sgx_v, const float *sgz_v,
+                     const float *rgx_v, const float *rgz_v, double *data)
+{
+    const int nz = P->nz, nx = P->nx, nt = P->nt, ng = P->ng;
+    const long nzx = (long)nz * nx;
+    const int angle = P->cig && P->cig_is_angle;
+    const R ds = RF(P->ns == 1 ? 0.0f : P->ds);
+    const R dh = RF(P->nh == 1 ? 0.0f : P->dh);
+    R *buf = (R *)malloc(sizeof(R) * (size_t)nzx * 18);
+    R *trace = (R *)malloc(sizeof(R) * (size_t)nt);
+    if (!buf || !trace) { free(buf); free(trace); return -1; }
+    R *ST = buf, *STx = buf + nzx, *RT = buf + 2 * nzx, *RTx = buf + 3 * nzx;
+    R *s0 = buf + 4 * nzx, *s1 = buf + 5 * nzx, *m0 = buf + 6 * nzx, *m1 = buf + 7 * nzx;
+    R *gsx = buf + 8 * nzx, *gsz = buf + 9 * nzx, *grx = buf + 10 * nzx, *grz = buf + 11 * nzx;
+    R *t1 = buf + 12 * nzx, *t2 = buf + 13 * nzx, *sgx = buf + 14 * nzx, *sgz = buf + 15 * nzx;
+    R *rgx = buf + 16 * nzx, *rgz = buf + 17 * nzx;
+    const R t0 = RF(P->t0), dt = RF(P->dt), tau = RF(P->tau), aal = RF(P->aal);
+    const R dz = RF(P->dz), dxg = RF(P->dx), x0 = RF(P->x0);
+    const R g0 = RF(P->g0), dg = RF(P->dg);
+
+    for (int is = 0; is < P->ns; is++) {
+        const R s = RF(P->s0) + (R)is * ds;
+        const float sf = P->s0 + (float)is * (P->ns == 1 ? 0.0f : P->ds);
+        const int ist = table_at(1, P, stab, sder, sf, s, P->sy0, P->sdy, P->sny, ST, STx,
+                                 s0, s1, m0, m1);
+        if (angle) {
+            if (P->use_input_grad) {
+                interp_volume_linear(sgx, sgx_v, P->sny, nzx, sf, s, P->sy0, P->sdy, s0, s1);
+                interp_volume_linear(sgz, sgz_v, P->sny, nzx, sf, s, P->sy0, P->sdy, s0, s1);
+            }
+            leg_gradient(P, ST, sgx, sgz, gsx, gsz, t1, t2);
+        }
+        for (int ih = 0; ih < P->nh; ih++) {
+            const R h = RF(P->h0) + (R)ih * dh;
+            const R rpos = P->cmp ? (s + h) : h;
+            const float hf = P->h0 + (float)ih * (P->nh == 1 ? 0.0f : P->dh);
+            const float rposf = P->cmp ? (sf + hf) : hf;
+            float rf = 0.0f;
+            if (P->rny > 1 && P->rdy != 0.0f) rf = (rposf - P->ry0) / P->rdy;
+            const int iht = (P->rny > 1 && P->rdy != 0.0f) ? (int)floorf(rf) : 0;
+            double *dst = data + ((long)is * P->nh + ih) * nt;
+            for (int it = 0; it < nt; it++) { trace[it] = RF(0); dst[it] = 0.0; }
+            R trace_w = RF(1);
+            if (P->aperture_trace != -1) {
+                const R ad = R_FABS((R)(iht - ist));
+                if (ad >= (R)P->aperture_trace) continue;
+                if (P->aperture_trace_taper > 0) {
+                    const R tb = MAXV(RF(0), (R)(P->aperture_trace - P->aperture_trace_taper));
+                    if (ad > tb) {
+                        const R den = (R)P->aperture_trace - tb;
+                        if (den > RF(0)) trace_w = RF(0.5) * (RF(1) + R_COS(R_PI * ((ad - tb) / den)));
+                    }
+                }
+            }
+            int ig_offset = 0;
+            if (P->cig && !P->cig_is_angle) {
+                const float u = (hf - P->g0) / P->dg + 0.5f;
+                ig_offset = (ng <= 0 || P->dg <= 0.0f || !isfinite(hf)) ? -1 : (int)floorf(u);
+                if (ig_offset >= ng) ig_offset = -1;
+                if (ig_offset < 0) continue;
+            }
+            table_at(0, P, rtab, rder, rposf, rpos, P->ry0, P->rdy, P->rny, RT, RTx, s0, s1, m0, m1);
+            if (angle) {
+                if (P->use_input_grad) {
+                    interp_volume_linear(rgx, rgx_v, P->rny, nzx, rposf, rpos, P->ry0, P->rdy, s0, s1);
+                    interp_volume_linear(rgz, rgz_v, P->rny, nzx, rposf, rpos, P->ry0, P->rdy, s0, s1);
+                }
+                leg_gradient(P, RT, rgx, rgz, grx, grz, t1, t2);
+            }
+            for (long i = 0; i < nzx; i++) {
+                const int iz = (int)(i % nz);
+                const int ix = (int)((i - iz) / nz);
+                const R zdist = MAXV(R_FABS((R)iz * dz), MAXV(RF(1.0e-12), RF(1.0e-6) * R_FABS(dz)));
+                const R ximg = x0 + (R)ix * dxg;
+                const R dsx = R_FABS(s - ximg);
+                const R drx = R_FABS(rpos - ximg);
+                const R as_deg = R_ATAN(dsx / zdist) * RF(180.0) / R_PI;
+                const R ar_deg = R_ATAN(drx / zdist) * RF(180.0) / R_PI;
+                const R ws = MAXV(aperture_leg_weight(as_deg, RF(P->aper), RF(P->aperture_taper)),
+                                  aperture_floor_weight(dsx, RF(P->aperture_rmin), RF(P->aperture_rtaper)));
+                const R wr = MAXV(aperture_leg_weight(ar_deg, RF(P->aper), RF(P->aperture_taper)),
+                                  aperture_floor_weight(drx, RF(P->aperture_rmin), RF(P->aperture_rtaper)));
+                const R apw = ws * wr;
+                if (apw <= RF(0)) continue;
+                const R ti = ST[i] + RT[i] + tau;
+                const R tx = MAXV(R_FABS(STx[i] * ds), R_FABS(RTx[i] * dh));
+                if (angle) {
+                    const R ang = angle_from_grad(gsx[i], gsz[i], grx[i], grz[i], P->half_angle);
+                    const R aw = angle_taper_weight(ang, RF(P->angle_taper_start), RF(P->angle_taper_end)) *
+                                 depth_mute_weight(ang, iz, nz, RF(P->oazmin), RF(P->oazmax), RF(P->oaztaper)) *
+                                 trace_w * apw;
+                    if (aw <= RF(0)) continue;
+                    if (P->angle_interp) {
+                        int ig0 = -1, ig1 = -1;
+                        R w0 = RF(0), w1 = RF(0);
+                        if (!linear_bins(ang, g0, dg, ng, &ig0, &ig1, &w0, &w1)) continue;
+                        kirmig_spray(ti, tx * aal, aw * w0 * (R)image[(long)ig0 * nzx + i], trace, nt, dt, t0);
+                        if (ig1 != ig0 && w1 > RF(0))
+                            kirmig_spray(ti, tx * aal, aw * w1 * (R)image[(long)ig1 * nzx + i], trace, nt, dt, t0);
+                    } else {
+                        const int ig = nearest_bin(ang, g0, dg, ng);
+                        if (ig < 0) continue;
+                        kirmig_spray(ti, tx * aal, aw * (R)image[(long)ig * nzx + i], trace, nt, dt, t0);
+                    }
+                } else {
+                    const int ig = P->cig ? ig_offset : 0;
+                    kirmig_spray(ti, tx * aal, trace_w * apw * (R)image[(long)ig * nzx + i], trace, nt, dt, t0);
+                }
+            }
+            doubint(nt, trace);
+            for (int it = 0; it < nt; it++) dst[it] = (double)trace[it];
+        }
+    }
+    free(buf);
+    free(trace);
     return 0;
 }

@@ -65,6 +65,8 @@ def lib(fp64: bool = True):
         L.oracle_migrate_adj.argtypes = [ctypes.POINTER(OracleParams), fp, fp, fp, fp, fp,
                                          fp, fp, fp, fp, dp]
         L.oracle_migrate_adj.restype = ctypes.c_int
+        L.oracle_model_fwd.argtypes = [ctypes.POINTER(OracleParams), fp, fp, fp, fp, fp, fp, fp, fp, fp, dp]
+        L.oracle_model_fwd.restype = ctypes.c_int
         L.oracle_doubint.argtypes = [ctypes.c_int, fp, dp, ctypes.c_int, ctypes.c_float]
         L.oracle_mute.argtypes = [ctypes.c_int, fp] + [ctypes.c_float] * 7 + [ctypes.c_int]
         L.oracle_pick.argtypes = [ctypes.c_double, ctypes.c_double, dp, ctypes.c_int,
@@ -100,6 +102,21 @@ def migrate_adj(p: OracleParams, data, stable, sderiv, rtable, rderiv, grads=Non
     if rc != 0:
         raise RuntimeError("oracle_migrate_adj failed: %d" % rc)
     return img.reshape(p.ng, p.nx, p.nz)
+
+
+def model_fwd(p: OracleParams, image, stable, sderiv, rtable, rderiv, grads=None, fp64: bool = True) -> np.ndarray:
+    """Forward-modelled data [ns][nh][nt] (float64) from image [ng][nx][nz]
+    (kirchmig2d_cig adj=0)."""
+    L = lib(fp64)
+    image, stable, sderiv, rtable, rderiv = map(_f32, (image, stable, sderiv, rtable, rderiv))
+    g = [None] * 4 if grads is None else [_f32(x) for x in grads]
+    out = np.zeros(p.ns * p.nh * p.nt, dtype=np.float64)
+    rc = L.oracle_model_fwd(ctypes.byref(p), _fptr(image), _fptr(stable), _fptr(sderiv), _fptr(rtable),
+                            _fptr(rderiv), *[_fptr(x) for x in g],
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if rc != 0:
+        raise RuntimeError("oracle_model_fwd failed: %d" % rc)
+    return out.reshape(p.ns, p.nh, p.nt)
 
 
 def doubint(trace, isdiff=0, dt=1.0, fp64=True) -> np.ndarray:

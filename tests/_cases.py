@@ -28,6 +28,13 @@ class Golden:
     def grads(self):
         return self.npz["gradx"], self.npz["gradz"]
 
+    @property
+    def fwd_cases(self):
+        return sorted(self.meta.get("fwd", {}))
+
+    def fwd_data(self, name):
+        return np.load(os.path.join(GOLDEN, "golden_fwd.npz"))[name]
+
     def data(self, case):
         return self.npz["data_" + self.meta["cases"][case]["data"]]
 
@@ -81,6 +88,17 @@ def case_setup(gd: Golden, case: str):
     axis = kd.output_axis(kp, kd.geometry(**geom))
     use_grad = bool(gd.meta["cases"][case].get("grads"))
     return kp, geom, axis, oracle_params(kp, geom, axis, use_grad), use_grad
+
+
+def fwd_setup(gd: Golden, name: str):
+    """adj=0 fixture: (library params, geometry dict, axis, oracle params,
+    model image [ng][nx][nz])."""
+    import kirch_datuming_b200 as kd
+    f = gd.meta["fwd"][name]
+    kp = kd.params(*f["tokens"])
+    geom = gd.geometry_dict(f["image"])
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    return kp, geom, axis, oracle_params(kp, geom, axis), gd.image(f["image"])
 
 
 def oracle_image(gd: Golden, case: str, fp64=True):

@@ -7,7 +7,8 @@ tests/golden/golden.npz, with the parameter tokens of each case in
 tests/golden/cases.json.  Needs the reference tree (only in the build
 container); the tests only read the committed outputs.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # everything
+    python tests/golden/make_golden.py --forward  # only the adj=0 fixtures
 """
 from __future__ import annotations
 
@@ -69,8 +70,32 @@ DATA = {
 }
 
 
-def run(cmd, cwd):
-    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+# Forward modelling (adj=0, oracle/_ref/kirchmig2d_cig_fwd: the reference tool
+# with its model-read helper fixed, oracle/ref_fixes.cpp) of the adjoint images:
+# model = the reference's
+# image of the named case, data geometry = that case's input data.  Run with
+# one OpenMP thread (the reference sums per-thread trace buffers in thread
+# order, so the thread count changes the FP32 rounding).
+FWD = {
+    "fwd_base": dict(image="base", tokens=["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60",
+                                          "angle_step=1", "angle_n=61"]),
+    "fwd_cmp1_half": dict(image="cmp1_half", tokens=["cig=1", "mode=angle", "cmp=1", "half_angle=1",
+                                                     "angle_min=0", "angle_max=45", "angle_step=1.5",
+                                                     "angle_n=31"]),
+    "fwd_options": dict(image="options", tokens=["cig=1", "mode=angle", "cmp=0", "angle_interp=0", "type=linear",
+                                                 "tau=0.01", "antialias=0.5", "aperture=60", "aperture_taper=5",
+                                                 "aperture_rmin=0.1", "aperture_rtaper=0.05",
+                                                 "angle_taper_start=30", "angle_taper_end=50", "oazmin=70",
+                                                 "oazmax=40", "oaztaper=5", "angle_min=0", "angle_max=60",
+                                                 "angle_step=2", "angle_n=31", "aperture_trace=8",
+                                                 "aperture_trace_taper=4"]),
+    "fwd_offset": dict(image="offset", tokens=["cig=1", "mode=offset", "cmp=1"]),
+    "fwd_stack": dict(image="stack", tokens=["cig=0", "cmp=0"]),
+}
+
+
+def run(cmd, cwd, env=None):
+    r = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, env=env)
     if r.returncode != 0:
         raise RuntimeError("%s failed:\n%s\n%s" % (cmd, r.stdout[-3000:], r.stderr[-3000:]))
     return r.stdout + r.stderr
@@ -121,7 +146,50 @@ def main():
     with open(os.path.join(HERE, "cases.json"), "w") as f:
         json.dump(meta, f, indent=1, sort_keys=True)
     print("wrote", os.path.join(HERE, "golden.npz"))
+    forward()
+
+
+def forward():
+    """adj=0 fixtures (golden_fwd.npz, cases.json "fwd") from the committed
+    tables and images."""
+    gz = np.load(os.path.join(HERE, "golden.npz"))
+    with open(os.path.join(HERE, "cases.json")) as f:
+        meta = json.load(f)
+    t = meta["table"]
+    out = {}
+    meta["fwd"] = {}
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/time.rsf", gz["T"], t["n"], t["o"], t["d"])
+        rsf.write(f"{wd}/tds.rsf", gz["tds"], t["n"], t["o"], t["d"])
+        for name, c in FWD.items():
+            ic = meta["cases"][c["image"]]
+            d = meta["data"][ic["data"]]
+            img = gz["img_" + c["image"]]
+            rsf.write(f"{wd}/img.rsf", img, ic["n"], ic["o"], ic["d"])
+            args = ["migration=img.rsf", f"seismic_data=fwd_{name}.rsf", "stable=time.rsf", "sderiv=tds.rsf",
+                    "rtable=time.rsf", "rderiv=tds.rsf", "adj=0", f"nt={meta['nt']}", f"nh={d['nh']}",
+                    f"ns={d['ns']}", "t0=0", f"dt={meta['dt']}", f"h0={d['h0']}", f"dh={d['dh']}",
+                    f"s0={d['s0']}", f"ds={d['ds']}"] + c["tokens"]
+            run([f"{REF}/kirchmig2d_cig_fwd"] + args, wd, env=env)
+            # the reference writes the adj=0 data header without its second and
+            # third axes (dat->headers->ndim is left unset, src/kirchmig2d_cig.cpp:
+            # 906-920); the binary holds every trace, read with the parameters' shape
+            dat = np.fromfile(f"{wd}/fwd_{name}.rsf@", dtype="<f4")
+            assert dat.size == d["ns"] * d["nh"] * meta["nt"], (name, dat.size)
+            dat = dat.reshape(d["ns"], d["nh"], meta["nt"])
+            out[name] = dat
+            meta["fwd"][name] = dict(image=c["image"], data=ic["data"], tokens=["adj=0"] + c["tokens"],
+                                     n=[meta["nt"], d["nh"], d["ns"]],
+                                     sha256=hashlib.sha256(dat.tobytes()).hexdigest())
+    np.savez_compressed(os.path.join(HERE, "golden_fwd.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_fwd.npz"))
 
 
 if __name__ == "__main__":
-    main()
+    if "--forward" in sys.argv:
+        forward()
+    else:
+        main()

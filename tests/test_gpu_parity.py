@@ -228,3 +228,72 @@ def test_cli_end_to_end(golden, o64, tmp_path):
         os.chdir(cwd)
     _, img2 = rsf.read(str(tmp_path / "mig2.rsf"))
     assert np.array_equal(img, img2)
+
+
+# ------------------------------------------------------ forward (adj=0) path --
+@pytest.mark.parametrize("name", _cases.Golden().fwd_cases)
+def test_model_vs_oracle_and_reference(golden, name):
+    kp, geom, axis, op, model = _cases.fwd_setup(golden, name)
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    out = np.zeros((geom["ns"], geom["nh"], geom["nt"]), np.float32)
+    plan.model(model, out)
+    plan.close()
+    o64 = oracle.model_fwd(op, model, T, D, T, D, fp64=True)
+    ref = golden.fwd_data(name)
+    assert oracle.rel_l2(out, o64) <= TOL_FP64
+    ref_err = oracle.rel_l2(ref, o64)
+    assert oracle.rel_l2(out, ref) <= 1.5 * ref_err + 1e-6
+
+
+@pytest.mark.parametrize("name", _cases.Golden().fwd_cases)
+def test_model_migrate_dot_product(golden, name):
+    # <F m, d> = <m, F^T d> with the library's forward and adjoint operators
+    import torch
+    kp, geom, axis, op, model = _cases.fwd_setup(golden, name)
+    kp.direct_mute = 0
+    kp.isdiff = 0
+    T, D = golden.tables()
+    tT, tD = torch.from_numpy(T).cuda(), torch.from_numpy(D).cuda()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(tT, tD, tT, tD)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    m = torch.randn(model.shape, generator=g, device="cuda")
+    d = torch.randn((geom["ns"], geom["nh"], geom["nt"]), generator=g, device="cuda")
+    Fm = torch.zeros_like(d)
+    Ftd = torch.zeros_like(m)
+    plan.model(m, Fm)
+    plan.migrate(d, Ftd)
+    plan.close()
+    lhs = float((Fm.double() * d.double()).sum())
+    rhs = float((m.double() * Ftd.double()).sum())
+    assert abs(lhs - rhs) <= 1e-5 * float(Fm.double().norm() * d.double().norm())
+
+
+def test_cli_forward_modelling(golden, tmp_path):
+    # the drop-in executable with adj=0 (the reference's own adj=0 cannot read
+    # its model; see oracle/ref_fixes.cpp) writes a three-axis data file
+    name = "fwd_base"
+    f = golden.meta["fwd"][name]
+    ic = golden.meta["cases"][f["image"]]
+    dd = golden.meta["data"][ic["data"]]
+    t = golden.meta["table"]
+    T, D = golden.tables()
+    rsf.write(str(tmp_path / "time.rsf"), T, t["n"], t["o"], t["d"])
+    rsf.write(str(tmp_path / "tds.rsf"), D, t["n"], t["o"], t["d"])
+    rsf.write(str(tmp_path / "img.rsf"), golden.image(f["image"]), ic["n"], ic["o"], ic["d"])
+    args = [os.path.join(os.path.dirname(kd.library_path), "bin", "kirchmig2d_cig"), "migration=img.rsf",
+            "seismic_data=out.rsf", "stable=time.rsf", "sderiv=tds.rsf", "rtable=time.rsf", "rderiv=tds.rsf",
+            "nt=%d" % golden.meta["nt"], "nh=%d" % dd["nh"], "ns=%d" % dd["ns"], "t0=0", "dt=%g" % golden.meta["dt"],
+            "h0=%g" % dd["h0"], "dh=%g" % dd["dh"], "s0=%g" % dd["s0"], "ds=%g" % dd["ds"]] + f["tokens"]
+    r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    h, out = rsf.read(str(tmp_path / "out.rsf"))
+    assert h.n[:3] == [golden.meta["nt"], dd["nh"], dd["ns"]] and h.extra["label3"] == "Shot"
+    kp, geom, axis, op, model = _cases.fwd_setup(golden, name)
+    o64 = oracle.model_fwd(op, model, T, D, T, D, fp64=True)
+    assert oracle.rel_l2(out.reshape(o64.shape), o64) <= TOL_FP64
+    # direct_mute is an adj=1 option, with the reference's message
+    r = subprocess.run(args + ["direct_mute=1"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "requires adj=1" in (r.stdout + r.stderr)

@@ -69,3 +69,32 @@ def test_oracle_mute_profile():
     mid = (t > boundary) & (t < boundary + 0.2)
     u = (t[mid] - boundary) / 0.2
     assert np.allclose(out[mid], 0.5 * (1 - np.cos(np.pi * u)), atol=1e-6)
+
+
+# ------------------------------------------------------ forward (adj=0) path --
+@pytest.mark.parametrize("name", _cases.Golden().fwd_cases)
+def test_oracle_fp32_forward_bitexact_vs_reference(golden, name):
+    # oracle/_ref/kirchmig2d_cig_fwd: the reference tool, one OpenMP thread
+    kp, geom, axis, op, model = _cases.fwd_setup(golden, name)
+    T, D = golden.tables()
+    got = oracle.model_fwd(op, model, T, D, T, D, fp64=False).astype(np.float32)
+    assert np.array_equal(got, golden.fwd_data(name))
+
+
+@pytest.mark.parametrize("name", _cases.Golden().fwd_cases)
+def test_oracle_forward_is_adjoint_of_migration(golden, name):
+    # <F m, d> = <m, F^T d>: the FP64 forward oracle against the FP64 adjoint
+    # oracle (itself pinned bit-exact to the reference) with the forward's
+    # own settings (the forward applies neither the direct mute nor diff2)
+    kp, geom, axis, op, model = _cases.fwd_setup(golden, name)
+    op.direct_mute = 0
+    op.isdiff = 0
+    T, D = golden.tables()
+    rng = np.random.default_rng(3)
+    m = rng.standard_normal(model.shape).astype(np.float32)
+    d = rng.standard_normal((geom["ns"], geom["nh"], geom["nt"])).astype(np.float32)
+    Fm = oracle.model_fwd(op, m, T, D, T, D, fp64=True)
+    Ftd = oracle.migrate_adj(op, d, T, D, T, D, fp64=True)
+    lhs = float(np.dot(Fm.ravel(), d.astype(np.float64).ravel()))
+    rhs = float(np.dot(m.astype(np.float64).ravel(), Ftd.ravel()))
+    assert abs(lhs - rhs) <= 1e-10 * (np.linalg.norm(Fm) * np.linalg.norm(d))
