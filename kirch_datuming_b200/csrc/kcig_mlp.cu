@@ -105,7 +105,7 @@ struct SgNet {
     float fstep, vref, zsrc;
 };
 
-__device__ __forceinline__ float sg_sig(float z) { return 1.0f / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float sg_sig(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float sg_silu(float z) { return z * sg_sig(z); }
 __device__ __forceinline__ float sg_dsilu(float z)
 {
@@ -137,17 +137,16 @@ __device__ __forceinline__ void sg_stage_w(unsigned char *dst, const __nv_bfloat
     }
 }
 
-// Fourier features of one input for row r, columns [64h, 64h+64): pairs
-// k in [32h, 32h+32), column 2k = sin th_k, 2k+1 = cos th_k, by rotation
-// from th_{32h} in steps of fstep*u
-__device__ __forceinline__ void sg_features(unsigned char *act, int r, int h, float u, float fstep)
+// Fourier features of one input for row r, pairs [p0, p0 + np) (np a
+// multiple of 4): column 2k = sin th_k, 2k+1 = cos th_k, by rotation from
+// th_{p0} in steps of fstep*u
+__device__ __forceinline__ void sg_features(unsigned char *act, int r, int p0, int np, float u, float fstep)
 {
     const float d = fstep * u;
     float s, c, sd, cd;
-    sincosf(d * (float)(32 * h + 1), &s, &c);
+    sincosf(d * (float)(p0 + 1), &s, &c);
     sincosf(d, &sd, &cd);
-#pragma unroll
-    for (int g = 0; g < 8; g++) {
+    for (int g = 0; g < np / 4; g++) {
         uint32_t pk[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -157,25 +156,25 @@ __device__ __forceinline__ void sg_features(unsigned char *act, int r, int h, fl
             s = s2;
             c = c2;
         }
-        *reinterpret_cast<uint4 *>(act + tc::canon_off(r, 64 * h + 8 * g, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4 *>(act + tc::canon_off(r, 2 * p0 + 8 * g, 128)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
 }
 
 // d tau / d u of one input from 32*nq columns of d tau / d f starting at
-// column 64h (G, FP32 from TMEM): sum over its pairs of G_sin (k+1) fstep cos th - G_cos (k+1) fstep sin th
-__device__ __forceinline__ float sg_feature_grad(uint32_t tG, int h, int nq, float u, float fstep)
+// column c0 (G, FP32 from TMEM): sum over its pairs of G_sin (k+1) fstep cos th - G_cos (k+1) fstep sin th
+__device__ __forceinline__ float sg_feature_grad(uint32_t tG, int c0, int nq, float u, float fstep)
 {
     const float d = fstep * u;
     float s, c, sd, cd;
-    sincosf(d * (float)(32 * h + 1), &s, &c);
+    sincosf(d * (float)(c0 / 2 + 1), &s, &c);
     sincosf(d, &sd, &cd);
     float acc = 0.0f;
     for (int q = 0; q < nq; q++) {
         float v[32];
-        tc::tmem_ld32(tG + 64 * h + 32 * q, v);
+        tc::tmem_ld32(tG + c0 + 32 * q, v);
 #pragma unroll
         for (int j = 0; j < 16; j++) {
-            const float kf = (float)(32 * h + 16 * q + j + 1) * fstep;
+            const float kf = (float)(c0 / 2 + 16 * q + j + 1) * fstep;
             acc += kf * (v[2 * j] * c - v[2 * j + 1] * s);
             const float s2 = s * cd + c * sd, c2 = c * cd - s * sd;
             s = s2;
@@ -194,13 +193,14 @@ __device__ __forceinline__ void sg_store8(unsigned char *dst, int r, int col, co
                    *reinterpret_cast<uint32_t *>(&b2), *reinterpret_cast<uint32_t *>(&b3));
 }
 
-// forward epilogue: h = SiLU(acc + bias) as BF16 into dst (row r, this
-// thread's 64 columns)
-__device__ __forceinline__ void sg_epi_silu(uint32_t tacc, const float *bias, unsigned char *dst, int r, int h)
+// forward epilogue: h = SiLU(acc + bias) as BF16 into dst (row r, the
+// thread's columns cb .. cb + 32*nq)
+__device__ __forceinline__ void sg_epi_silu(uint32_t tacc, const float *bias, unsigned char *dst, int r, int cb,
+                                            int nq)
 {
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < nq; q++) {
         float v[32];
-        const int c0 = 64 * h + 32 * q;
+        const int c0 = cb + 32 * q;
         tc::tmem_ld32(tacc + c0, v);
 #pragma unroll
         for (int j = 0; j < 32; j++) v[j] = sg_silu(v[j] + bias[c0 + j]);
@@ -212,12 +212,12 @@ __device__ __forceinline__ void sg_epi_silu(uint32_t tacc, const float *bias, un
 // backward epilogue: g = G * SiLU'(z + bias) as BF16 into dst; returns the
 // sum over the thread's columns of bf16(g) * vdot (vdot may be null)
 __device__ __forceinline__ float sg_epi_back(uint32_t tG, uint32_t tZ, const float *bias, unsigned char *dst, int r,
-                                             int h, const float *vdot, float *colsum)
+                                             int cb, int nq, const float *vdot, float *colsum)
 {
     float dot = 0.0f;
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < nq; q++) {
         float G[32], Z[32];
-        const int c0 = 64 * h + 32 * q;
+        const int c0 = cb + 32 * q;
         tc::tmem_ld32(tG + c0, G);
         tc::tmem_ld32(tZ + c0, Z);
 #pragma unroll
@@ -285,17 +285,16 @@ struct SgFieldArgs {
 };
 constexpr int kSgFieldSmem = 7 * sg::TB;
 
-__global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
+__global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
 {
     using namespace sg;
     extern __shared__ __align__(1024) unsigned char dsm[];
     unsigned char *sW1z = dsm, *sW1x = dsm + TB, *sW2 = dsm + 2 * TB, *sW3 = dsm + 3 * TB, *sW4 = dsm + 4 * TB;
     unsigned char *actA = dsm + 5 * TB, *actB = dsm + 6 * TB;
-    // the dynamic tiles take 224 of the 227 KB a CTA may hold: the small
-    // arrays share the rest (the per-leg features alias the exchange rows)
+    // the dynamic tiles take 224 of the 227 KB a CTA may hold; the small
+    // per-leg arrays fit in the rest
     __shared__ float b1p[H], vleg[H];
-    __shared__ float xch[3][H];  // from the upper column half: out and d/du_xs partials, d/du_x
-    float *fx = xch[0], *dfx = xch[1];
+    __shared__ float fx[H], dfx[H];  // per-leg xs features and their derivatives
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tslot;
     const SgNet &n = a.net;
@@ -343,16 +342,23 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
                 dfx[2 * tid + 1] = -(float)(tid + 1) * n.fstep * sn;
             }
             __syncthreads();
-            if (tid < H) {
-                float acc = n.P[OFF_B1 + tid], accv = 0.0f;
-                const __nv_bfloat16 *w = n.W + OFF_W1 + (size_t)tid * FEAT;
-                for (int c = 0; c < H; c++) {
+            {   // four threads per output row, 32 columns each
+                const int o = tid >> 2, c0 = 32 * (tid & 3);
+                float acc = 0.0f, accv = 0.0f;
+                const __nv_bfloat16 *w = n.W + OFF_W1 + (size_t)o * FEAT;
+                for (int c = c0; c < c0 + 32; c++) {
                     const float wc = __bfloat162float(w[c]);
                     acc += wc * fx[c];
                     accv += wc * dfx[c];
                 }
-                b1p[tid] = acc;
-                vleg[tid] = accv;
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                accv += __shfl_xor_sync(0xffffffffu, accv, 1);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                accv += __shfl_xor_sync(0xffffffffu, accv, 2);
+                if ((tid & 3) == 0) {
+                    b1p[o] = n.P[OFF_B1 + o] + acc;
+                    vleg[o] = accv;
+                }
             }
             __syncthreads();
         }
@@ -362,8 +368,8 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
         const float zf = a.z0 + (float)iz * a.dz, xf = a.x0 + (float)ix * a.dx;
         const float uz = (zf - n.lo[1]) * n.sc[1] - 1.0f, ux = (xf - n.lo[2]) * n.sc[2] - 1.0f;
 
-        sg_features(actA, r, h, uz, n.fstep);
-        sg_features(actB, r, h, ux, n.fstep);
+        sg_features(actA, r, 16 * h, 16, uz, n.fstep);
+        sg_features(actB, r, 16 * h, 16, ux, n.fstep);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T1, aA, LBO_K, SBO_K, aW1z, LBO_K, SBO_K, 128, ID_KK, false);
@@ -371,21 +377,21 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_silu(D1, b1p, actA, r, h);
+        sg_epi_silu(D1, b1p, actA, r, 32 * h, 1);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T2, aA, LBO_K, SBO_K, aW2, LBO_K, SBO_K, 128, ID_KK, false);
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_silu(D2, bias2, actB, r, h);
+        sg_epi_silu(D2, bias2, actB, r, 32 * h, 1);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T3, aB, LBO_K, SBO_K, aW3, LBO_K, SBO_K, 128, ID_KK, false);
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_silu(D3, bias3, actA, r, h);
+        sg_epi_silu(D3, bias3, actA, r, 32 * h, 1);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T4, aA, LBO_K, SBO_K, aW4, LBO_K, SBO_K, 128, ID_KK, false);
@@ -394,20 +400,17 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
         if (!(ok = sg_wait(&bar, phase))) break;
         float out_part;
         {   // output layer and the start of the backward pass (d tau / d out = 1)
-            float part = 0.0f;
-            for (int q = 0; q < 2; q++) {
-                float v[32];
-                const int c0 = 64 * h + 32 * q;
-                tc::tmem_ld32(D4 + c0, v);
+            float part = 0.0f, v[32];
+            const int c0 = 32 * h;
+            tc::tmem_ld32(D4 + c0, v);
 #pragma unroll
-                for (int jj = 0; jj < 32; jj++) {
-                    const float z = v[jj] + bias4[c0 + jj];
-                    part += sg_silu(z) * wo[c0 + jj];
-                    v[jj] = wo[c0 + jj] * sg_dsilu(z);
-                }
-#pragma unroll
-                for (int g = 0; g < 4; g++) sg_store8(actB, r, c0 + 8 * g, v + 8 * g);
+            for (int jj = 0; jj < 32; jj++) {
+                const float z = v[jj] + bias4[c0 + jj];
+                part += sg_silu(z) * wo[c0 + jj];
+                v[jj] = wo[c0 + jj] * sg_dsilu(z);
             }
+#pragma unroll
+            for (int g = 0; g < 4; g++) sg_store8(actB, r, c0 + 8 * g, v + 8 * g);
             out_part = part;
         }
         sg_sync_for_mma();
@@ -416,21 +419,21 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_back(D4, D3, bias3, actA, r, h, nullptr, nullptr);
+        sg_epi_back(D4, D3, bias3, actA, r, 32 * h, 1, nullptr, nullptr);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T3, aA, LBO_K, SBO_K, aW3, LBO_M, SBO_M, 128, ID_KM, false);
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_back(D3, D2, bias2, actB, r, h, nullptr, nullptr);
+        sg_epi_back(D3, D2, bias2, actB, r, 32 * h, 1, nullptr, nullptr);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T2, aB, LBO_K, SBO_K, aW2, LBO_M, SBO_M, 128, ID_KM, false);
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        const float xs_part = sg_epi_back(D2, D1, b1p, actA, r, h, vleg, nullptr);
+        const float xs_part = sg_epi_back(D2, D1, b1p, actA, r, 32 * h, 1, vleg, nullptr);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
             tc::gemm(T3, aA, LBO_K, SBO_K, aW1z, LBO_M, SBO_M, 128, ID_KM, false);
@@ -438,20 +441,31 @@ __global__ void __launch_bounds__(256, 1) k_sg_fields(SgFieldArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        // the lower half takes d tau/d u_z (all of G0z), the upper d tau/d u_x
-        const float gzx = h == 0 ? sg_feature_grad(D3, 0, 4, uz, n.fstep) : sg_feature_grad(D4, 0, 4, ux, n.fstep);
-        if (h == 1) {
-            xch[0][r] = out_part;
-            xch[1][r] = xs_part;
-            xch[2][r] = gzx;
+        // each column quarter: its part of d tau/d u_z (G0z) and d tau/d u_x
+        // (G0x); the four partials of each quantity meet in actB, which no
+        // MMA reads any more in this item
+        {
+            const float gz_part = sg_feature_grad(D3, 32 * h, 1, uz, n.fstep);
+            const float gx_part = sg_feature_grad(D4, 32 * h, 1, ux, n.fstep);
+            float *xq = reinterpret_cast<float *>(actB);  // [quantity][quarter][row]
+            xq[(0 * 4 + h) * 128 + r] = out_part;
+            xq[(1 * 4 + h) * 128 + r] = xs_part;
+            xq[(2 * 4 + h) * 128 + r] = gz_part;
+            xq[(3 * 4 + h) * 128 + r] = gx_part;
         }
         tc::fence_before();
         __syncthreads();
         if (h == 0 && valid) {
-            const float tau = 1.0f + out_part + xch[0][r] + bo;
-            const float gxs = (xs_part + xch[1][r]) * n.sc[0];
-            const float gz = gzx * n.sc[1];
-            const float gx = xch[2][r] * n.sc[2];
+            const float *xq = reinterpret_cast<const float *>(actB);
+            float sum[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                sum[k] = (xq[(k * 4) * 128 + r] + xq[(k * 4 + 1) * 128 + r]) +
+                         (xq[(k * 4 + 2) * 128 + r] + xq[(k * 4 + 3) * 128 + r]);
+            const float tau = 1.0f + sum[0] + bo;
+            const float gxs = sum[1] * n.sc[0];
+            const float gz = sum[2] * n.sc[1];
+            const float gx = sum[3] * n.sc[2];
             float T0, bxs, bz, bx;
             sg_background(n, xs, zf, xf, T0, bxs, bz, bx);
             const float T = T0 * tau;
@@ -560,7 +574,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
         // layer 1, three feature chunks
         for (int c = 0; c < 3 && ok; c++) {
             sg_stage_w(wbuf, n.W + OFF_W1, FEAT, 128 * c);
-            sg_features(fbuf, r, h, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
+            sg_features(fbuf, r, 32 * h, 32, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
             sg_sync_for_mma();
             if (warp == 0 && tc::elect_one()) {
                 tc::gemm(T1, aF, LBO_K, SBO_K, aW, LBO_K, SBO_K, 128, ID_KK, c > 0);
@@ -569,7 +583,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
             ok = sg_wait(&bar, phase);
         }
         if (!ok) break;
-        sg_epi_silu(D1, bias[0], H1, r, h);
+        sg_epi_silu(D1, bias[0], H1, r, 64 * h, 2);
         sg_stage_w(wbuf, n.W + OFF_W2, H, 0);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
@@ -577,7 +591,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_silu(D2, bias[1], H2, r, h);
+        sg_epi_silu(D2, bias[1], H2, r, 64 * h, 2);
         sg_stage_w(wbuf, n.W + OFF_W3, H, 0);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
@@ -585,7 +599,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_silu(D3, bias[2], H3, r, h);
+        sg_epi_silu(D3, bias[2], H3, r, 64 * h, 2);
         sg_stage_w(wbuf, n.W + OFF_W4, H, 0);
         sg_sync_for_mma();
         if (warp == 0 && tc::elect_one()) {
@@ -686,14 +700,14 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
                 sg_dump_tile(a.stages + 5 * 16384, gbuf);
                 sg_dump_tile(a.stages + 6 * 16384, wbuf);
             }
-            sg_epi_back(Dk, Dpk, bias[2 - k], gbuf, r, h, nullptr,
+            sg_epi_back(Dk, Dpk, bias[2 - k], gbuf, r, 64 * h, 2, nullptr,
                         MODE == SG_TRAIN ? colsum[2 - k] : nullptr);
         }
         if (!ok) break;
         // layer 1: weight gradient per feature chunk (TRAIN) or input gradient (EVAL)
         for (int c = 0; c < 3 && ok; c++) {
             if (MODE == SG_TRAIN) {
-                sg_features(fbuf, r, h, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
+                sg_features(fbuf, r, 32 * h, 32, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
                 sg_sync_for_mma();
                 if (warp == 0 && tc::elect_one()) {
                     tc::gemm(T1, aG, LBO_M, SBO_M, aF, LBO_M, SBO_M, 128, ID_MM, false);
@@ -718,7 +732,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
                 }
                 if (!(ok = sg_wait(&bar, phase))) break;
                 if (c == 0) sg_dump(a.stages ? a.stages + 4 * 16384 : nullptr, D1, r, h);
-                red[1 + c][h][r] = sg_feature_grad(D1, h, 2, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
+                red[1 + c][h][r] = sg_feature_grad(D1, 64 * h, 2, c == 0 ? u0 : (c == 1 ? u1 : u2), n.fstep);
             }
         }
         if (!ok) break;
@@ -833,7 +847,7 @@ static int launch_sg_fields(const SgNet &net, const LegInterp *legs, int nlegs, 
     const long long items = (long long)nlegs * ((g.nz * g.nx + 127) / 128);
     const int grid = (int)std::min<long long>(sms, items);
     KCIG_TRY(set_dyn_smem((const void *)k_sg_fields, kSgFieldSmem));
-    k_sg_fields<<<grid, 256, kSgFieldSmem, st>>>(a);
+    k_sg_fields<<<grid, 512, kSgFieldSmem, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
