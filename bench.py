@@ -62,7 +62,7 @@ def make_workload(seed: int):
     from kirch_datuming_b200 import synth
     v, refl = synth.five_layer_salt(NZ, NX, DZ, DZ, seed=7)
     vel = torch.from_numpy(v).cuda()
-    T, D = kd.eikonal_tables(vel, DZ, DZ, NPOS, 0.0, DP, iterations=3)
+    T, D = kd.eikonal_tables(vel, DZ, DZ, NPOS, 0.0, DP)
     g = synth.Geometry(nz=NZ, nx=NX, dz=DZ, dx=DZ, z0=0, x0=0, ns=NPOS, s0=0.0, ds=DP, nh=NPOS, h0=0.0, dh=DP,
                        cmp=0, nt=NT, dt=DT, t0=0.0, npos=NPOS, p0=0.0, dp=DP)
     amps = synth.reflectivities(len(refl), seed)
@@ -364,7 +364,7 @@ def batched_section(steps: int, warmup: int, seed: int = 21):
     for w, (r0, r1) in enumerate(rows):
         nzw = r1 - r0
         vw = torch.from_numpy(np.ascontiguousarray(vel[:, r0:r1])).cuda()
-        T, D = kd.eikonal_tables(vw, dz, dz, nx, 0.0, dz, iterations=3)
+        T, D = kd.eikonal_tables(vw, dz, dz, nx, 0.0, dz)
         g = synth.Geometry(nz=nzw, nx=nx, dz=dz, dx=dz, z0=0.0, x0=0.0, ns=nshot, s0=0.0, ds=4.0 / (nshot - 1),
                            nh=nrg, h0=0.0, dh=dh, cmp=0, nt=nt_max, dt=0.001, t0=0.0, npos=nx, p0=0.0, dp=dz)
         cube = synth.shot_gathers(T, g, [(np.full(nx, 20), amps[w])], 20.0, seed=seed + w, noise_on_device=True)
@@ -551,7 +551,7 @@ def main():
         "config": {"workload": WORKLOAD, "pairs_per_gpu_step": pairs, "parallelism": "dp%d (shots per rank, "
                    "image all-reduce)" % world if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (1.9 GB traces, 3.1 GB tables per step)",
-                   "tables": "GPU fast-sweeping eikonal (kcig_eikonal_tables), 400 positions"},
+                   "tables": "GPU eikods2d tables (kcig_eikods: order 2, tds1), 400 positions"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "kernel": "k_sum", "kernel_ms": ksum_ms,
                      "algorithmic_bytes_per_pair": B_PAIR,

@@ -166,14 +166,47 @@ int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry *g, const 
                             int is_source, double pos, double *T, float *Tx, double *phi, float *w,
                             void *stream);
 
-/* Traveltime tables for the migration, the role of eikods2d
- * (src/eikods2d.cpp:149-765, SERECKIRCH/src/eikods.cpp:66-211): sources at
- * depth zsrc and lateral positions p0 + k*dp (k < npos); vel [nx][nz] in
- * km/s (device).  Writes time [npos][nx][nz] and, if deriv is not NULL, the
- * derivative of time with respect to the source position [npos][nx][nz]
- * (device).  First-order fast sweeping (iterations x 4 sweeps) with the
- * straight-ray times inside the (b1, b2) box around the source; the position
- * derivative is the centred difference of neighbouring positions' tables. */
+/* Options of kcig_eikods (the eikods2d parameters of src/eikods2d.cpp:149-300). */
+typedef struct kcig_eikods_opts {
+    int order;            /* 1 or 2: accuracy order of the upwind update (order=, default 2) */
+    int b1, b2;           /* constant-slowness box half-widths in samples along depth and lateral
+                             (b1=, b2=; values below 1 become 1) */
+    int l;                /* source perturbation axis of tdl1/tds1: 1 lateral (l=, default), 0 depth */
+    int vel_is_slowness2; /* 0: vel is velocity (vel=1, default); 1: slowness squared (vel=0) */
+    int max_iter;         /* bound on sweep iterations (4 sweeps each) per source; 0 = 256 */
+} kcig_eikods_opts;
+
+/* First-arrival traveltime tables, the computation of eikods2d
+ * (src/eikods2d.cpp:149-765; SERECKIRCH/src/eikods.cpp:66-211 and
+ * neighbors.cpp) on a 2-D grid: vel [nx][nz] (device, depth fastest) with
+ * origins o1 (depth), o2 (lateral), samplings d1, d2, and the third-axis
+ * origin/sampling o3/d3 of the velocity header (o3=0, d3=1 for a 2-D file);
+ * shots [nshot][3] (host) as in the shot file: depth, lateral, third axis.
+ * Writes time [nshot][nx][nz] (device) and, where not NULL, tdl1/tds1 (the
+ * first derivatives with respect to the source position; both or neither),
+ * gradz/gradx (the branch-aware upwind gradients of eikods2d.cpp:30-68), all
+ * [nshot][nx][nz] (device), and iters [nshot] (host): the sweeps each source
+ * took.  nz in 3..1800, nx >= 3.  The same local problem as the marching
+ * code, solved by sweeps to the fixed point: identical results for order 1,
+ * within ~1e-4 s for order 2 (whose marching result depends on the heap's
+ * acceptance order).  KCIG_ERR_DEVICE if a source has no fixed point within
+ * max_iter. */
+int kcig_eikods(const float *vel, int nz, int nx, float o1, float o2, float d1, float d2, float o3, float d3,
+                const float *shots, int nshot, const kcig_eikods_opts *opt, float *time, float *tdl1,
+                float *tds1, float *gradz, float *gradx, int *iters, void *stream);
+
+/* The drop-in eikods2d (src/eikods2d.cpp:149-765) for 2-D velocity files:
+ * same keys (in= out= tdl1= tds1= shotfile= gradz= gradx= order= b1= b2= br1=
+ * br2= vel= l= zshot= yshot= xshot=), required outputs, error texts and
+ * output headers; the tables are computed by kcig_eikods.  efmm=1,
+ * plane-wave sources, tdl2=/tds2= and 3-D volumes return
+ * KCIG_ERR_UNSUPPORTED.  Returns 0 or a KCIG_ERR_* (message logged). */
+int kcig_run_eikods_cli(int argc, char **argv);
+
+/* Tables for sources at depth zsrc and lateral positions p0 + k*dp
+ * (k < npos), as the shot files of shotgen give them: kcig_eikods with
+ * order 2, boxes (b1, b2), l = 1; deriv (may be NULL) receives tds1.
+ * iterations bounds the sweep iterations (0 = 256). */
 int kcig_eikonal_tables(const float *vel, int nz, int nx, float dz, float dx, float z0, float x0,
                         int npos, float p0, float dp, float zsrc, int b1, int b2, int iterations,
                         float *time, float *deriv, void *stream);

@@ -15,11 +15,13 @@ import os
 import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
-           "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "library_path", "cli_path"]
+           "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "eikods", "library_path",
+           "cli_path", "eikods_cli_path"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(_HERE, "libkcig.so")
 cli_path = os.path.join(_HERE, "bin", "kirchmig2d_cig")
+eikods_cli_path = os.path.join(_HERE, "bin", "eikods2d")
 
 MEM_HOST = 0
 MEM_DEVICE = 1
@@ -35,6 +37,12 @@ class KcigError(RuntimeError):
 class SurrogateConfig(ctypes.Structure):
     _fields_ = [("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("fmax", ctypes.c_float),
                 ("vref", ctypes.c_float), ("zsrc", ctypes.c_float)]
+
+
+class EikodsOpts(ctypes.Structure):
+    """kcig_eikods_opts (include/kcig.h)."""
+    _fields_ = [("order", ctypes.c_int), ("b1", ctypes.c_int), ("b2", ctypes.c_int), ("l", ctypes.c_int),
+                ("vel_is_slowness2", ctypes.c_int), ("max_iter", ctypes.c_int)]
 
 
 class Shot(ctypes.Structure):
@@ -96,6 +104,9 @@ def lib():
         L.kcig_eikonal_tables.argtypes = [fp, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 4 + [
             ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
             fp, fp, vp]
+        L.kcig_eikods.argtypes = ([fp, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 6
+                                  + [fp, ctypes.c_int, ctypes.POINTER(EikodsOpts)] + [fp] * 5
+                                  + [ctypes.POINTER(ctypes.c_int), vp])
         L.kcig_tc_selftest.argtypes = [vp, vp, fp, vp, vp]
         SC = ctypes.POINTER(SurrogateConfig)
         L.kcig_surrogate_create.argtypes = [SC, ctypes.c_ulonglong, ctypes.POINTER(vp)]
@@ -326,10 +337,47 @@ def leg_fields_device(plan: Plan, is_source: int, pos: float):
     return T, Tx, phi, w
 
 
+def eikods(vel, d1: float, d2: float, shots, o1: float = 0.0, o2: float = 0.0, o3: float = 0.0, d3: float = 1.0,
+           order: int = 2, b1: int = 2, b2: int = 2, l: int = 1, vel_is_slowness2: bool = False,
+           max_iter: int = 0, derivs: bool = True, grads: bool = False):
+    """eikods2d's tables on the GPU (kcig_eikods).
+
+    vel: CUDA float32 tensor [nx][nz] (velocity, or slowness squared with
+    vel_is_slowness2); shots: [nshot][3] (depth, lateral, third axis) as in
+    an eikods2d shot file.  Returns a dict of CUDA tensors [nshot][nx][nz]:
+    'time', and 'tdl1'/'tds1' (derivs), 'gradz'/'gradx' (grads), plus
+    'sweeps' (numpy [nshot], the sweeps each source took)."""
+    import numpy as np
+    import torch
+    if not (vel.is_cuda and vel.dtype == torch.float32 and vel.is_contiguous() and vel.dim() == 2):
+        raise ValueError("vel must be a contiguous CUDA float32 tensor [nx][nz]")
+    nx, nz = vel.shape
+    sh = np.ascontiguousarray(np.asarray(shots, dtype=np.float32).reshape(-1, 3))
+    ns = sh.shape[0]
+    new = lambda: torch.empty((ns, nx, nz), dtype=torch.float32, device=vel.device)  # noqa: E731
+    out = {"time": new()}
+    if derivs:
+        out["tdl1"], out["tds1"] = new(), new()
+    if grads:
+        out["gradz"], out["gradx"] = new(), new()
+    o = EikodsOpts(order, b1, b2, l, 1 if vel_is_slowness2 else 0, max_iter)
+    sweeps = np.zeros(ns, np.int32)
+    ptr = lambda k: out[k].data_ptr() if k in out else None  # noqa: E731
+    st = torch.cuda.current_stream().cuda_stream
+    _check(lib().kcig_eikods(vel.data_ptr(), nz, nx, o1, o2, d1, d2, o3, d3, sh.ctypes.data, ns, ctypes.byref(o),
+                             ptr("time"), ptr("tdl1"), ptr("tds1"), ptr("gradz"), ptr("gradx"),
+                             sweeps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.c_void_p(st)))
+    out["sweeps"] = sweeps
+    return out
+
+
 def eikonal_tables(vel, dz: float, dx: float, npos: int, p0: float, dp: float, z0: float = 0.0,
-                   x0: float = 0.0, zsrc: float = 0.0, b1: int = 2, b2: int = 2, iterations: int = 3,
+                   x0: float = 0.0, zsrc: float = 0.0, b1: int = 2, b2: int = 2, iterations: int = 0,
                    deriv: bool = True):
-    """Traveltime tables on the GPU for sources at p0 + k*dp (k < npos).
+    """Traveltime tables on the GPU for sources at depth zsrc and lateral
+    positions p0 + k*dp (k < npos): eikods with order 2 (the eikods2d
+    default); deriv is tds1.  iterations bounds the sweep iterations (0 =
+    the library default).
 
     vel: CUDA float32 tensor [nx][nz] (km/s).  Returns (time, deriv) CUDA
     tensors [npos][nx][nz] (deriv None when not requested)."""

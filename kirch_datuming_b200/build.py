@@ -4,7 +4,8 @@
 
 produces, in-tree,
     kirch_datuming_b200/libkcig.so          the C-ABI library (include/kcig.h)
-    kirch_datuming_b200/bin/kirchmig2d_cig  the drop-in command-line tool
+    kirch_datuming_b200/bin/kirchmig2d_cig  the drop-in migration / modelling tool
+    kirch_datuming_b200/bin/eikods2d        the drop-in table generator
 compiled for sm_100a only (nvcc cross-compiles; no GPU needed to build).
 """
 from __future__ import annotations
@@ -19,8 +20,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libkcig.so")
 CLI = os.path.join(PKG, "bin", "kirchmig2d_cig")
+EIK_CLI = os.path.join(PKG, "bin", "eikods2d")
 
-SOURCES = ["kcig_kernels.cu", "kcig_plan.cu", "kcig_eikonal.cu", "kcig_mlp.cu", "kcig_params.cpp", "kcig_rsf.cpp", "kcig_cli.cpp"]
+SOURCES = ["kcig_kernels.cu", "kcig_plan.cu", "kcig_eikods.cu", "kcig_mlp.cu", "kcig_params.cpp", "kcig_rsf.cpp", "kcig_cli.cpp",
+           "kcig_eikods_cli.cpp"]
 HEADERS = ["kcig_common.h", "kcig_tc.h", "kcig_aperture.h", "kcig_par.h", "kcig_rsf.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -55,15 +58,15 @@ def build(force: bool = False, verbose: bool = False) -> None:
             raise RuntimeError("nvcc failed:\n" + r.stdout[-6000:] + r.stderr[-6000:])
         if verbose:
             sys.stderr.write(r.stderr)
-    main = os.path.join(CSRC, "kirchmig2d_cig_main.cpp")
-    if force or _stale(CLI, [LIB, main]):
-        os.makedirs(os.path.dirname(CLI), exist_ok=True)
-        cmd = [nvcc(), *ARCH, *host, "-O2", "-std=c++17", "-o", CLI, main, "-L" + PKG, "-lkcig",
-               "-Xlinker", "-rpath=$ORIGIN/.."]
-        r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True, env=env)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc (cli) failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
-
+    for exe, src in ((CLI, "kirchmig2d_cig_main.cpp"), (EIK_CLI, "eikods2d_main.cpp")):
+        main = os.path.join(CSRC, src)
+        if force or _stale(exe, [LIB, main]):
+            os.makedirs(os.path.dirname(exe), exist_ok=True)
+            cmd = [nvcc(), *ARCH, *host, "-O2", "-std=c++17", "-o", exe, main, "-L" + PKG, "-lkcig",
+                   "-Xlinker", "-rpath=$ORIGIN/.."]
+            r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True, env=env)
+            if r.returncode != 0:
+                raise RuntimeError("nvcc (%s) failed:\n" % src + r.stdout[-4000:] + r.stderr[-4000:])
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)

@@ -153,6 +153,46 @@ def leg_fields(p: OracleParams, is_source: int, tab, der, pos, grads=(None, None
     return outs
 
 
+_eik = None
+
+
+def eikods(vel, d1, d2, shots, o1=0.0, o2=0.0, o3=0.0, d3=1.0, b1=2, b2=2, order=2, l=1, method=0,
+           vel_is_s2=False, max_iter=256, grads=False):
+    """eikods2d's tables on the CPU (kcig_eikods_oracle.c).  vel [nx][nz];
+    shots [nshot][3] (depth, lateral, third axis).  method 0: the marching
+    solver eikods2d runs; 1: sweeps to the fixed point of the same update.
+    Returns a dict of float32 arrays [nshot][nx][nz] (time, tdl1, tds1 and,
+    with grads, gradz/gradx) plus 'sweeps' [nshot]."""
+    global _eik
+    if _eik is None:
+        path = os.path.join(HERE, "libeikods_oracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError("oracle not built: run `make -C oracle` (%s)" % path)
+        _eik = ctypes.CDLL(path)
+        fp = ctypes.POINTER(ctypes.c_float)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _eik.oracle_eikods.argtypes = ([ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [fp, ctypes.c_int, fp]
+                                       + [ctypes.c_int] * 6 + [fp] * 5 + [ip])
+        _eik.oracle_eikods.restype = ctypes.c_int
+    vel = _f32(vel)
+    nx, nz = vel.shape
+    shots = _f32(np.asarray(shots, np.float32).reshape(-1, 3))
+    ns = shots.shape[0]
+    out = {k: np.zeros((ns, nx, nz), np.float32) for k in ("time", "tdl1", "tds1")}
+    if grads:
+        out["gradz"] = np.zeros((ns, nx, nz), np.float32)
+        out["gradx"] = np.zeros((ns, nx, nz), np.float32)
+    sweeps = np.zeros(ns, np.int32)
+    rc = _eik.oracle_eikods(int(method), nz, nx, o1, o2, d1, d2, o3, d3, _fptr(vel), int(vel_is_s2), _fptr(shots),
+                            ns, b1, b2, order, l, max_iter, _fptr(out["time"]), _fptr(out["tdl1"]),
+                            _fptr(out["tds1"]), _fptr(out.get("gradz")), _fptr(out.get("gradx")),
+                            sweeps.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != 0:
+        raise RuntimeError("oracle_eikods failed: %d" % rc)
+    out["sweeps"] = sweeps
+    return out
+
+
 def rel_l2(a, b) -> float:
     """||a-b|| / ||b|| in double, the reference comparator (src/rsf_l2cmp.cpp:9-10)."""
     a = np.asarray(a, dtype=np.float64).ravel()

@@ -9,6 +9,7 @@ container); the tests only read the committed outputs.
 
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py --forward  # only the adj=0 fixtures
+    python tests/golden/make_golden.py --eikods   # only the table-generator fixtures
 """
 from __future__ import annotations
 
@@ -188,8 +189,45 @@ def forward():
     print("wrote", os.path.join(HERE, "golden_fwd.npz"))
 
 
+# table generator: the five-layer salt model on a 31 x 61 grid of 10 m, shots
+# off the grid nodes and below the surface, three parameter sets
+EIK_NZ, EIK_NX = 31, 61
+EIK_SHOTS = [(0.0, 0.05, 0.0), (0.0, 0.2345, 0.0), (0.1, 0.4, 0.0), (0.0, 0.595, 0.0), (0.25, 0.31, 0.0)]
+EIK_RUNS = {"o2": ["order=2"], "o1": ["order=1"], "o2_l0": ["order=2", "l=0"]}
+
+
+def eikods():
+    """eikods2d fixtures (golden_eikods.npz, cases.json "eikods")."""
+    with open(os.path.join(HERE, "cases.json")) as f:
+        meta = json.load(f)
+    v, _ = synth.five_layer_salt(EIK_NZ, EIK_NX, DZ, DZ)
+    shots = np.asarray(EIK_SHOTS, np.float32)
+    out = {"vel": v, "shots": shots}
+    meta["eikods"] = {"nz": EIK_NZ, "nx": EIK_NX, "d": DZ, "b1": 2, "b2": 2, "runs": EIK_RUNS}
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/vel.rsf", v, [EIK_NZ, EIK_NX], [0, 0], [DZ, DZ])
+        rsf.write(f"{wd}/sht.rsf", shots, [3, len(EIK_SHOTS)], [0, 0], [1, 1])
+        for name, toks in EIK_RUNS.items():
+            run([f"{REF}/eikods2d", "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf",
+                 "tds1=tds.rsf", "gradz=gz.rsf", "gradx=gx.rsf", "b1=2", "b2=2"] + toks, wd, env=env)
+            for f, k in (("time", "time"), ("tdl", "tdl1"), ("tds", "tds1"), ("gz", "gradz"), ("gx", "gradx")):
+                if name == "o2_l0" and k not in ("tdl1", "tds1"):
+                    continue  # l only changes the derivatives
+                h, a = rsf.read(f"{wd}/{f}.rsf")
+                out[f"{name}_{k}"] = a.reshape(len(EIK_SHOTS), EIK_NX, EIK_NZ)
+                if name == "o2" and k == "time":
+                    meta["eikods"]["header"] = dict(n=h.n[:3], o=h.o[:3], d=h.d[:3])
+    np.savez_compressed(os.path.join(HERE, "golden_eikods.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_eikods.npz"))
+
+
 if __name__ == "__main__":
     if "--forward" in sys.argv:
         forward()
+    elif "--eikods" in sys.argv:
+        eikods()
     else:
         main()

@@ -24,10 +24,10 @@ def test_eikonal_linear_vz_accuracy():
     nz, nx, dz = 121, 241, 0.01
     vel = torch.from_numpy(synth.velocity_linear_vz(nz, nx, dz)).cuda()
     npos, p0, dp = 5, 0.4, 0.35
-    T, D = kd.eikonal_tables(vel, dz, dz, npos, p0, dp, iterations=2)
+    T, D = kd.eikonal_tables(vel, dz, dz, npos, p0, dp)
     T = T.cpu().numpy()
-    # first-order upwind sweeping: the relative error is largest beside the
-    # (b1=b2=2) source box and decays with distance
+    # the relative error of the upwind update is largest beside the (b1=b2=2)
+    # source box and decays with distance
     z, x = np.arange(nz) * dz, np.arange(nx) * dz
     zz, xx = np.meshgrid(z, x)
     for j in range(npos):
