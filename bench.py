@@ -238,6 +238,69 @@ def cpu_sample(threads: int, tables=None):
         shutil.rmtree(wd, ignore_errors=True)
 
 
+# ---------------------------------------------------------- tables section ---
+def tables_section(steps: int, warmup: int, threads: int):
+    """The table generator on the migration's grid: kcig_eikods (order 2,
+    time + tdl1 + tds1, the eikods2d outputs the migration reads) for the
+    400 surface positions, device time per call with CUDA events; beside it
+    the reference eikods2d on a bounded sample of the same positions with all
+    host threads, and the deviation of the GPU tables from the reference's on
+    that sample (order 2: the marching result depends on the heap's
+    acceptance order, see kcig_eikods)."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import rsf, synth
+    v, _ = synth.five_layer_salt(NZ, NX, DZ, DZ, seed=7)
+    vel = torch.from_numpy(v).cuda()
+    shots = np.zeros((NPOS, 3), np.float32)
+    shots[:, 1] = np.arange(NPOS, dtype=np.float32) * np.float32(DP)
+    for _ in range(max(1, min(warmup, 1))):
+        r = kd.eikods(vel, DZ, DZ, shots)
+    del r
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = max(1, min(steps, 3))
+    e0.record()
+    for _ in range(n):
+        r = kd.eikods(vel, DZ, DZ, shots)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    sweeps = r["sweeps"]
+    out = {"workload": "five-layer salt 601x1601@10m, %d surface sources every %g km: time, tdl1, tds1" % (NPOS, DP),
+           "value": NPOS / (ms / 1e3), "unit": "tables/s", "ms_per_call": ms,
+           "sweeps": {"min": int(sweeps.min()), "mean": float(sweeps.mean()), "max": int(sweeps.max())}}
+    if os.path.exists(REF_EIK):
+        nsmp = max(8, threads)
+        idx = np.linspace(0, NPOS - 1, nsmp).round().astype(int)
+        wd = tempfile.mkdtemp(prefix="kcig_eik_")
+        try:
+            rsf.write(f"{wd}/vel.rsf", v, [NZ, NX], [0, 0], [DZ, DZ])
+            rsf.write(f"{wd}/sht.rsf", shots[idx], [3, nsmp], [0, 0], [1, 1])
+            t = time.perf_counter()
+            subprocess.run([REF_EIK, "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf",
+                            "tds1=tds.rsf", "b1=2", "b2=2"], cwd=wd, check=True, capture_output=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+            el = time.perf_counter() - t
+            _, Tr = rsf.read(f"{wd}/time.rsf")
+            _, Dr = rsf.read(f"{wd}/tds.rsf")
+        finally:
+            shutil.rmtree(wd, ignore_errors=True)
+        Tg = r["time"][torch.from_numpy(idx).cuda()].cpu().numpy().ravel()
+        Dg = r["tds1"][torch.from_numpy(idx).cuda()].cpu().numpy().ravel()
+        dT, dD = np.abs(Tg - Tr), np.abs(Dg - Dr)
+        out["cpu_baseline"] = {"value": nsmp / el, "unit": "tables/s", "cores": threads, "kind": "reference",
+                               "seconds": round(el, 3),
+                               "sample": "%d of the %d positions, eikods2d b1=2 b2=2 (order 2)" % (nsmp, NPOS)}
+        out["vs_reference_sample"] = {
+            "time_exact_frac": float((dT == 0).mean()), "time_max_abs_s": float(dT.max()),
+            "time_p99_abs_s": float(np.percentile(dT, 99)), "tds1_exact_frac": float((dD == 0).mean()),
+            "tds1_p99_abs": float(np.percentile(dD, 99))}
+    del r
+    torch.cuda.empty_cache()
+    return out
+
+
 # -------------------------------------------------------------------- main ---
 # ------------------------------------------------------- surrogate section ---
 SG_FLOPS_EVAL = 2 * 128 * (256 + 3 * 128 + 3 * 128 + 256)  # tensor FLOPs per (leg, point) in k_sg_fields
@@ -426,6 +489,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
+    ap.add_argument("--no-tables", action="store_true", help="skip the table-generator section")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the uneven five-window workload and print its object (profiling)")
     ap.add_argument("--surrogate-steps", type=int, default=40000,
@@ -566,6 +630,8 @@ def main():
             line["cpu_baseline"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()))
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(e)[:300]}
+    if dist is None and not args.no_tables and args.size == "full":
+        line["tables"] = tables_section(args.steps, args.warmup, threads)
     if dist is None and args.surrogate_steps > 0:
         line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup)
     if dist is None and not args.no_batched:

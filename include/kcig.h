@@ -186,11 +186,11 @@ typedef struct kcig_eikods_opts {
  * first derivatives with respect to the source position; both or neither),
  * gradz/gradx (the branch-aware upwind gradients of eikods2d.cpp:30-68), all
  * [nshot][nx][nz] (device), and iters [nshot] (host): the sweeps each source
- * took.  nz in 3..1800, nx >= 3.  The same local problem as the marching
- * code, solved by sweeps to the fixed point: identical results for order 1,
- * within ~1e-4 s for order 2 (whose marching result depends on the heap's
- * acceptance order).  KCIG_ERR_DEVICE if a source has no fixed point within
- * max_iter. */
+ * took.  nz in 3..1400, nx >= 3; the call allocates 4 bytes of scratch per
+ * output sample.  The same local problem as the marching code, solved by
+ * sweeps to the fixed point: identical results for order 1, within ~2.5e-4 s
+ * for order 2 (whose marching result depends on the heap's acceptance
+ * order).  KCIG_ERR_DEVICE if a source has no fixed point within max_iter. */
 int kcig_eikods(const float *vel, int nz, int nx, float o1, float o2, float d1, float d2, float o3, float d3,
                 const float *shots, int nshot, const kcig_eikods_opts *opt, float *time, float *tdl1,
                 float *tds1, float *gradz, float *gradx, int *iters, void *stream);

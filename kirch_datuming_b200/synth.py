@@ -181,7 +181,7 @@ def config1_workload(seed: int = 4, device: str = "cuda"):
     import kirch_datuming_b200 as kd
     nz, nx, dz = 201, 401, 0.01
     vel = torch.from_numpy(velocity_linear_vz(nz, nx, dz)).to(device)
-    T, D = kd.eikonal_tables(vel, dz, dz, nx, 0.0, dz, iterations=3)
+    T, D = kd.eikonal_tables(vel, dz, dz, nx, 0.0, dz)
     g = Geometry(nz=nz, nx=nx, dz=dz, dx=dz, z0=0.0, x0=0.0, ns=64, s0=0.0, ds=4.0 / 63, nh=201, h0=1.0, dh=dz,
                  cmp=0, nt=1001, dt=0.002, t0=0.0, npos=nx, p0=0.0, dp=dz)
     amps = reflectivities(3, seed)

@@ -128,3 +128,15 @@ def test_drop_in_cli_order1_equals_reference_files():
         r = subprocess.run([kd.eikods_cli_path, "in=vel.rsf", "out=t2.rsf", "shotfile=sht.rsf", "tds1=x.rsf"],
                            cwd=wd, capture_output=True, text=True)
         assert r.returncode != 0 and "Output derivative tdl1= missing." in r.stderr
+
+
+def test_gpu_more_than_1024_rows():
+    # nz > 1024: four rows per thread
+    nz, nx, d = 1100, 40, 0.01
+    v, _ = synth.five_layer_salt(nz, nx, d, d, seed=5)
+    shots = np.array([[0.0, 0.2, 0.0], [5.55, 0.131, 0.0]], np.float32)
+    got = _gpu(v, d, shots)
+    ref = O.eikods(v, d, d, shots, method=1, grads=True)
+    np.testing.assert_array_equal(got["sweeps"], ref["sweeps"])
+    for k in FIELDS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
