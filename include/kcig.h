@@ -57,6 +57,10 @@ typedef struct kcig_params {
     int axis_min_given, axis_max_given, axis_step_given, axis_n_given;
     float axis_min, axis_max, axis_step;
     int axis_n;
+    /* which tool's semantics: 0 kirchmig2d_cig (above), 1 kirchmig2d
+     * (src/kirchmig2d.cpp): cone aperture on both legs, cig=1 gives one
+     * image per trace offset index, no mute, no angle gathers */
+    int tool;
 } kcig_params;
 
 /* Axes of the data cube and of the traveltime tables (header values as the
@@ -86,6 +90,12 @@ int kcig_params_init(kcig_params *p);
  * direct mute.  argv[0] is skipped.  File keys (seismic_data=, ...) are
  * ignored here; kcig_run_cli handles them. */
 int kcig_params_parse(int argc, char **argv, kcig_params *p);
+
+/* The parameter block of kirchmig2d (src/kirchmig2d.cpp:55-340) into
+ * kcig_params with tool = 1: adj (1), cig (0; 1 = common-offset gathers, one
+ * image per offset index), cmp (1), diff (0), aperture_trace (-1, hard cut),
+ * tau (0), aperture (90 deg, hard cone), antialias (1), type (hermit). */
+int kcig_params_parse_kirchmig2d(int argc, char **argv, kcig_params *p);
 
 /* Resolve the output (n3,o3,d3) axis for these data axes, as
  * parse_output_axis (src/kirchmig2d_cig.cpp:323-368). */
@@ -124,6 +134,11 @@ int kcig_plan_last_stats(const kcig_plan *plan, int *sum_launches, float *sum_ms
 /* The drop-in executable: same argv, files, defaults, messages and exit
  * status as kirchmig2d_cig adj=1.  Returns 0 on success, else a KCIG_ERR_*. */
 int kcig_run_cli(int argc, char **argv);
+
+/* The drop-in kirchmig2d (src/kirchmig2d.cpp:35-612), adj=1: same keys,
+ * defaults, error texts and output header; adj=0 returns
+ * KCIG_ERR_UNSUPPORTED. */
+int kcig_run_kirchmig2d_cli(int argc, char **argv);
 
 /* ---- building blocks, device buffers, on `stream` ----------------------- */
 

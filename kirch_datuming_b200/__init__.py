@@ -16,11 +16,12 @@ import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
            "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "eikods", "library_path",
-           "cli_path", "eikods_cli_path"]
+           "cli_path", "eikods_cli_path", "kirchmig2d_cli_path", "params_kirchmig2d"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(_HERE, "libkcig.so")
 cli_path = os.path.join(_HERE, "bin", "kirchmig2d_cig")
+kirchmig2d_cli_path = os.path.join(_HERE, "bin", "kirchmig2d")
 eikods_cli_path = os.path.join(_HERE, "bin", "eikods2d")
 
 MEM_HOST = 0
@@ -59,7 +60,8 @@ class Params(ctypes.Structure):
         "angle_taper_start", "angle_taper_end", "oazmin", "oazmax", "oaztaper", "direct_mute_slope",
         "direct_mute_intercept", "direct_mute_taper")] + [(n, ctypes.c_int) for n in (
         "axis_min_given", "axis_max_given", "axis_step_given", "axis_n_given")] + [
-        (n, ctypes.c_float) for n in ("axis_min", "axis_max", "axis_step")] + [("axis_n", ctypes.c_int)]
+        (n, ctypes.c_float) for n in ("axis_min", "axis_max", "axis_step")] + [("axis_n", ctypes.c_int),
+                                                                             ("tool", ctypes.c_int)]
 
 
 class Geometry(ctypes.Structure):
@@ -87,6 +89,8 @@ def lib():
         L.kcig_last_error.restype = ctypes.c_char_p
         L.kcig_params_init.argtypes = [P]
         L.kcig_params_parse.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), P]
+        L.kcig_params_parse_kirchmig2d.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), P]
+        L.kcig_run_kirchmig2d_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
         L.kcig_output_axis.argtypes = [P, G, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float),
                                        ctypes.POINTER(ctypes.c_float)]
         L.kcig_plan_create.argtypes = [P, G, ctypes.c_ulonglong, ctypes.POINTER(vp)]
@@ -157,6 +161,15 @@ def params(*tokens, **kw) -> Params:
     p = Params()
     argc, argv = _argv(toks)
     _check(lib().kcig_params_parse(argc, argv, ctypes.byref(p)))
+    return p
+
+
+def params_kirchmig2d(*tokens, **kw) -> Params:
+    """kcig_params from kirchmig2d key=value tokens (tool = 1)."""
+    toks = list(tokens) + ["%s=%s" % (k, v) for k, v in kw.items()]
+    p = Params()
+    argc, argv = _argv(toks)
+    _check(lib().kcig_params_parse_kirchmig2d(argc, argv, ctypes.byref(p)))
     return p
 
 

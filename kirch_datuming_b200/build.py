@@ -6,6 +6,7 @@ produces, in-tree,
     kirch_datuming_b200/libkcig.so          the C-ABI library (include/kcig.h)
     kirch_datuming_b200/bin/kirchmig2d_cig  the drop-in migration / modelling tool
     kirch_datuming_b200/bin/eikods2d        the drop-in table generator
+    kirch_datuming_b200/bin/kirchmig2d      the drop-in plain Kirchhoff migration
 compiled for sm_100a only (nvcc cross-compiles; no GPU needed to build).
 """
 from __future__ import annotations
@@ -21,6 +22,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libkcig.so")
 CLI = os.path.join(PKG, "bin", "kirchmig2d_cig")
 EIK_CLI = os.path.join(PKG, "bin", "eikods2d")
+K2D_CLI = os.path.join(PKG, "bin", "kirchmig2d")
 
 SOURCES = ["kcig_kernels.cu", "kcig_plan.cu", "kcig_eikods.cu", "kcig_mlp.cu", "kcig_params.cpp", "kcig_rsf.cpp", "kcig_cli.cpp",
            "kcig_eikods_cli.cpp"]
@@ -58,7 +60,8 @@ def build(force: bool = False, verbose: bool = False) -> None:
             raise RuntimeError("nvcc failed:\n" + r.stdout[-6000:] + r.stderr[-6000:])
         if verbose:
             sys.stderr.write(r.stderr)
-    for exe, src in ((CLI, "kirchmig2d_cig_main.cpp"), (EIK_CLI, "eikods2d_main.cpp")):
+    for exe, src in ((CLI, "kirchmig2d_cig_main.cpp"), (EIK_CLI, "eikods2d_main.cpp"),
+                     (K2D_CLI, "kirchmig2d_main.cpp")):
         main = os.path.join(CSRC, src)
         if force or _stale(exe, [LIB, main]):
             os.makedirs(os.path.dirname(exe), exist_ok=True)

@@ -1,4 +1,5 @@
-// kcig_run_cli: the drop-in kirchmig2d_cig (adj=1 migration, adj=0 forward modelling).  Same argv keys, files,
+// kcig_run_cli: the drop-in kirchmig2d_cig (adj=1 migration, adj=0 forward modelling), and
+// kcig_run_kirchmig2d_cli: the drop-in kirchmig2d (adj=1).  Same argv keys, files,
 // defaults, ERROR texts, output header and exit status as
 // src/kirchmig2d_cig.cpp:494-1401; the migration itself runs on the GPU.
 #include <cuda_runtime.h>
@@ -17,6 +18,7 @@
 
 namespace kcig {
 int params_from_map(const ParMap &m, kcig_params *p);
+int params_from_map_kirchmig2d(const ParMap &m, kcig_params *p);
 }
 
 using namespace kcig;
@@ -59,14 +61,17 @@ static void qc_mute(float *trace, int nt, float t0, float dt, float sx, float rx
     }
 }
 
-extern "C" int kcig_run_cli(int argc, char **argv)
+// tool 0: kirchmig2d_cig; tool 1: kirchmig2d (src/kirchmig2d.cpp:35-612),
+// whose flow is the same with its own parameter block and no angle, mute or
+// gradient-file options
+static int run_tool(int argc, char **argv, int tool)
 {
     ParMap m;
     int rc = m.parse(argc, argv);
     if (rc) return fail(rc);
     kcig_params p;
     // mode is validated before the file keys (:554-563)
-    {
+    if (tool == 0) {
         const std::string mode =
             m.have("mode") ? m.str("mode") : (m.have("cig_mode") ? m.str("cig_mode") : "offset");
         std::string lm;
@@ -80,8 +85,9 @@ extern "C" int kcig_run_cli(int argc, char **argv)
                                      {"rtable", "Need rtable="},             {"rderiv", "Need rderiv="}};
     for (auto &k : need)
         if (!m.have(k[0])) return fail(set_error(KCIG_ERR_ARG, "%s", k[1]));
-    rc = params_from_map(m, &p);
+    rc = tool == 1 ? params_from_map_kirchmig2d(m, &p) : params_from_map(m, &p);
     if (rc) return fail(rc);
+    if (tool == 1 && !p.adj) return fail(set_error(KCIG_ERR_UNSUPPORTED, "kirchmig2d adj=0 is not built"));
     const bool fwd = !p.adj;  // adj=0: migration= is read, seismic_data= written (:643-701)
     const bool angle = p.cig && p.cig_is_angle;
     int use_grad = 0;
@@ -281,3 +287,7 @@ extern "C" int kcig_run_cli(int argc, char **argv)
     if ((rc = rsf_write(m.str("migration"), 3, n3, o3, d3, keys, img.data(), (long long)img.size()))) return fail(rc);
     return KCIG_OK;
 }
+
+extern "C" int kcig_run_cli(int argc, char **argv) { return run_tool(argc, argv, 0); }
+
+extern "C" int kcig_run_kirchmig2d_cli(int argc, char **argv) { return run_tool(argc, argv, 1); }

@@ -46,6 +46,12 @@ struct LegInterp {
     double gw;     // weight of gi1 (0: copy gi0)
     double pos;    // surface position of the leg (aperture)
     float scale;   // ds (source) or dh (receiver): Tx is stored as Tx*scale
+    float posf;    // the same position in the reference's float arithmetic
+    // kirchmig2d, cmp=1 receiver right of its source: the cone's right-side
+    // test is written ((x0 + ix*dx) - s) - h there (:461), so the leg keeps
+    // its shot's s and h (cexact = 1) instead of using posf = s + h
+    int cexact;
+    float cs, ch;
 };
 
 // Device views of a batch of leg fields.  The opening angle of a pair is the
@@ -65,6 +71,7 @@ struct FieldArgs {
     float dz, dx, x0;
     int radius, smooth, angle, use_grad;
     float aper, aper_taper, rmin, rtaper;
+    int cone;  // kirchmig2d: the w field holds the leg's two cone flags (see k_leg_interp)
 };
 
 // Workspace for the gradient pipeline: 4 double planes per position.
@@ -116,7 +123,7 @@ struct SumArgs {
     float *image;          // [ng][nzx]
     int zero_init;
     int nz, nx, nt, nsb, nh, ng;
-    int mode;              // 0 angle two-bin, 1 angle nearest, 2 single bin (offset/stack)
+    int mode;              // 0 angle two-bin, 1 angle nearest, 2 single bin (offset/stack), 3 kirchmig2d cone + bin
     int unit_tw;           // every trace weight of the batch is 1: trw is not read
     int shared_r;          // receiver fields indexed by ih only (cmp=0)
     int half;

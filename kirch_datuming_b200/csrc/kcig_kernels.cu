@@ -283,7 +283,23 @@ __global__ void k_leg_interp(FieldArgs a, LegFields out, double *work)
         Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
     }
     const int iz = i % a.nz, ix = i / a.nz;
-    const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin, a.rtaper);
+    double w;
+    if (a.cone) {
+        // kirchmig2d.cpp:455-488 in its float arithmetic: the pair is dropped
+        // when the image point lies beyond the cone of the left leg on its
+        // left or of the right leg on its right.  w = 1 (left-side test
+        // passes) + 2 (right-side test passes); the pair's kernel picks the
+        // left leg's bit 1 and the right leg's bit 2.
+        const float zi = __fmul_rn((float)iz, a.dz), xd = __fmul_rn((float)ix, a.dx);
+        const float lnum = __fsub_rn(__fsub_rn(L.posf, a.x0), xd);   // p - x0 - ix*dx
+        const float rnum = L.cexact ? __fsub_rn(__fsub_rn(__fadd_rn(a.x0, xd), L.cs), L.ch)  // x0 + ix*dx - s - h
+                                    : __fsub_rn(__fadd_rn(a.x0, xd), L.posf);              // x0 + ix*dx - p
+        const bool lcut = (double)atanf(__fdiv_rn(lnum, zi)) * 180. / M_PI > (double)a.aper;
+        const bool rcut = (double)atanf(__fdiv_rn(rnum, zi)) * 180. / M_PI > (double)a.aper;
+        w = (lcut ? 0.0 : 1.0) + (rcut ? 0.0 : 2.0);
+    } else {
+        w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin, a.rtaper);
+    }
     out.TP[base + i] = make_double2(T, 0.0);
     // reference: stablex[i]*ds, an FP32 product of the FP32 table derivative
     out.XW[base + i] = make_float2((float)Tx * L.scale, (float)w);
@@ -653,7 +669,17 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 if (!(apw > 0.0f)) continue;
                 int b0 = 0;
                 float w0 = 1.0f, w1 = 0.0f, aw;
-                if (MODE == 2) {
+                if (MODE == 3) {
+                    // kirchmig2d (:455-488): the trace weight's sign says
+                    // whether the source is the left leg; each leg's w holds
+                    // its cone flags (1: left side inside, 2: right side inside)
+                    const int sw = (int)sXW[k].y, rw = (int)rXW.y;
+                    const bool keep = tw > 0.0f ? ((sw & 1) && (rw & 2)) : ((rw & 1) && (sw & 2));
+                    if (!keep) continue;
+                    b0 = __ldg(a.igo + trc) - gc0;
+                    if (b0 < 0 || b0 >= nb) continue;
+                    aw = 1.0f;
+                } else if (MODE == 2) {
                     b0 = __ldg(a.igo + trc) - gc0;
                     if (b0 < 0 || b0 >= nb) continue;
                     aw = tw * apw;
@@ -865,10 +891,12 @@ static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
     if (a.shared_r) {
         if (a.mode == 0) return launch_sum_t<TZ, TX, KB, true, 0>(a, nb, st);
         if (a.mode == 1) return launch_sum_t<TZ, TX, KB, true, 1>(a, nb, st);
+        if (a.mode == 3) return launch_sum_t<TZ, TX, KB, true, 3>(a, nb, st);
         return launch_sum_t<TZ, TX, KB, true, 2>(a, nb, st);
     }
     if (a.mode == 0) return launch_sum_t<TZ, TX, 1, false, 0>(a, nb, st);
     if (a.mode == 1) return launch_sum_t<TZ, TX, 1, false, 1>(a, nb, st);
+    if (a.mode == 3) return launch_sum_t<TZ, TX, 1, false, 3>(a, nb, st);
     return launch_sum_t<TZ, TX, 1, false, 2>(a, nb, st);
 }
 

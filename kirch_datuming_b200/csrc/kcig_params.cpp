@@ -207,9 +207,48 @@ int params_from_map(const ParMap &m, kcig_params *p)
     return KCIG_OK;
 }
 
+// kirchmig2d's parameter block (src/kirchmig2d.cpp:55-340): its own keys
+// and defaults; everything it does not have stays off.
+int params_from_map_kirchmig2d(const ParMap &m, kcig_params *p)
+{
+    kcig_params_init(p);
+    p->tool = 1;
+    p->cig_is_angle = 0;
+    p->aperture_trace_taper = 0;  // a hard trace-index cut (:57-60, :423)
+    p->aperture_taper = 0.0f;     // a hard cone (:459-486)
+    p->aperture_rmin = 0.0f;
+    p->direct_mute = 0;
+    if (m.have("aperture_trace")) m.get_int("aperture_trace", &p->aperture_trace);
+    if (m.have("adj")) m.get_int("adj", &p->adj);
+    p->cig = 0;
+    if (m.have("cig")) m.get_int("cig", &p->cig);
+    p->cmp = 1;
+    if (m.have("cmp")) m.get_int("cmp", &p->cmp);
+    if (m.have("diff")) m.get_int("diff", &p->isdiff);
+    if (m.have("tau")) m.get_float("tau", &p->tau);
+    if (m.have("aperture")) m.get_float("aperture", &p->aperture);
+    if (m.have("antialias")) m.get_float("antialias", &p->antialias);
+    std::string type = m.have("type") ? m.str("type") : "hermit";
+    if (type.empty() || (type[0] != 'l' && type[0] != 'p' && type[0] != 'h'))
+        return set_error(KCIG_ERR_ARG,
+                         "Unknown interpolation type: %s. Supported types are: linear (l), partial (p) and hermite (h)",
+                         type.c_str());
+    p->interp_type = type[0];
+    return KCIG_OK;
+}
+
 }  // namespace kcig
 
 using namespace kcig;
+
+extern "C" int kcig_params_parse_kirchmig2d(int argc, char **argv, kcig_params *p)
+{
+    if (!p) return set_error(KCIG_ERR_ARG, "kcig_params_parse_kirchmig2d: null");
+    ParMap m;
+    int rc = m.parse(argc, argv);
+    if (rc) return rc;
+    return params_from_map_kirchmig2d(m, p);
+}
 
 extern "C" const char *kcig_last_error(void) { return g_err.c_str(); }
 
@@ -265,6 +304,12 @@ extern "C" int kcig_output_axis(const kcig_params *p, const kcig_geometry *g, in
         *ng = 1;
         *g0 = 0.0f;
         *dg = 1.0f;
+        return KCIG_OK;
+    }
+    if (p->tool == 1) {  // kirchmig2d: one image per offset index (:243, :283-287)
+        *ng = g->nh;
+        *g0 = g->h0;
+        *dg = g->nh == 1 ? 0.0f : g->dh;
         return KCIG_OK;
     }
     const int is_angle = p->cig_is_angle;

@@ -128,10 +128,20 @@ int leg_interp(const kcig_plan *P, int is_source, float posf, double pos, LegInt
     memset(L, 0, sizeof *L);
     L->type = P->p.interp_type;
     L->pos = pos;
+    L->posf = posf;
     L->i1 = -1;
     float f = 0.0f;
     bool left;
-    if (is_source) {
+    int tool1_index = 0;
+    if (P->p.tool == 1) {
+        // kirchmig2d.cpp:372-395, :413-440: the index is the float quotient
+        // truncated; at or below 0 the first slice and at or above n-1 the
+        // last are taken unchanged (the first interval is not interpolated,
+        // unlike kirchmig2d_cig); the raw index also drives aperture_trace
+        tool1_index = (df != 0.0f) ? (int)((posf - of) / df) : 0;
+        left = tool1_index <= 0;
+        f = left ? 0.0f : (tool1_index >= n - 1 ? (float)(n - 1) : (float)tool1_index);
+    } else if (is_source) {
         left = (n <= 1 || df == 0.0f);
         if (!left) f = (posf - of) / df;
         if (!left && f <= 0.0f) left = true;
@@ -147,7 +157,7 @@ int leg_interp(const kcig_plan *P, int is_source, float posf, double pos, LegInt
         L->i0 = n - 1;
         ret = n - 1;
     } else {
-        const int i0 = (int)floorf(f);
+        const int i0 = P->p.tool == 1 ? tool1_index : (int)floorf(f);
         const double x = pos - (o + (double)i0 * d);
         const double t = x / d;
         L->i0 = i0;
@@ -176,6 +186,7 @@ int leg_interp(const kcig_plan *P, int is_source, float posf, double pos, LegInt
             L->e[0] = g00 / d; L->e[1] = g10; L->e[2] = g01 / d; L->e[3] = g11;
         }
     }
+    if (P->p.tool == 1) ret = tool1_index;
     // interp_volume_linear_stream (:294-322) for the optional gradient files
     L->gi0 = 0;
     L->gi1 = 0;
@@ -235,6 +246,7 @@ int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int
         a.aper_taper = P->p.aperture_taper;
         a.rmin = P->p.aperture_rmin;
         a.rtaper = P->p.aperture_rtaper;
+        a.cone = P->p.tool == 1;
         LegFields out{TP + (size_t)j0 * nzx, XW + (size_t)j0 * nzx};
         int nl = 0;
         KCIG_TRY(launch_leg_fields(a, out, P->d_work.as<double>(), P->st, &nl));
@@ -476,7 +488,9 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             mrx[t] = rpos;
             float rf = 0.0f;
             if (g.rny > 1 && g.rdy != 0.0f) rf = (rposf - g.ry0) / g.rdy;
-            const int iht = (g.rny > 1 && g.rdy != 0.0f) ? (int)floorf(rf) : 0;
+            int iht = (g.rny > 1 && g.rdy != 0.0f) ? (int)floorf(rf) : 0;
+            // kirchmig2d: the truncated quotient (:413)
+            if (p.tool == 1) iht = g.rdy != 0.0f ? (int)((rposf - g.ry0) / g.rdy) : 0;
             double w = 1.0;
             if (p.aperture_trace != -1) {
                 const double ad = fabs((double)(iht - ist[is]));
@@ -489,7 +503,14 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
                     }
                 }
             }
-            if (p.cig && !p.cig_is_angle) {
+            if (p.tool == 1) {
+                // kirchmig2d: image = offset index (cig=1) or the stack; the
+                // weight's sign says whether the source is the left leg of
+                // the cone test (:457 cmp: h >= 0; :474 h - s >= 0)
+                igo[t] = p.cig ? ih : 0;
+                const bool src_left = p.cmp ? (hxf[ih] >= 0.0f) : (hxf[ih] - sxf[is] >= 0.0f);
+                if (!src_left) w = -w;
+            } else if (p.cig && !p.cig_is_angle) {
                 // value_to_nearest_bin(h) (:35-41), a discrete decision in float
                 int ig = -1;
                 if (P->ng > 0 && P->dg > 0.0f && isfinite(hxf[ih])) {
@@ -573,7 +594,9 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             if (rc) break;
             // per-trace arrays of this (shot batch, receiver chunk)
             std::vector<LegInterp> rl;
-            std::map<std::pair<double, float>, int> seen;  // (FP64, float) receiver position
+            // receiver legs by (FP64, float) position; kirchmig2d's cmp=1 cone
+            // test also depends on the shot of a leg right of its source
+            std::map<std::tuple<double, float, float>, int> seen;
             for (int k = 0; k < nsh; k++)
                 for (int r = 0; r < nhb; r++) {
                     const size_t t = (size_t)(s0 + k) * g.nh + (r0 + r);
@@ -585,12 +608,17 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
                     if (shared_r) {
                         h_rfi[b] = r;
                     } else {
-                        const std::pair<double, float> key(mrx[t], sxf[s0 + k] + hxf[r0 + r]);
+                        const bool cexact = p.tool == 1 && p.cmp && hxf[r0 + r] >= 0.0f;
+                        const std::tuple<double, float, float> key(mrx[t], sxf[s0 + k] + hxf[r0 + r],
+                                                                   cexact ? sxf[s0 + k] : 0.0f);
                         auto it = seen.find(key);
                         if (it == seen.end()) {
                             LegInterp L;
-                            leg_interp(P, 0, key.second, key.first, &L);
+                            leg_interp(P, 0, std::get<1>(key), std::get<0>(key), &L);
                             L.scale = (float)dh;
+                            L.cexact = cexact ? 1 : 0;
+                            L.cs = sxf[s0 + k];
+                            L.ch = hxf[r0 + r];
                             it = seen.emplace(key, (int)rl.size()).first;
                             rl.push_back(L);
                         }
@@ -653,7 +681,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             sa.nsb = nsh;
             sa.nh = nhb;
             sa.ng = P->ng;
-            sa.mode = angle ? (p.angle_interp ? 0 : 1) : 2;
+            sa.mode = p.tool == 1 ? 3 : (angle ? (p.angle_interp ? 0 : 1) : 2);
             // a uniform flag spares the pair loop a dependent load per pair
             sa.unit_tw = std::all_of(h_trw.begin(), h_trw.begin() + nb, [](float v) { return v == 1.0f; }) ? 1 : 0;
             sa.tile = P->tile;
@@ -741,6 +769,8 @@ extern "C" float kcig_plan_last_prelude_ms(const kcig_plan *P) { return P ? P->p
 extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_surrogate *rcv)
 {
     if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_surrogate: null plan");
+    if (P->p.tool == 1 && (src || rcv))
+        return set_error(KCIG_ERR_UNSUPPORTED, "kirchmig2d with a traveltime surrogate is not built");
     P->sg_src = src;
     P->sg_rcv = rcv;
     return KCIG_OK;
@@ -757,6 +787,7 @@ extern "C" int kcig_model(kcig_plan *P, const float *image, float *data, int mem
     if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab)) return set_error(KCIG_ERR_ARG, "kcig_model: tables not set");
     const kcig_params &p = P->p;
     const kcig_geometry &g = P->g;
+    if (p.tool == 1) return set_error(KCIG_ERR_UNSUPPORTED, "kirchmig2d adj=0 is not built");
     if (p.direct_mute) return set_error(KCIG_ERR_ARG, "direct_mute=1 is an input-data preprocessing option and requires adj=1.");
     const size_t nzx = (size_t)g.nz * g.nx;
     const int angle = p.cig && p.cig_is_angle;
@@ -1076,6 +1107,7 @@ int run_prepared(kcig_plan *P, float *d_img, cudaStream_t st, cudaEvent_t *ev = 
 extern "C" int kcig_shots_prepare(kcig_plan *P, int nshots, const kcig_shot *shots, int memory)
 {
     if (!P || nshots < 0 || (nshots > 0 && !shots)) return set_error(KCIG_ERR_ARG, "kcig_shots_prepare: bad arguments");
+    if (P->p.tool == 1) return set_error(KCIG_ERR_UNSUPPORTED, "kirchmig2d shots of uneven size are not built");
     const kcig_params &p = P->p;
     const kcig_geometry &g = P->g;
     if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab))
@@ -1595,6 +1627,7 @@ extern "C" int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry
     a.aper_taper = p->aperture_taper;
     a.rmin = p->aperture_rmin;
     a.rtaper = p->aperture_rtaper;
+    a.cone = p->tool == 1;
     KCIG_TRY(launch_leg_fields(a, LegFields{d_tp, d_xw}, d_work, st));
     struct Cp { void *dst; const char *src; size_t el, pitch; } cps[4] = {
         {T, (const char *)d_tp, sizeof(double), sizeof(double2)},

@@ -720,6 +720,102 @@ int oracle_migrate_adj(const oracle_params *P, const float *data, const float *s
  * of the adjoint path; each trace is the sum of the sprayed picks, then
  * doubint (its own adjoint).  No direct mute and no diff2 are applied, as in
  * the reference's forward branch.  Serial (the trace is the scatter target). */
+/* ------------------------------------------------------------ kirchmig2d --
+ * src/kirchmig2d.cpp:366-540 (adj=1), the plain Kirchhoff tool: the table
+ * index is the truncated float quotient, and a position in the first
+ * interval takes slice 0 unchanged (:372-395, :413-440); a trace is dropped
+ * when |iht - ist| >= aperture_trace (:423); a pair is dropped outside the
+ * cone test of :455-488, evaluated in the reference's float arithmetic in
+ * both builds; ti = t1 + t2 + tau; the pick goes to image ih (cig=1) or 0.
+ * P->ng must be nh (cig=1) or 1. */
+static int table_at_k2d(const oracle_params *P, const float *tab, const float *der, float posf, R pos, float of,
+                        float df, int n, R *T, R *Tx, R *s0, R *s1, R *m0, R *m1)
+{
+    const long nzx = (long)P->nz * P->nx;
+    const int it = (df != 0.0f) ? (int)((posf - of) / df) : 0;
+    if (it <= 0) {
+        load_slice(T, tab, 0, nzx);
+        load_slice(Tx, der, 0, nzx);
+    } else if (it >= n - 1) {
+        load_slice(T, tab, n - 1, nzx);
+        load_slice(Tx, der, n - 1, nzx);
+    } else {
+        const R coord = pos - ((R)of + (R)it * (R)df);
+        load_slice(s0, tab, it, nzx);
+        load_slice(s1, tab, it + 1, nzx);
+        load_slice(m0, der, it, nzx);
+        load_slice(m1, der, it + 1, nzx);
+        interp_slices(P->interp_type, T, Tx, coord, (R)df, s0, s1, m0, m1, P->nz, (int)nzx, RF(P->dx));
+    }
+    return it;
+}
+
+static int cone_cut(float num, float zi, float aper)
+{
+    return atanf(num / zi) * 180. / 3.14159265358979323846 > aper;
+}
+
+int oracle_kirchmig2d_adj(const oracle_params *P, const float *data, const float *stab, const float *sder,
+                          const float *rtab, const float *rder, double *image)
+{
+    const int nz = P->nz, nx = P->nx, nt = P->nt, ng = P->ng;
+    const long nzx = (long)nz * nx;
+    const float dsf = P->ns == 1 ? 0.0f : P->ds, dhf = P->nh == 1 ? 0.0f : P->dh;
+    const R ds = RF(dsf), dh = RF(dhf);
+    R *buf = (R *)malloc(sizeof(R) * (size_t)nzx * 8);
+    R *trace = (R *)malloc(sizeof(R) * (size_t)nt * 2);
+    R *out = (R *)calloc((size_t)nzx * ng, sizeof(R));
+    if (!buf || !trace || !out) { free(buf); free(trace); free(out); return -1; }
+    R *ST = buf, *STx = buf + nzx, *RT = buf + 2 * nzx, *RTx = buf + 3 * nzx;
+    R *s0 = buf + 4 * nzx, *s1 = buf + 5 * nzx, *m0 = buf + 6 * nzx, *m1 = buf + 7 * nzx;
+    const R t0 = RF(P->t0), dt = RF(P->dt), tau = RF(P->tau), aal = RF(P->aal);
+    for (int is = 0; is < P->ns; is++) {
+        const float sf = P->s0 + (float)is * dsf;
+        const R s = RF(P->s0) + (R)is * ds;
+        const int ist = table_at_k2d(P, stab, sder, sf, s, P->sy0, P->sdy, P->sny, ST, STx, s0, s1, m0, m1);
+        for (int ih = 0; ih < P->nh; ih++) {
+            const float hf = P->h0 + (float)ih * dhf;
+            const R h = RF(P->h0) + (R)ih * dh;
+            const float rposf = P->cmp ? sf + hf : hf;
+            const R rpos = P->cmp ? s + h : h;
+            const int iht = (P->rdy != 0.0f) ? (int)((rposf - P->ry0) / P->rdy) : 0;
+            if (P->aperture_trace != -1 && fabs((double)(iht - ist)) >= (double)P->aperture_trace) continue;
+            const float *src = data + ((long)is * P->nh + ih) * nt;
+            for (int it = 0; it < nt; it++) trace[it] = (R)src[it];
+            doubint(nt, trace);
+            if (P->isdiff == 1) diff2(trace, nt, dt, trace + nt);
+            (void)table_at_k2d(P, rtab, rder, rposf, rpos, P->ry0, P->rdy, P->rny, RT, RTx, s0, s1, m0, m1);
+            R *img = out + (long)(P->cig ? ih : 0) * nzx;
+#pragma omp parallel for
+            for (long i = 0; i < nzx; i++) {
+                const int iz = (int)(i % nz), ix = (int)(i / nz);
+                const float zi = (float)iz * P->dz, xd = (float)ix * P->dx;
+                int cut;
+                if (P->cmp) {
+                    if (hf >= 0.0f)
+                        cut = cone_cut(sf - P->x0 - xd, zi, P->aper) || cone_cut(P->x0 + xd - sf - hf, zi, P->aper);
+                    else
+                        cut = cone_cut(sf + hf - P->x0 - xd, zi, P->aper) || cone_cut(P->x0 + xd - sf, zi, P->aper);
+                } else {
+                    if (hf - sf >= 0.0f)
+                        cut = cone_cut(sf - P->x0 - xd, zi, P->aper) || cone_cut(P->x0 + xd - hf, zi, P->aper);
+                    else
+                        cut = cone_cut(hf - P->x0 - xd, zi, P->aper) || cone_cut(P->x0 + xd - sf, zi, P->aper);
+                }
+                if (cut) continue;
+                const R ti = ST[i] + RT[i] + tau;
+                const R tx = MAXV(R_FABS(STx[i] * ds), R_FABS(RTx[i] * dh));
+                img[i] += kirmig_pick(ti, tx * aal, trace, nt, dt, t0);
+            }
+        }
+    }
+    for (long i = 0; i < nzx * ng; i++) image[i] = (double)out[i];
+    free(buf);
+    free(trace);
+    free(out);
+    return 0;
+}
+
 int oracle_model_fwd(const oracle_params *P, const float *image, const float *stab, const float *sder,
                      const float *rtab, const float *rder, const float *sgx_v, const float *sgz_v,
                      const float *rgx_v, const float *rgz_v, double *data)

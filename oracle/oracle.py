@@ -65,6 +65,8 @@ def lib(fp64: bool = True):
         L.oracle_migrate_adj.argtypes = [ctypes.POINTER(OracleParams), fp, fp, fp, fp, fp,
                                          fp, fp, fp, fp, dp]
         L.oracle_migrate_adj.restype = ctypes.c_int
+        L.oracle_kirchmig2d_adj.argtypes = [ctypes.POINTER(OracleParams), fp, fp, fp, fp, fp, dp]
+        L.oracle_kirchmig2d_adj.restype = ctypes.c_int
         L.oracle_model_fwd.argtypes = [ctypes.POINTER(OracleParams), fp, fp, fp, fp, fp, fp, fp, fp, fp, dp]
         L.oracle_model_fwd.restype = ctypes.c_int
         L.oracle_doubint.argtypes = [ctypes.c_int, fp, dp, ctypes.c_int, ctypes.c_float]
@@ -101,6 +103,19 @@ def migrate_adj(p: OracleParams, data, stable, sderiv, rtable, rderiv, grads=Non
                               img.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     if rc != 0:
         raise RuntimeError("oracle_migrate_adj failed: %d" % rc)
+    return img.reshape(p.ng, p.nx, p.nz)
+
+
+def migrate_kirchmig2d(p: OracleParams, data, stable, sderiv, rtable, rderiv, fp64: bool = True) -> np.ndarray:
+    """kirchmig2d adj=1 (src/kirchmig2d.cpp:366-540): image [ng][nx][nz],
+    ng = nh for cig=1 else 1 (p.ng must say so)."""
+    L = lib(fp64)
+    data, stable, sderiv, rtable, rderiv = map(_f32, (data, stable, sderiv, rtable, rderiv))
+    img = np.zeros(p.ng * p.nx * p.nz, dtype=np.float64)
+    rc = L.oracle_kirchmig2d_adj(ctypes.byref(p), _fptr(data), _fptr(stable), _fptr(sderiv), _fptr(rtable),
+                                 _fptr(rderiv), img.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if rc != 0:
+        raise RuntimeError("oracle_kirchmig2d_adj failed: %d" % rc)
     return img.reshape(p.ng, p.nx, p.nz)
 
 

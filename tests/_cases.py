@@ -45,9 +45,16 @@ class Golden:
     def tokens(self, case):
         return list(self.meta["cases"][case]["tokens"])
 
-    def geometry_dict(self, case):
-        c = self.meta["cases"][case]
-        d = self.meta["data"][c["data"]]
+    @property
+    def k2d_cases(self):
+        return sorted(self.meta.get("k2d", {}))
+
+    def k2d_image(self, name):
+        c = self.meta["k2d"][name]
+        return np.load(os.path.join(GOLDEN, "golden_k2d.npz"))[name].reshape(c["n"][2], c["n"][1], c["n"][0])
+
+    def geometry_dict(self, case, data_key=None):
+        d = self.meta["data"][data_key or self.meta["cases"][case]["data"]]
         t = self.meta["table"]
         f = lambda v: float(np.float32(v))  # header values are read as float  # noqa: E731
         return dict(nt=self.meta["nt"], nh=d["nh"], ns=d["ns"], t0=0.0, dt=f(self.meta["dt"]), h0=f(d["h0"]),
@@ -90,6 +97,16 @@ def case_setup(gd: Golden, case: str):
     return kp, geom, axis, oracle_params(kp, geom, axis, use_grad), use_grad
 
 
+def k2d_setup(gd: Golden, name: str):
+    """kirchmig2d fixture: (library params, geometry dict, axis, oracle params)."""
+    import kirch_datuming_b200 as kd
+    c = gd.meta["k2d"][name]
+    kp = kd.params_kirchmig2d(*c["tokens"])
+    geom = gd.geometry_dict(None, data_key=c["data"])
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    return kp, geom, axis, oracle_params(kp, geom, axis)
+
+
 def fwd_setup(gd: Golden, name: str):
     """adj=0 fixture: (library params, geometry dict, axis, oracle params,
     model image [ng][nx][nz])."""
@@ -116,4 +133,5 @@ def ub_columns(gd: Golden, case: str) -> int:
     """Leading lateral columns where the reference's type=partial derivative
     reads outside its table slice (tinterpsr.cpp:119-124): its image there is
     undefined and is not compared."""
-    return 3 if any(t.startswith("type=p") for t in gd.tokens(case)) else 0
+    toks = gd.meta["k2d"][case]["tokens"] if case in gd.meta.get("k2d", {}) else gd.tokens(case)
+    return 3 if any(t.startswith("type=p") for t in toks) else 0

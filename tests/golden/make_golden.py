@@ -10,6 +10,7 @@ container); the tests only read the committed outputs.
     python tests/golden/make_golden.py            # everything
     python tests/golden/make_golden.py --forward  # only the adj=0 fixtures
     python tests/golden/make_golden.py --eikods   # only the table-generator fixtures
+    python tests/golden/make_golden.py --kirchmig2d  # only the plain-tool fixtures
 """
 from __future__ import annotations
 
@@ -224,9 +225,52 @@ def eikods():
     print("wrote", os.path.join(HERE, "golden_eikods.npz"))
 
 
+# the plain tool kirchmig2d on the same inputs (oracle/_ref/kirchmig2d), one
+# OpenMP thread
+K2D = {
+    "k2d_default": dict(data="cmp1", tokens=["cmp=1"]),
+    "k2d_cig_cmp0": dict(data="cmp0", tokens=["cmp=0", "cig=1", "aperture=40", "antialias=0.5", "tau=0.004",
+                                              "diff=1", "type=linear"]),
+    "k2d_trace_ap": dict(data="cmp1", tokens=["cmp=1", "cig=1", "aperture=60", "aperture_trace=6",
+                                              "type=partial"]),
+    "k2d_stack_cmp0": dict(data="cmp0", tokens=["cmp=0", "aperture=25"]),
+}
+
+
+def kirchmig2d():
+    """kirchmig2d fixtures (golden_k2d.npz, cases.json "k2d")."""
+    gz = np.load(os.path.join(HERE, "golden.npz"))
+    with open(os.path.join(HERE, "cases.json")) as f:
+        meta = json.load(f)
+    t = meta["table"]
+    out = {}
+    meta["k2d"] = {}
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/time.rsf", gz["T"], t["n"], t["o"], t["d"])
+        rsf.write(f"{wd}/tds.rsf", gz["tds"], t["n"], t["o"], t["d"])
+        for name, d in DATA.items():
+            rsf.write(f"{wd}/data_{name}.rsf", gz["data_" + name], [NT, d["nh"], d["ns"]], [0, d["h0"], d["s0"]],
+                      [DT, d["dh"], d["ds"]], extra={"unit1": "s"})
+        for name, c in K2D.items():
+            args = [f"seismic_data=data_{c['data']}.rsf", "migration=img.rsf", "stable=time.rsf", "sderiv=tds.rsf",
+                    "rtable=time.rsf", "rderiv=tds.rsf"] + c["tokens"]
+            run([f"{REF}/kirchmig2d"] + args, wd, env=env)
+            h, img = rsf.read(f"{wd}/img.rsf")
+            out[name] = img.reshape(h.n[2], h.n[1], h.n[0])
+            meta["k2d"][name] = dict(data=c["data"], tokens=c["tokens"], n=h.n[:3], o=h.o[:3], d=h.d[:3],
+                                     extra={k: v for k, v in h.extra.items() if k.startswith(("label", "unit"))})
+    np.savez_compressed(os.path.join(HERE, "golden_k2d.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_k2d.npz"))
+
+
 if __name__ == "__main__":
     if "--forward" in sys.argv:
         forward()
+    elif "--kirchmig2d" in sys.argv:
+        kirchmig2d()
     elif "--eikods" in sys.argv:
         eikods()
     else:
