@@ -30,6 +30,7 @@ extern "C" {
 
 #define KCIG_MEM_HOST 0   /* pointer is ordinary or pinned host memory         */
 #define KCIG_MEM_DEVICE 1 /* pointer is device memory of the plan's device      */
+#define KCIG_MEM_HOST_STREAM 2 /* tables only: stay in host memory, slices copied per leg batch */
 
 /* Parameters of kirchmig2d_cig.  Field meanings and defaults are those of
  * src/kirchmig2d_cig.cpp:494-958; kcig_params_init() fills the defaults. */
@@ -113,7 +114,14 @@ int kcig_plan_set_stream(kcig_plan *plan, void *stream);
 
 /* Traveltime tables and their position derivatives ([npos][nx][nz]).  Host
  * tables are copied to the device; device tables are used in place and must
- * outlive the plan.  Passing the same stable/rtable pointers shares one copy. */
+ * outlive the plan.  Passing the same stable/rtable pointers shares one copy.
+ * KCIG_MEM_HOST_STREAM keeps host tables where they are (they must stay valid
+ * while the plan uses them; pinned memory copies fastest): each batch of leg
+ * fields copies only the slices it interpolates into a staging buffer, so
+ * tables larger than the device memory can be migrated.  Results are
+ * identical to device-resident tables.  kcig_migrate, kcig_model and
+ * kcig_leg_fields_device take streamed tables; kcig_migrate_prepared does
+ * not (KCIG_ERR_UNSUPPORTED). */
 int kcig_plan_set_tables(kcig_plan *plan, const float *stable, const float *sderiv,
                          const float *rtable, const float *rderiv, int memory);
 

@@ -26,6 +26,7 @@ eikods_cli_path = os.path.join(_HERE, "bin", "eikods2d")
 
 MEM_HOST = 0
 MEM_DEVICE = 1
+MEM_HOST_STREAM = 2
 
 
 class KcigError(RuntimeError):
@@ -210,15 +211,22 @@ class Plan:
         if stream is not None:
             _check(lib().kcig_plan_set_stream(self._h, ctypes.c_void_p(stream)))
 
-    def set_tables(self, stable, sderiv, rtable=None, rderiv=None):
+    def set_tables(self, stable, sderiv, rtable=None, rderiv=None, stream=False):
+        """stream=True (host arrays only): the tables stay in host memory and
+        each leg batch copies the slices it needs (KCIG_MEM_HOST_STREAM)."""
         rtable = stable if rtable is None else rtable
         rderiv = sderiv if rderiv is None else rderiv
         ptrs = [_ptr(x) for x in (stable, sderiv, rtable, rderiv)]
         mem = {m for _, m in ptrs}
         if len(mem) != 1:
             raise ValueError("tables must all be host or all be device arrays")
+        mem = mem.pop()
+        if stream:
+            if mem != MEM_HOST:
+                raise ValueError("stream=True needs host tables")
+            mem = MEM_HOST_STREAM
         self._keep += [stable, sderiv, rtable, rderiv]
-        _check(lib().kcig_plan_set_tables(self._h, *[p for p, _ in ptrs], mem.pop()))
+        _check(lib().kcig_plan_set_tables(self._h, *[p for p, _ in ptrs], mem))
 
     def set_gradients(self, sgradx, sgradz, rgradx, rgradz):
         ptrs = [_ptr(x) for x in (sgradx, sgradz, rgradx, rgradz)]

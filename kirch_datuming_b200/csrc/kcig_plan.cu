@@ -59,6 +59,11 @@ struct kcig_plan {
     DevBuf own_stab, own_sder, own_rtab, own_rder, own_sgx, own_sgz, own_rgx, own_rgz;
     DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
     DevBuf d_part;  // partial images of a split summation (small grids)
+    // tables left in host memory (KCIG_MEM_HOST_STREAM): the slices of each
+    // leg batch are copied into d_stage
+    int stream_tables = 0;
+    const float *h_stab = nullptr, *h_sder = nullptr, *h_rtab = nullptr, *h_rder = nullptr;
+    DevBuf d_stage;
     int sum_launches = 0, all_launches = 0;
     float sum_ms = 0.f, fields_ms = 0.f, prelude_ms = 0.f;
     kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
@@ -211,8 +216,10 @@ int field_batch(const kcig_plan *P, size_t nlegs)
     return std::max(1, std::min<int>((int)nlegs, (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
 }
 
-// Leg fields of n legs whose LegInterp records are already on the device.
-int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int n, double2 *TP, float2 *XW)
+// Leg fields of n legs whose LegInterp records are already on the device;
+// tab/der (device) replace the plan's tables when given (staged slices).
+int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int n, double2 *TP, float2 *XW,
+                       const float *tab = nullptr, const float *der = nullptr)
 {
     const kcig_geometry &g = P->g;
     const size_t nzx = (size_t)g.nz * g.nx;
@@ -222,13 +229,15 @@ int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int
         P->all_launches += 1;
         return KCIG_OK;
     }
+    if (P->stream_tables && !tab)
+        return set_error(KCIG_ERR_UNSUPPORTED, "tables kept in host memory need the host-side leg path");
     const int angle = P->p.cig && P->p.cig_is_angle;
     const int FB = field_batch(P, (size_t)n);
     if (angle) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
     for (int j0 = 0; j0 < n; j0 += FB) {
         FieldArgs a;
-        a.tab = is_source ? P->stab : P->rtab;
-        a.der = is_source ? P->sder : P->rder;
+        a.tab = tab ? tab : (is_source ? P->stab : P->rtab);
+        a.der = der ? der : (is_source ? P->sder : P->rder);
         a.gxv = is_source ? P->sgx : P->rgx;
         a.gzv = is_source ? P->sgz : P->rgz;
         a.legs = d_legs + j0;
@@ -259,9 +268,58 @@ int compute_fields(kcig_plan *P, int is_source, const std::vector<LegInterp> &le
 {
     KCIG_TRY(P->d_legs.ensure(legs.size() * sizeof(LegInterp)));
     if (legs.empty()) return KCIG_OK;
-    KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
-                              P->st));
-    return compute_fields_dev(P, is_source, P->d_legs.as<LegInterp>(), (int)legs.size(), TP, XW);
+    if (!P->stream_tables || (is_source ? P->sg_src : P->sg_rcv)) {
+        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, legs.data(), legs.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
+                                  P->st));
+        return compute_fields_dev(P, is_source, P->d_legs.as<LegInterp>(), (int)legs.size(), TP, XW);
+    }
+    // Tables in host memory: legs go in groups whose slices fit the staging
+    // buffer (two per leg of a field launch at most, and a quarter of the
+    // plan's budget); each group's slices are copied in stream order, the
+    // group's legs renumbered to their staging slots, and its fields
+    // computed.  Values are read exactly as from device tables.
+    const size_t nzx = (size_t)P->g.nz * P->g.nx, slice = nzx * sizeof(float);
+    const float *ht = is_source ? P->h_stab : P->h_rtab, *hd = is_source ? P->h_sder : P->h_rder;
+    const int npos = is_source ? P->g.sny : P->g.rny;
+    const int FB = field_batch(P, legs.size());
+    const size_t by_budget = P->budget / 4 / (2 * slice);
+    const int cap = (int)std::max<size_t>(2, std::min<size_t>((size_t)2 * FB, by_budget));
+    KCIG_TRY(P->d_stage.ensure((size_t)2 * cap * slice));
+    float *sT = P->d_stage.as<float>(), *sD = sT + (size_t)cap * nzx;
+    std::vector<LegInterp> grp;
+    std::map<int, int> slot;
+    size_t j = 0;
+    while (j < legs.size()) {
+        grp.clear();
+        slot.clear();
+        size_t k = j;
+        for (; k < legs.size(); k++) {
+            LegInterp L = legs[k];
+            const int need = (slot.count(L.i0) ? 0 : 1) + (L.i1 >= 0 && L.i1 != L.i0 && !slot.count(L.i1) ? 1 : 0);
+            if ((int)slot.size() + need > cap) break;
+            for (int *ip : {&L.i0, &L.i1}) {
+                if (*ip < 0) continue;
+                if (*ip >= npos) return set_error(KCIG_ERR_ARG, "table slice %d outside [0,%d)", *ip, npos);
+                auto it = slot.find(*ip);
+                if (it == slot.end()) {
+                    const int q = (int)slot.size();
+                    KCIG_CUDA(cudaMemcpyAsync(sT + (size_t)q * nzx, ht + (size_t)*ip * nzx, slice,
+                                              cudaMemcpyHostToDevice, P->st));
+                    KCIG_CUDA(cudaMemcpyAsync(sD + (size_t)q * nzx, hd + (size_t)*ip * nzx, slice,
+                                              cudaMemcpyHostToDevice, P->st));
+                    it = slot.emplace(*ip, q).first;
+                }
+                *ip = it->second;
+            }
+            grp.push_back(L);
+        }
+        KCIG_CUDA(cudaMemcpyAsync(P->d_legs.p, grp.data(), grp.size() * sizeof(LegInterp), cudaMemcpyHostToDevice,
+                                  P->st));
+        KCIG_TRY(compute_fields_dev(P, is_source, P->d_legs.as<LegInterp>(), (int)grp.size(), TP + j * nzx,
+                                    XW + j * nzx, sT, sD));
+        j = k;
+    }
+    return KCIG_OK;
 }
 
 }  // namespace
@@ -311,7 +369,7 @@ extern "C" int kcig_plan_destroy(kcig_plan *P)
     DevBuf *bufs[] = {&P->own_stab, &P->own_sder, &P->own_rtab, &P->own_rder, &P->own_sgx, &P->own_sgz,
                       &P->own_rgx,  &P->own_rgz,  &P->d_data,   &P->d_image,  &P->d_rT,   &P->d_rF,
                       &P->d_sT,     &P->d_sF,   &P->d_work,   &P->d_D,      &P->d_legs, &P->d_tr,
-                      &P->d_part};
+                      &P->d_part,   &P->d_stage};
     for (DevBuf *b : bufs) b->release();
     release_shots(P);
     if (P->own_st) cudaStreamDestroy(P->own_st);
@@ -348,6 +406,24 @@ extern "C" int kcig_plan_set_tables(kcig_plan *P, const float *stable, const flo
                                     const float *rderiv, int memory)
 {
     if (!P) return set_error(KCIG_ERR_ARG, "null plan");
+    P->stream_tables = 0;
+    if (memory == KCIG_MEM_HOST_STREAM) {
+        if (!stable || !sderiv || !rtable || !rderiv) return set_error(KCIG_ERR_ARG, "missing table pointer");
+        for (DevBuf *b : {&P->own_stab, &P->own_sder, &P->own_rtab, &P->own_rder}) b->release();
+        P->stream_tables = 1;
+        P->h_stab = stable;
+        P->h_sder = sderiv;
+        P->h_rtab = rtable;
+        P->h_rder = rderiv;
+        // the device pointers only mark the tables as set; no kernel reads them
+        P->stab = stable;
+        P->sder = sderiv;
+        P->rtab = rtable;
+        P->rder = rderiv;
+        return KCIG_OK;
+    }
+    if (memory != KCIG_MEM_HOST && memory != KCIG_MEM_DEVICE)
+        return set_error(KCIG_ERR_ARG, "kcig_plan_set_tables: unknown memory kind %d", memory);
     KCIG_TRY(bind_volume(P, P->own_stab, stable, P->g.sny, memory, &P->stab, nullptr, nullptr));
     KCIG_TRY(bind_volume(P, P->own_sder, sderiv, P->g.sny, memory, &P->sder, nullptr, nullptr));
     const bool same = (P->g.rny == P->g.sny);
