@@ -302,6 +302,88 @@ def tables_section(steps: int, warmup: int, threads: int):
 
 
 # -------------------------------------------------------------------- main ---
+# ------------------------------------------------------ config-5 sample ---
+C5_NZ, C5_NX, C5_NT, C5_NPOS, C5_NS = 1201, 4001, 4001, 800, 8
+C5_TOKENS = ["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=90", "angle_step=1", "angle_n=91",
+             "direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05"]
+
+
+def c5_sample_section():
+    """The config-5 grid (1201 x 4001 at 10 m, nt=4001 at 1 ms, 91 angle bins)
+    with its tables kept in pinned host memory (KCIG_MEM_HOST_STREAM), on a
+    sample of the survey: 8 shots x 800 receivers on a fixed spread, tables at
+    the 800 receiver positions (c5's 1000 x 800 survey needs 4001 positions,
+    154 GB of host tables; this sample needs 31 GB).  Tables from kcig_eikods
+    on the device, copied to pinned host memory, freed on the device; then
+    one untimed and one timed migration through the C ABI with host data."""
+    import psutil
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import synth
+    nzx = C5_NZ * C5_NX
+    host_bytes = 2 * C5_NPOS * nzx * 4
+    avail = psutil.virtual_memory().available
+    if avail < 2.5 * host_bytes:
+        return {"skipped": "host memory: %.0f GB available, %.0f GB of host tables" % (avail / 1e9, host_bytes / 1e9)}
+    dz = 0.01
+    x_lo = 16.0
+    v, refl = synth.five_layer_salt(C5_NZ, C5_NX, dz, dz, seed=11)
+    vel = torch.from_numpy(v).cuda()
+    pos = np.float32(x_lo) + np.arange(C5_NPOS, dtype=np.float32) * np.float32(dz)
+    shots = np.zeros((C5_NPOS, 3), np.float32)
+    shots[:, 1] = pos
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = kd.eikods(vel, dz, dz, shots)
+    torch.cuda.synchronize()
+    t_tables = time.perf_counter() - t0
+    T, D = r["time"], r["tds1"]
+    del r["tdl1"]
+    ds_km = 1.0  # shots every 100 receivers
+    g = synth.Geometry(nz=C5_NZ, nx=C5_NX, dz=dz, dx=dz, z0=0, x0=0, ns=C5_NS, s0=float(pos[0]), ds=ds_km,
+                       nh=C5_NPOS, h0=float(pos[0]), dh=dz, cmp=0, nt=C5_NT, dt=0.001, t0=0.0, npos=C5_NPOS,
+                       p0=float(pos[0]), dp=dz)
+    amps = synth.reflectivities(len(refl), 5)
+    data = synth.shot_gathers(T, g, [(rows, a) for rows, a in zip(refl.values(), amps)], 15.0, seed=5,
+                              noise_on_device=True)
+    hT = torch.empty(T.shape, dtype=torch.float32, pin_memory=True)
+    hD = torch.empty(D.shape, dtype=torch.float32, pin_memory=True)
+    hT.copy_(T)
+    hD.copy_(D)
+    hdata = data.cpu().pin_memory()
+    del T, D, r, data, vel
+    torch.cuda.empty_cache()
+    f = lambda x: float(np.float32(x))  # noqa: E731
+    geom = dict(nt=C5_NT, nh=C5_NPOS, ns=C5_NS, t0=0.0, dt=f(0.001), h0=f(pos[0]), dh=f(dz), s0=f(pos[0]),
+                ds=f(ds_km), nz=C5_NZ, nx=C5_NX, z0=0.0, dz=f(dz), x0=0.0, dx=f(dz), sny=C5_NPOS, sy0=f(pos[0]),
+                sdy=f(dz), rny=C5_NPOS, ry0=f(pos[0]), rdy=f(dz))
+    kp = kd.params(*C5_TOKENS)
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    ng = plan.ng
+    himg = torch.zeros((ng, C5_NX, C5_NZ), dtype=torch.float32).pin_memory()
+    free0, total = torch.cuda.mem_get_info()
+    ts = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plan.set_tables(hT, hD, hT, hD, stream=True)
+        plan.migrate(hdata, himg)
+        ts.append(time.perf_counter() - t0)
+    free1, _ = torch.cuda.mem_get_info()
+    plan.close()
+    pairs = C5_NS * C5_NPOS * nzx
+    out = {"workload": "config-5 grid 1201x4001@10m (five-layer salt), nt=4001 dt=1ms, 91 angle bins; sample of "
+                       "8 shots x 800 receivers (cmp=0, 10 m); tables at the 800 receiver positions in pinned "
+                       "host memory (KCIG_MEM_HOST_STREAM)",
+           "value": pairs / ts[-1] / 1e9, "unit": "Gpairs/s", "pairs": pairs, "seconds": ts[-1],
+           "host_tables_gb": host_bytes / 1e9, "tables_seconds": t_tables,
+           "device_used_gb_during_migration": (total - free1) / 1e9,
+           "image_finite": bool(torch.isfinite(himg).all().item()),
+           "image_rms": float(himg.double().pow(2).mean().sqrt().item())}
+    del hT, hD, hdata, himg
+    return out
+
+
 # ------------------------------------------------------- surrogate section ---
 SG_FLOPS_EVAL = 2 * 128 * (256 + 3 * 128 + 3 * 128 + 256)  # tensor FLOPs per (leg, point) in k_sg_fields
 SG_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m, 64 shots x 201 receivers (cmp=0, 10 m), nt=1001 dt=2ms, 61 angle bins, "
@@ -491,6 +573,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
     ap.add_argument("--no-tables", action="store_true", help="skip the table-generator section")
     ap.add_argument("--no-stream", action="store_true", help="skip the host-resident-tables measurement")
+    ap.add_argument("--c5-sample", action="store_true",
+                    help="only the config-5 grid sample with host-resident tables (one JSON object)")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the uneven five-window workload and print its object (profiling)")
     ap.add_argument("--surrogate-steps", type=int, default=40000,
@@ -539,6 +623,9 @@ def main():
     import torch
     import kirch_datuming_b200 as kd
     torch.cuda.set_device(local)
+    if args.c5_sample:
+        print(json.dumps({"c5_sample": c5_sample_section()}), flush=True)
+        return 0
     if args.only_batched:
         print(json.dumps({"batched": batched_section(args.steps, args.warmup)}), flush=True)
         return 0
