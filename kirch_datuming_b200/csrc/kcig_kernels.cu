@@ -635,6 +635,10 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
             if (sb + k < s_hi) {
                 sTP[k] = __ldg(a.STP + (size_t)(sb + k) * nzx + i);
                 sXW[k] = __ldg(a.SXW + (size_t)(sb + k) * nzx + i);
+                // the shot's share of the pick position and of the
+                // antialias width, once per shot block instead of per pair
+                sTP[k].x = (sTP[k].x + a.tau - a.t0) * a.inv_dt;
+                sXW[k].x = fabsf(sXW[k].x) * a.aal;
             } else {
                 sTP[k] = make_double2(0.0, 0.0);
                 sXW[k] = make_float2(0.f, 0.f);
@@ -654,6 +658,9 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
         for (int r = 0; r < nr; r++) {
             double2 rTP = nTP;
             float2 rXW = nXW;
+            // the receiver's share, once per receiver for the KB shots
+            rTP.x *= a.inv_dt;
+            rXW.x = fabsf(rXW.x) * a.aal;
             if (r + 1 < nr) {  // next receiver, one ahead of use
                 const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)__ldg(a.rfi + (size_t)sb * a.nh + r + 1);
                 nTP = __ldg(a.RTP + f1 * nzx + i);
@@ -718,8 +725,11 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 }
                 // kirmig_pick (kirmig.cpp:34-58): sample positions of t,
                 // t-deltat-dt and t+deltat+dt in FP64; every test fails on NaN
-                const double ft0 = (sTP[k].x + rTP.x + a.tau - a.t0) * a.inv_dt;
-                const double sh = fma((double)(fmaxf(fabsf(sXW[k].x), fabsf(rXW.x)) * a.aal), a.inv_dt, 1.0);
+                // ft0 = (Ts + Tr + tau - t0) / dt from the two shares; the
+                // width max(|dTs ds|, |dTr dh|) * aal equals the max of the
+                // scaled shares (aal >= 0, rounding is monotone)
+                const double ft0 = sTP[k].x + rTP.x;
+                const double sh = fma((double)fmaxf(sXW[k].x, rXW.x), a.inv_dt, 1.0);
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
                 const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
                 if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
@@ -727,7 +737,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 const double2 q0 = __ldg(Dk + (int)fl0);
                 const double2 qm = __ldg(Dk + (int)flm);
                 const double2 qp = __ldg(Dk + (int)flp);
-                const float r1 = 1.0f / (1.0f + 2.0f * (float)sh);  // dt / (dt + tp - tm)
+                const float r1 = __fdividef(1.0f, 1.0f + 2.0f * (float)sh);  // dt / (dt + tp - tm), 2 ulp
                 const double sum = 2.0 * fma(ft0 - fl0, q0.y, q0.x) - fma(ftm0 - flm, qm.y, qm.x) -
                                    fma(ftp0 - flp, qp.y, qp.x);
                 const float picked = (float)((double)(r1 * r1) * sum) * aw;
