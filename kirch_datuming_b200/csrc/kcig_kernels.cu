@@ -623,6 +623,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     const double ulo = -1.0e-5, uhi = (double)(a.ng - 1) + 1.0e-5;
     const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;  // u = th*uk - ub
     const double top = (double)(a.nt - 1);
+    const float inv_dt_f = (float)a.inv_dt;
 
     for (int sb = s_lo; sb < s_hi; sb += KB) {
         // last usable sample of this shot's traces: ragged shots (receivers
@@ -638,7 +639,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 // the shot's share of the pick position and of the
                 // antialias width, once per shot block instead of per pair
                 sTP[k].x = (sTP[k].x + a.tau - a.t0) * a.inv_dt;
-                sXW[k].x = fabsf(sXW[k].x) * a.aal;
+                sXW[k].x = fabsf(sXW[k].x) * a.aal * inv_dt_f;
             } else {
                 sTP[k] = make_double2(0.0, 0.0);
                 sXW[k] = make_float2(0.f, 0.f);
@@ -660,7 +661,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
             float2 rXW = nXW;
             // the receiver's share, once per receiver for the KB shots
             rTP.x *= a.inv_dt;
-            rXW.x = fabsf(rXW.x) * a.aal;
+            rXW.x = fabsf(rXW.x) * a.aal * inv_dt_f;
             if (r + 1 < nr) {  // next receiver, one ahead of use
                 const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)__ldg(a.rfi + (size_t)sb * a.nh + r + 1);
                 nTP = __ldg(a.RTP + f1 * nzx + i);
@@ -716,7 +717,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                             b0 = (int)fl;
                             const double f1 = u - fl;
                             w1 = (float)f1;
-                            w0 = (float)(1.0 - f1);
+                            w0 = 1.0f - w1;
                         }
                     } else {
                         b0 = (int)fl;
@@ -726,10 +727,12 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 // kirmig_pick (kirmig.cpp:34-58): sample positions of t,
                 // t-deltat-dt and t+deltat+dt in FP64; every test fails on NaN
                 // ft0 = (Ts + Tr + tau - t0) / dt from the two shares; the
-                // width max(|dTs ds|, |dTr dh|) * aal equals the max of the
-                // scaled shares (aal >= 0, rounding is monotone)
+                // half window in samples, 1 + max(|dTs ds|, |dTr dh|) * aal / dt,
+                // from the max of the scaled shares (the scale is >= 0 and
+                // rounding is monotone), in FP32: it only sets the window
                 const double ft0 = sTP[k].x + rTP.x;
-                const double sh = fma((double)fmaxf(sXW[k].x, rXW.x), a.inv_dt, 1.0);
+                const float shf = 1.0f + fmaxf(sXW[k].x, rXW.x);
+                const double sh = (double)shf;
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
                 const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
                 if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
@@ -737,10 +740,10 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 const double2 q0 = __ldg(Dk + (int)fl0);
                 const double2 qm = __ldg(Dk + (int)flm);
                 const double2 qp = __ldg(Dk + (int)flp);
-                const float r1 = __fdividef(1.0f, 1.0f + 2.0f * (float)sh);  // dt / (dt + tp - tm), 2 ulp
+                const float r1 = __fdividef(1.0f, fmaf(2.0f, shf, 1.0f));  // dt / (dt + tp - tm), 2 ulp
                 const double sum = 2.0 * fma(ft0 - fl0, q0.y, q0.x) - fma(ftm0 - flm, qm.y, qm.x) -
                                    fma(ftp0 - flp, qp.y, qp.x);
-                const float picked = (float)((double)(r1 * r1) * sum) * aw;
+                const float picked = (float)sum * (r1 * r1 * aw);
                 if (b0 >= 0 && b0 < nb) acc[b0 * P + tid] += w0 * picked;
                 if (MODE == 0 && w1 > 0.0f && b0 + 1 >= 0 && b0 + 1 < nb) acc[(b0 + 1) * P + tid] += w1 * picked;
             }
