@@ -579,13 +579,14 @@ __device__ __forceinline__ float depth_weight(float ang, float cutoff, float ban
 // with its time-to-sample mapping and six-term sum in FP64.  Rejections are
 // mostly uniform across a warp (32 neighbouring image points), so skipping
 // them costs little.
-// Resident CTAs per SM the register allocation must allow: 6 CTAs of 128
-// threads (24 warps) is the most the 61-bin accumulators' shared memory
-// admits without spilling registers; occupancy is what this latency-bound
-// loop needs (measured: 16x16 tiles at 2 CTAs/SM 16.2 ms, 16x8 at 6 CTAs/SM
-// 13.8 ms on the 64x64-position case of the benchmark model).
+// Resident CTAs per SM the register allocation must allow: 7 CTAs of 128
+// threads (28 warps, 72 registers, no spills) is the most the 61-bin
+// accumulators' shared memory admits (7 x 31 KB); occupancy is what this
+// latency- and issue-bound loop needs (measured on the benchmark: 6 CTAs/SM
+// at 80 registers 500 ms per launch, 7 CTAs/SM 482 ms; earlier 16x16 tiles at
+// 2 CTAs/SM were slower still).
 #ifndef KCIG_SUM_MINB
-#define KCIG_SUM_MINB 6
+#define KCIG_SUM_MINB 7
 #endif
 
 template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
