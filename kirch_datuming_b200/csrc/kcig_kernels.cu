@@ -621,6 +621,11 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     // cutoff of angle_depth_mute_weight (:200-211) depends only on depth
     const float zf = (a.nz > 1) ? (float)iz / (float)(a.nz - 1) : 0.0f;
     const float cutoff = a.oazmin + zf * (a.oazmax - a.oazmin);
+    // angles (radians) at or below this carry both weights 1 when the angle
+    // taper is off: no FP32 angle is formed for them (the depth weight is
+    // continuous at the cutoff, so the comparison's rounding is immaterial)
+    const bool no_taper = a.ats < 0.0f || a.ate <= a.ats;
+    const double th_one = no_taper ? (double)cutoff / a.deg : -1.0;
     const double ulo = -1.0e-5, uhi = (double)(a.ng - 1) + 1.0e-5;
     const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;  // u = th*uk - ub
     const double top = (double)(a.nt - 1);
@@ -708,9 +713,13 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                         fl = floor(u + 0.5);
                         if (!(fl >= 0.0 && fl < (double)a.ng)) continue;
                     }
-                    const float ang = (float)(th * a.deg);
-                    aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw * apw;
-                    if (!(aw > 0.0f)) continue;
+                    if (th <= th_one) {
+                        aw = tw * apw;
+                    } else {
+                        const float ang = (float)(th * a.deg);
+                        aw = taper_weight(ang, a.ats, a.ate) * depth_weight(ang, cutoff, a.oaztaper) * tw * apw;
+                        if (!(aw > 0.0f)) continue;
+                    }
                     if (MODE == 0) {
                         if (u <= 0.0) { b0 = 0; w0 = 1.0f; w1 = 0.0f; }
                         else if (u >= (double)(a.ng - 1)) { b0 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
