@@ -554,7 +554,7 @@ __device__ __forceinline__ float taper_weight(float ang, float start, float end)
     if (ang <= start) return 1.0f;
     if (ang >= end) return 0.0f;
     const float x = (ang - start) / (end - start);
-    return 0.5f * (1.0f + cosf(3.14159265358979f * x));
+    return 0.5f * (1.0f + cospif(x));  // cos(pi x) for x in [0, 1]: no large-argument path
 }
 
 __device__ __forceinline__ float depth_weight(float ang, float cutoff, float band)
@@ -563,7 +563,7 @@ __device__ __forceinline__ float depth_weight(float ang, float cutoff, float ban
     if (ang <= cutoff) return 1.0f;
     if (ang >= cutoff + band) return 0.0f;
     const float u = (ang - cutoff) / band;
-    return 0.5f * (1.0f + cosf(3.14159265358979f * u));
+    return 0.5f * (1.0f + cospif(u));
 }
 
 // One CTA owns a TZ x TX image tile (one thread per image point) and keeps
