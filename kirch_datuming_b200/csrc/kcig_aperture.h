@@ -4,7 +4,8 @@
 
 namespace kcig {
 
-// kirchmig2d_cig.cpp:226-269: raised-cosine aperture legs, max-combined with
+// kirchmig2d_cig.cpp:226-269: raised-cosine aperture legs (cos(pi x) as cospi,
+// which needs no large-argument reduction), max-combined with
 // the shallow floor disk.  Evaluated once per (position, image point) instead
 // of once per pair: the value depends only on this leg.
 __device__ __forceinline__ double leg_cone(double leg, double aper, double band)
@@ -14,7 +15,7 @@ __device__ __forceinline__ double leg_cone(double leg, double aper, double band)
     const double inner = aper - band;
     if (leg <= inner) return 1.0;
     if (leg >= aper) return 0.0;
-    return 0.5 * (1.0 + cos(3.14159265358979323846 * ((leg - inner) / band)));
+    return 0.5 * (1.0 + cospi((leg - inner) / band));
 }
 
 __device__ __forceinline__ double leg_floor(double d, double rmin, double rt)
@@ -24,11 +25,11 @@ __device__ __forceinline__ double leg_floor(double d, double rmin, double rt)
     const double inner = rmin - rt;
     if (inner <= 0.0) {
         if (d >= rmin) return 0.0;
-        return 0.5 * (1.0 + cos(3.14159265358979323846 * (d / rmin)));
+        return 0.5 * (1.0 + cospi(d / rmin));
     }
     if (d <= inner) return 1.0;
     if (d >= rmin) return 0.0;
-    return 0.5 * (1.0 + cos(3.14159265358979323846 * ((d - inner) / rt)));
+    return 0.5 * (1.0 + cospi((d - inner) / rt));
 }
 
 // the leg weight of :1221-1263 for a leg at surface position `pos` and the

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
             const double t = a.t0 + (double)i * a.dt;
             double w = 0.0;
             if (t >= boundary + a.taper) w = 1.0;
-            else if (t > boundary) w = 0.5 * (1.0 - cos(kPi * ((t - boundary) / a.taper)));
+            else if (t > boundary) w = 0.5 * (1.0 - cospi((t - boundary) / a.taper));
             v *= w;
         }
         s[i] = v;

@@ -144,8 +144,10 @@ __device__ __forceinline__ void sg_features(unsigned char *act, int r, int p0, i
 {
     const float d = fstep * u;
     float s, c, sd, cd;
-    sincosf(d * (float)(p0 + 1), &s, &c);
-    sincosf(d, &sd, &cd);
+    // angles as multiples of pi (sincospif: no large-argument reduction)
+    const float dp = d * 0.318309886f;
+    sincospif(dp * (float)(p0 + 1), &s, &c);
+    sincospif(dp, &sd, &cd);
     for (int g = 0; g < np / 4; g++) {
         uint32_t pk[4];
 #pragma unroll
@@ -166,8 +168,9 @@ __device__ __forceinline__ float sg_feature_grad(uint32_t tG, int c0, int nq, fl
 {
     const float d = fstep * u;
     float s, c, sd, cd;
-    sincosf(d * (float)(c0 / 2 + 1), &s, &c);
-    sincosf(d, &sd, &cd);
+    const float dp = d * 0.318309886f;
+    sincospif(dp * (float)(c0 / 2 + 1), &s, &c);
+    sincospif(dp, &sd, &cd);
     float acc = 0.0f;
     for (int q = 0; q < nq; q++) {
         float v[32];
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
             if (tid < NF) {
                 float sn, cs;
                 const float th = (float)(tid + 1) * n.fstep * u0;
-                sincosf(th, &sn, &cs);
+                sincospif(th * 0.318309886f, &sn, &cs);
                 fx[2 * tid] = __bfloat162float(__float2bfloat16_rn(sn));
                 fx[2 * tid + 1] = __bfloat162float(__float2bfloat16_rn(cs));
                 dfx[2 * tid] = (float)(tid + 1) * n.fstep * cs;
