@@ -722,7 +722,10 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "kernel": "k_sum", "kernel_ms": ksum_ms,
                      "algorithmic_bytes_per_pair": B_PAIR,
-                     "traffic": (tpp * pairs) if tpp is not None else None},
+                     "traffic": (tpp * pairs) if tpp is not None else None,
+                     "note": "16 B/pair counts the receiver leg's fields once per pair; k_sum loads each "
+                             "receiver leg once per block of 4 shots, so its DRAM traffic (ncu, 'traffic') is "
+                             "below the algorithmic bytes and frac can pass 1: the kernel is issue-bound"},
         "e2e": {"value": world * pairs / (e2e_ms / 1e3) / 1e9 if world == 1 else None, "unit": "Gpairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "streamed_tables": None if stream_ms is None else {

@@ -566,6 +566,14 @@ __device__ __forceinline__ float depth_weight(float ang, float cutoff, float ban
     return 0.5f * (1.0f + cospif(u));
 }
 
+// floor(x) + 1.5 * 2^52 for 0 <= x < 2^31 (also -1 <= x < 0), exact: the sum
+// is rounded down onto the integer grid of [2^52, 2^53), so its low mantissa
+// word is floor(x) as a two's-complement int (__double2loint) and subtracting
+// the shift again gives floor(x) as a double.  Two FP64 adds instead of a
+// round-to-integer and a conversion.
+static constexpr double kFloorShift = 6755399441055744.0;
+__device__ __forceinline__ double floor_shift(double x) { return __dadd_rd(x, kFloorShift); }
+
 // One CTA owns a TZ x TX image tile (one thread per image point) and keeps
 // its [bins][points] FP32 accumulators in shared memory: each thread only
 // touches its own column, so there are no atomics and no block barriers.
@@ -630,6 +638,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
     const double uk = a.deg * a.uinv, ub = a.ug0 * a.uinv;  // u = th*uk - ub
     const double top = (double)(a.nt - 1);
     const float inv_dt_f = (float)a.inv_dt;
+    const bool aal_pos = a.aal >= 0.0f;
 
     for (int sb = s_lo; sb < s_hi; sb += KB) {
         // last usable sample of this shot's traces: ragged shots (receivers
@@ -703,11 +712,10 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                     double th = fabs(sTP[k].y - rTP.y);
                     th = (th > kPiD) ? kTwoPi - th : th;
                     const double u = fma(th, uk, -ub);  // bin coordinate; NaN: vanishing gradient
-                    double fl;
+                    double fl = 0.0;
                     if (MODE == 0) {
                         // value_to_linear_bins (:54-79)
                         if (!(u >= ulo && u <= uhi)) continue;
-                        fl = floor(u);
                     } else {
                         // value_to_nearest_bin (:35-41)
                         fl = floor(u + 0.5);
@@ -724,9 +732,9 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                         if (u <= 0.0) { b0 = 0; w0 = 1.0f; w1 = 0.0f; }
                         else if (u >= (double)(a.ng - 1)) { b0 = a.ng - 1; w0 = 1.0f; w1 = 0.0f; }
                         else {
-                            b0 = (int)fl;
-                            const double f1 = u - fl;
-                            w1 = (float)f1;
+                            const double fu = floor_shift(u);  // u in (0, ng - 1)
+                            b0 = __double2loint(fu);
+                            w1 = (float)(u - (fu - kFloorShift));
                             w0 = 1.0f - w1;
                         }
                     } else {
@@ -744,15 +752,27 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                 const float shf = 1.0f + fmaxf(sXW[k].x, rXW.x);
                 const double sh = (double)shf;
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
-                const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
-                if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
+                // the reference's six tests on the three floors (0 <= flm <=
+                // fl0 <= flp < top); with aal >= 0 the half window is >= 1 or
+                // NaN, so fl0 lies between the other two and the tests reduce
+                // to ftm0 >= 0 and ftp0 < top (top is an integer; NaN fails)
+                if (aal_pos) {
+                    if (!(ftm0 >= 0.0 && ftp0 < topk)) continue;
+                } else {
+                    const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
+                    if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
+                }
+                // all three positions are now in [0, nt - 1): floors by the
+                // shifted add, the sample indices from its low word
+                const double f0s = floor_shift(ft0), fms = floor_shift(ftm0), fps = floor_shift(ftp0);
                 const double2 *Dk = a.D + (size_t)trc * a.nt;
-                const double2 q0 = __ldg(Dk + (int)fl0);
-                const double2 qm = __ldg(Dk + (int)flm);
-                const double2 qp = __ldg(Dk + (int)flp);
+                const double2 q0 = __ldg(Dk + __double2loint(f0s));
+                const double2 qm = __ldg(Dk + __double2loint(fms));
+                const double2 qp = __ldg(Dk + __double2loint(fps));
                 const float r1 = __fdividef(1.0f, fmaf(2.0f, shf, 1.0f));  // dt / (dt + tp - tm), 2 ulp
-                const double sum = 2.0 * fma(ft0 - fl0, q0.y, q0.x) - fma(ftm0 - flm, qm.y, qm.x) -
-                                   fma(ftp0 - flp, qp.y, qp.x);
+                const double sum = 2.0 * fma(ft0 - (f0s - kFloorShift), q0.y, q0.x) -
+                                   fma(ftm0 - (fms - kFloorShift), qm.y, qm.x) -
+                                   fma(ftp0 - (fps - kFloorShift), qp.y, qp.x);
                 const float picked = (float)sum * (r1 * r1 * aw);
                 if (b0 >= 0 && b0 < nb) acc[b0 * P + tid] += w0 * picked;
                 if (MODE == 0 && w1 > 0.0f && b0 + 1 >= 0 && b0 + 1 < nb) acc[(b0 + 1) * P + tid] += w1 * picked;
