@@ -488,14 +488,15 @@ MUTE_SLOPES = (50.0, 40.0, 30.0, 20.0, 10.0)
 MUTE_TAPERS = (0.05, 0.06, 0.07, 0.08, 0.10)
 
 
-def batched_section(steps: int, warmup: int, seed: int = 21):
+def batched_section(steps: int, warmup: int, seed: int = 21, small: bool = False):
     """The uneven-workload configuration: every depth window is a plan of its
     own with ragged shots prepared on the device, the summation tile is
-    autotuned per window, and one CUDA graph replays all five windows."""
+    autotuned per window, and one CUDA graph replays all five windows.
+    small: the first window and 64 shots only (a case for profilers)."""
     import torch
     import kirch_datuming_b200 as kd
     from kirch_datuming_b200 import synth
-    nz_all, nx, dz, nshot, dh, nrg, nt_max = 201, 401, 0.01, 512, 0.008, 501, 4001
+    nz_all, nx, dz, nshot, dh, nrg, nt_max = 201, 401, 0.01, 64 if small else 512, 0.008, 501, 4001
     rng = np.random.default_rng(seed)
     nh = rng.integers(96, 481, nshot)
     nts = rng.integers(1501, 4002, nshot)
@@ -503,7 +504,7 @@ def batched_section(steps: int, warmup: int, seed: int = 21):
     i0 = np.clip(np.round((sx - nh * dh / 2) / dh).astype(int), 0, nrg - nh)
     vel = synth.velocity_linear_vz(nz_all, nx, dz)
     amps = synth.reflectivities(5, seed)
-    rows = [(0, 40), (40, 80), (80, 120), (120, 160), (160, 201)]
+    rows = [(0, 40), (40, 80), (80, 120), (120, 160), (160, 201)][:1 if small else 5]
     f = lambda v: float(np.float32(v))  # noqa: E731
     plans, images, tuned, pairs = [], [], [], 0
     for w, (r0, r1) in enumerate(rows):
@@ -554,7 +555,8 @@ def batched_section(steps: int, warmup: int, seed: int = 21):
     graph.close()
     for p in plans:
         p.close()
-    return {"workload": BATCH_WORKLOAD, "pairs_per_step": pairs,
+    return {"workload": BATCH_WORKLOAD if not small else "first window of: " + BATCH_WORKLOAD.replace("512", "64"),
+            "pairs_per_step": pairs,
             "value": pairs / (ms_graph / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_graph,
             "direct": {"value": pairs / (ms_direct / 1e3) / 1e9, "ms_per_step": ms_direct,
                        "stage_ms_per_window": stages},
@@ -627,7 +629,8 @@ def main():
         print(json.dumps({"c5_sample": c5_sample_section()}), flush=True)
         return 0
     if args.only_batched:
-        print(json.dumps({"batched": batched_section(args.steps, args.warmup)}), flush=True)
+        print(json.dumps({"batched": batched_section(args.steps, args.warmup, small=args.size == "small")}),
+              flush=True)
         return 0
     dist = None
     if world > 1:
@@ -747,7 +750,7 @@ def main():
         plan.close()
         del T, D, data, image
         torch.cuda.empty_cache()
-        line["batched"] = batched_section(args.steps, args.warmup)
+        line["batched"] = batched_section(args.steps, args.warmup, small=args.size == "small")
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

@@ -15,8 +15,9 @@ namespace kcig {
 int set_error(int code, const char *fmt, ...);
 // Raises a kernel's dynamic shared-memory limit to at least `bytes` on the
 // current device, calling the runtime only when the limit must grow (so a
-// launch sequence under stream capture makes no attribute calls once warm).
-int set_dyn_smem(const void *fn, int bytes);
+// launch sequence under stream capture makes no attribute calls once warm);
+// carveout >= 0 also sets the kernel's preferred shared-memory carveout then.
+int set_dyn_smem(const void *fn, int bytes, int carveout = -1);
 int cuda_error(cudaError_t e, const char *what);
 
 #define KCIG_CUDA(call)                                               \

@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(64) k_doubint_plain(const IN *in, OUT *out, in
     for (int i = lane; i < nt; i += 32) out[(size_t)tr * nt + i] = (OUT)s[i];
 }
 
-int set_dyn_smem(const void *fn, int bytes)
+int set_dyn_smem(const void *fn, int bytes, int carveout)
 {
     static std::mutex mu;
     static std::map<std::pair<int, const void *>, int> done;
@@ -176,6 +176,7 @@ int set_dyn_smem(const void *fn, int bytes)
     int &have = done[std::make_pair(dev, fn)];
     if (bytes <= have) return KCIG_OK;
     KCIG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (carveout >= 0) KCIG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, carveout));
     have = bytes;
     return KCIG_OK;
 }
@@ -587,18 +588,20 @@ __device__ __forceinline__ double floor_shift(double x) { return __dadd_rd(x, kF
 // with its time-to-sample mapping and six-term sum in FP64.  Rejections are
 // mostly uniform across a warp (32 neighbouring image points), so skipping
 // them costs little.
-// Resident CTAs per SM the register allocation must allow: 7 CTAs of 128
-// threads (28 warps, 72 registers, no spills) is the most the 61-bin
-// accumulators' shared memory admits (7 x 31 KB); occupancy is what this
-// latency- and issue-bound loop needs (measured on the benchmark: 6 CTAs/SM
-// at 80 registers 500 ms per launch, 7 CTAs/SM 482 ms; earlier 16x16 tiles at
-// 2 CTAs/SM were slower still).
+// Resident CTAs of 128 threads per SM the register allocation must allow
+// (scaled for other tile sizes, so every tile gets 28 warps and at most 72
+// registers): 7 CTAs of 128 threads is the most the 61-bin accumulators'
+// shared memory admits (7 x 31 KB); occupancy is what this latency- and
+// issue-bound loop needs (measured on the benchmark: 6 CTAs/SM at 80
+// registers 500 ms per launch, 7 CTAs/SM 482 ms; earlier 16x16 tiles at 2
+// CTAs/SM were slower still; 8x8 tiles of ragged shots at 82 registers held
+// 10 CTAs, 20 warps, and waited on their gathers).
 #ifndef KCIG_SUM_MINB
 #define KCIG_SUM_MINB 7
 #endif
 
 template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
-__global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_constant__ SumArgs a)
+__global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum(const __grid_constant__ SumArgs a)
 {
     constexpr int P = TZ * TX;
     constexpr double kPiD = 3.141592653589793238463, kTwoPi = 6.283185307179586476925;
@@ -666,10 +669,15 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
         const int nr = (!SHARED_R && a.snh) ? __ldg(a.snh + sb) : a.nh;
         double2 nTP = make_double2(0.0, 0.0);
         float2 nXW = make_float2(0.f, 0.f);
+        // unshared receivers: field index of the receiver after next, so the
+        // index load does not stand in front of the field load
+        const int *rfi_s = a.rfi + (size_t)sb * a.nh;
+        int fnext = 0;
         if (nr > 0) {
-            const size_t f0 = SHARED_R ? 0 : (size_t)__ldg(a.rfi + (size_t)sb * a.nh);
+            const size_t f0 = SHARED_R ? 0 : (size_t)__ldg(rfi_s);
             nTP = __ldg(a.RTP + f0 * nzx + i);
             nXW = __ldg(a.RXW + f0 * nzx + i);
+            if (!SHARED_R && nr > 1) fnext = __ldg(rfi_s + 1);
         }
         for (int r = 0; r < nr; r++) {
             double2 rTP = nTP;
@@ -678,9 +686,10 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
             rTP.x *= a.inv_dt;
             rXW.x = fabsf(rXW.x) * a.aal * inv_dt_f;
             if (r + 1 < nr) {  // next receiver, one ahead of use
-                const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)__ldg(a.rfi + (size_t)sb * a.nh + r + 1);
+                const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)fnext;
                 nTP = __ldg(a.RTP + f1 * nzx + i);
                 nXW = __ldg(a.RXW + f1 * nzx + i);
+                if (!SHARED_R && r + 2 < nr) fnext = __ldg(rfi_s + r + 2);
             }
 #pragma unroll
             for (int k = 0; k < KB; k++) {
@@ -774,8 +783,9 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB) k_sum(const __grid_cons
                                    fma(ftm0 - (fms - kFloorShift), qm.y, qm.x) -
                                    fma(ftp0 - (fps - kFloorShift), qp.y, qp.x);
                 const float picked = (float)sum * (r1 * r1 * aw);
-                if (b0 >= 0 && b0 < nb) acc[b0 * P + tid] += w0 * picked;
-                if (MODE == 0 && w1 > 0.0f && b0 + 1 >= 0 && b0 + 1 < nb) acc[(b0 + 1) * P + tid] += w1 * picked;
+                // 0 <= b < nb as one unsigned test each
+                if ((unsigned)b0 < (unsigned)nb) acc[b0 * P + tid] += w0 * picked;
+                if (MODE == 0 && w1 > 0.0f && (unsigned)(b0 + 1) < (unsigned)nb) acc[(b0 + 1) * P + tid] += w1 * picked;
             }
         }
     }
@@ -921,7 +931,10 @@ static int launch_sum_t(const SumArgs &a, int nb, cudaStream_t st)
     constexpr int P = TZ * TX;
     const size_t sm = (size_t)nb * P * sizeof(float);
     auto kern = k_sum<TZ, TX, KB, SR, MODE>;
-    KCIG_TRY(set_dyn_smem((const void *)kern, (int)sm));
+    // all of the unified L1/shared memory as shared: the accumulators of as
+    // many CTAs as the registers allow (the driver's own choice held 8x8
+    // tiles to 10 CTAs per SM)
+    KCIG_TRY(set_dyn_smem((const void *)kern, (int)sm, cudaSharedmemCarveoutMaxShared));
     const int tiles = ((a.nz + TZ - 1) / TZ) * ((a.nx + TX - 1) / TX);
     kern<<<dim3(tiles, a.nsplit > 1 ? a.nsplit : 1), P, sm, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
