@@ -71,10 +71,6 @@ struct kcig_plan {
     int use_graph = 0;                                     // replay kcig_migrate_prepared as a CUDA graph
     int tile = 0;                                          // summation tile variant (kcig_plan_autotune)
     cudaStream_t own_st = nullptr;                         // capture stream when the plan's is the legacy one
-    // host data of kcig_migrate: copied on its own stream while the leg
-    // fields (which need only the tables) are computed on st
-    cudaStream_t cst = nullptr;
-    cudaEvent_t ev_prior = nullptr, ev_data = nullptr;
 };
 
 // Ragged shots on the device, batched (kcig_shots_prepare); the launch
@@ -117,23 +113,6 @@ int upload(DevBuf &b, const void *src, size_t bytes, cudaStream_t st)
 {
     KCIG_TRY(b.ensure(bytes));
     KCIG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, st));
-    return KCIG_OK;
-}
-
-// Starts the copy of `bytes` of host data into P->d_data on the plan's copy
-// stream, after the work already queued on st (which may still read the
-// buffer); P->ev_data marks its end.  The copy engine then runs beside the
-// kernels st queues next.
-int upload_data_async(kcig_plan *P, const void *src, size_t bytes)
-{
-    KCIG_TRY(P->d_data.ensure(bytes));
-    if (!P->cst) KCIG_CUDA(cudaStreamCreateWithFlags(&P->cst, cudaStreamNonBlocking));
-    if (!P->ev_prior) KCIG_CUDA(cudaEventCreateWithFlags(&P->ev_prior, cudaEventDisableTiming));
-    if (!P->ev_data) KCIG_CUDA(cudaEventCreateWithFlags(&P->ev_data, cudaEventDisableTiming));
-    KCIG_CUDA(cudaEventRecord(P->ev_prior, P->st));
-    KCIG_CUDA(cudaStreamWaitEvent(P->cst, P->ev_prior, 0));
-    KCIG_CUDA(cudaMemcpyAsync(P->d_data.p, src, bytes, cudaMemcpyHostToDevice, P->cst));
-    KCIG_CUDA(cudaEventRecord(P->ev_data, P->cst));
     return KCIG_OK;
 }
 
@@ -394,9 +373,6 @@ extern "C" int kcig_plan_destroy(kcig_plan *P)
     for (DevBuf *b : bufs) b->release();
     release_shots(P);
     if (P->own_st) cudaStreamDestroy(P->own_st);
-    if (P->cst) cudaStreamDestroy(P->cst);
-    if (P->ev_prior) cudaEventDestroy(P->ev_prior);
-    if (P->ev_data) cudaEventDestroy(P->ev_data);
     delete P;
     return KCIG_OK;
 }
@@ -548,17 +524,8 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     const float *d_data = data;
     float *d_img = image;
     const size_t data_bytes = (size_t)g.ns * g.nh * g.nt * sizeof(float);
-    // host data: copied beside the leg-field kernels, joined before the
-    // first prelude (and in any case before this call returns)
-    bool data_pending = false;
-    struct JoinCopy {  // every return path waits for the copy of the caller's data
-        kcig_plan *P;
-        const bool &pending;
-        ~JoinCopy() { if (pending) cudaStreamSynchronize(P->cst); }
-    } join{P, data_pending};
     if (memory == KCIG_MEM_HOST) {
-        KCIG_TRY(upload_data_async(P, data, data_bytes));
-        data_pending = true;
+        KCIG_TRY(upload(P->d_data, data, data_bytes, st));
         d_data = P->d_data.as<float>();
         KCIG_TRY(P->d_image.ensure((size_t)P->ng * nzx * sizeof(float)));
         d_img = P->d_image.as<float>();
@@ -768,14 +735,6 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             pa.slope = p.direct_mute_slope;
             pa.intercept = p.direct_mute_intercept;
             pa.taper = p.direct_mute_taper;
-            if (data_pending) {
-                cudaError_t e = cudaStreamWaitEvent(st, P->ev_data, 0);
-                if (e != cudaSuccess) {
-                    rc = cuda_error(e, "cudaStreamWaitEvent(data)");
-                    break;
-                }
-                data_pending = false;
-            }
             rc = launch_prelude(pa, st);
             if (rc) break;
             P->all_launches++;
@@ -852,12 +811,6 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     if (rc == KCIG_OK && memory == KCIG_MEM_HOST) {
         cudaError_t e = cudaMemcpyAsync(image, d_img, (size_t)P->ng * nzx * sizeof(float), cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) rc = cuda_error(e, "cudaMemcpyAsync(image)");
-    }
-    // the caller's data buffer must not be read after this call returns
-    if (data_pending) {
-        cudaError_t e = cudaStreamSynchronize(P->cst);
-        if (rc == KCIG_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(data)");
-        data_pending = false;
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == KCIG_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(migrate)");
