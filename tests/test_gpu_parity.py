@@ -117,6 +117,27 @@ def test_many_bins_chunked(golden):
     assert oracle.rel_l2(img, ref) <= TOL_FP64
 
 
+@pytest.mark.parametrize("aal", ["0", "-0.001", "3"])
+def test_antialias_values(golden, aal):
+    # the summation tests the pick window in two ways: a short form for
+    # antialias >= 0 (half window >= 1 sample) and the reference's six tests
+    # otherwise; both against the FP64 oracle
+    import oracle as O
+    kp = kd.params(*golden.tokens("base"), "antialias=" + aal)
+    assert kp.antialias == np.float32(float(aal))
+    geom = golden.geometry_dict("base")
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    T, D = golden.tables()
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    plan.set_tables(T, D, T, D)
+    img = np.zeros((axis[0], geom["nx"], geom["nz"]), np.float32)
+    plan.migrate(np.ascontiguousarray(golden.data("base")), img)
+    plan.close()
+    ref = O.migrate_adj(_cases.oracle_params(kp, geom, axis), golden.data("base"), T, D, T, D)
+    assert np.abs(ref).max() > 0
+    assert oracle.rel_l2(img, ref) <= TOL_FP64
+
+
 @pytest.mark.parametrize("ns,nh", [(1, 21), (5, 1), (1, 1)])
 def test_single_shot_or_receiver(golden, ns, nh):
     import oracle as O
