@@ -642,6 +642,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
     const double top = (double)(a.nt - 1);
     const float inv_dt_f = (float)a.inv_dt;
     const bool aal_pos = a.aal >= 0.0f;
+    const float aal_abs = fabsf(a.aal), aal_sgn = aal_pos ? 1.0f : -1.0f;
 
     for (int sb = s_lo; sb < s_hi; sb += KB) {
         // last usable sample of this shot's traces: ragged shots (receivers
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 // the shot's share of the pick position and of the
                 // antialias width, once per shot block instead of per pair
                 sTP[k].x = (sTP[k].x + a.tau - a.t0) * a.inv_dt;
-                sXW[k].x = fabsf(sXW[k].x) * a.aal * inv_dt_f;
+                sXW[k].x = fabsf(sXW[k].x) * aal_abs * inv_dt_f;
             } else {
                 sTP[k] = make_double2(0.0, 0.0);
                 sXW[k] = make_float2(0.f, 0.f);
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
             float2 rXW = nXW;
             // the receiver's share, once per receiver for the KB shots
             rTP.x *= a.inv_dt;
-            rXW.x = fabsf(rXW.x) * a.aal * inv_dt_f;
+            rXW.x = fabsf(rXW.x) * aal_abs * inv_dt_f;
             if (r + 1 < nr) {  // next receiver, one ahead of use
                 const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)fnext;
                 nTP = __ldg(a.RTP + f1 * nzx + i);
@@ -755,10 +756,11 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 // t-deltat-dt and t+deltat+dt in FP64; every test fails on NaN
                 // ft0 = (Ts + Tr + tau - t0) / dt from the two shares; the
                 // half window in samples, 1 + max(|dTs ds|, |dTr dh|) * aal / dt,
-                // from the max of the scaled shares (the scale is >= 0 and
-                // rounding is monotone), in FP32: it only sets the window
+                // as 1 + sign(aal) * (max of the shares scaled by |aal| / dt):
+                // the scale is >= 0 and rounding is monotone, and negation is
+                // exact; in FP32: it only sets the window
                 const double ft0 = sTP[k].x + rTP.x;
-                const float shf = 1.0f + fmaxf(sXW[k].x, rXW.x);
+                const float shf = fmaf(aal_sgn, fmaxf(sXW[k].x, rXW.x), 1.0f);
                 const double sh = (double)shf;
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
                 // the reference's six tests on the three floors (0 <= flm <=
