@@ -302,17 +302,17 @@ def tables_section(steps: int, warmup: int, threads: int):
 
 
 # -------------------------------------------------------------------- main ---
-# ------------------------------------------------------ config-5 sample ---
-C5_NZ, C5_NX, C5_NT, C5_NPOS, C5_NS = 1201, 4001, 4001, 800, 8
-C5_TOKENS = ["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=90", "angle_step=1", "angle_n=91",
+# ------------------------------------------- 1201x4001 grid sample ---
+BIG_NZ, BIG_NX, BIG_NT, BIG_NPOS, BIG_NS = 1201, 4001, 4001, 800, 8
+BIG_TOKENS = ["cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=90", "angle_step=1", "angle_n=91",
              "direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05"]
 
 
-def c5_sample_section():
-    """The config-5 grid (1201 x 4001 at 10 m, nt=4001 at 1 ms, 91 angle bins)
+def large_grid_sample_section():
+    """The 1201 x 4001 grid at 10 m (nt=4001 at 1 ms, 91 angle bins)
     with its tables kept in pinned host memory (KCIG_MEM_HOST_STREAM), on a
     sample of the survey: 8 shots x 800 receivers on a fixed spread, tables at
-    the 800 receiver positions (c5's 1000 x 800 survey needs 4001 positions,
+    the 800 receiver positions (the full 1000 x 800 survey needs 4001 positions,
     154 GB of host tables; this sample needs 31 GB).  Tables from kcig_eikods
     on the device, copied to pinned host memory, freed on the device; then
     one untimed and one timed migration through the C ABI with host data."""
@@ -320,17 +320,17 @@ def c5_sample_section():
     import torch
     import kirch_datuming_b200 as kd
     from kirch_datuming_b200 import synth
-    nzx = C5_NZ * C5_NX
-    host_bytes = 2 * C5_NPOS * nzx * 4
+    nzx = BIG_NZ * BIG_NX
+    host_bytes = 2 * BIG_NPOS * nzx * 4
     avail = psutil.virtual_memory().available
     if avail < 2.5 * host_bytes:
         return {"skipped": "host memory: %.0f GB available, %.0f GB of host tables" % (avail / 1e9, host_bytes / 1e9)}
     dz = 0.01
     x_lo = 16.0
-    v, refl = synth.five_layer_salt(C5_NZ, C5_NX, dz, dz, seed=11)
+    v, refl = synth.five_layer_salt(BIG_NZ, BIG_NX, dz, dz, seed=11)
     vel = torch.from_numpy(v).cuda()
-    pos = np.float32(x_lo) + np.arange(C5_NPOS, dtype=np.float32) * np.float32(dz)
-    shots = np.zeros((C5_NPOS, 3), np.float32)
+    pos = np.float32(x_lo) + np.arange(BIG_NPOS, dtype=np.float32) * np.float32(dz)
+    shots = np.zeros((BIG_NPOS, 3), np.float32)
     shots[:, 1] = pos
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -340,8 +340,8 @@ def c5_sample_section():
     T, D = r["time"], r["tds1"]
     del r["tdl1"]
     ds_km = 1.0  # shots every 100 receivers
-    g = synth.Geometry(nz=C5_NZ, nx=C5_NX, dz=dz, dx=dz, z0=0, x0=0, ns=C5_NS, s0=float(pos[0]), ds=ds_km,
-                       nh=C5_NPOS, h0=float(pos[0]), dh=dz, cmp=0, nt=C5_NT, dt=0.001, t0=0.0, npos=C5_NPOS,
+    g = synth.Geometry(nz=BIG_NZ, nx=BIG_NX, dz=dz, dx=dz, z0=0, x0=0, ns=BIG_NS, s0=float(pos[0]), ds=ds_km,
+                       nh=BIG_NPOS, h0=float(pos[0]), dh=dz, cmp=0, nt=BIG_NT, dt=0.001, t0=0.0, npos=BIG_NPOS,
                        p0=float(pos[0]), dp=dz)
     amps = synth.reflectivities(len(refl), 5)
     data = synth.shot_gathers(T, g, [(rows, a) for rows, a in zip(refl.values(), amps)], 15.0, seed=5,
@@ -354,13 +354,13 @@ def c5_sample_section():
     del T, D, r, data, vel
     torch.cuda.empty_cache()
     f = lambda x: float(np.float32(x))  # noqa: E731
-    geom = dict(nt=C5_NT, nh=C5_NPOS, ns=C5_NS, t0=0.0, dt=f(0.001), h0=f(pos[0]), dh=f(dz), s0=f(pos[0]),
-                ds=f(ds_km), nz=C5_NZ, nx=C5_NX, z0=0.0, dz=f(dz), x0=0.0, dx=f(dz), sny=C5_NPOS, sy0=f(pos[0]),
-                sdy=f(dz), rny=C5_NPOS, ry0=f(pos[0]), rdy=f(dz))
-    kp = kd.params(*C5_TOKENS)
+    geom = dict(nt=BIG_NT, nh=BIG_NPOS, ns=BIG_NS, t0=0.0, dt=f(0.001), h0=f(pos[0]), dh=f(dz), s0=f(pos[0]),
+                ds=f(ds_km), nz=BIG_NZ, nx=BIG_NX, z0=0.0, dz=f(dz), x0=0.0, dx=f(dz), sny=BIG_NPOS, sy0=f(pos[0]),
+                sdy=f(dz), rny=BIG_NPOS, ry0=f(pos[0]), rdy=f(dz))
+    kp = kd.params(*BIG_TOKENS)
     plan = kd.Plan(kp, kd.geometry(**geom))
     ng = plan.ng
-    himg = torch.zeros((ng, C5_NX, C5_NZ), dtype=torch.float32).pin_memory()
+    himg = torch.zeros((ng, BIG_NX, BIG_NZ), dtype=torch.float32).pin_memory()
     free0, total = torch.cuda.mem_get_info()
     ts = []
     for _ in range(2):
@@ -371,8 +371,8 @@ def c5_sample_section():
         ts.append(time.perf_counter() - t0)
     free1, _ = torch.cuda.mem_get_info()
     plan.close()
-    pairs = C5_NS * C5_NPOS * nzx
-    out = {"workload": "config-5 grid 1201x4001@10m (five-layer salt), nt=4001 dt=1ms, 91 angle bins; sample of "
+    pairs = BIG_NS * BIG_NPOS * nzx
+    out = {"workload": "1201x4001@10m grid (five-layer salt), nt=4001 dt=1ms, 91 angle bins; sample of "
                        "8 shots x 800 receivers (cmp=0, 10 m); tables at the 800 receiver positions in pinned "
                        "host memory (KCIG_MEM_HOST_STREAM)",
            "value": pairs / ts[-1] / 1e9, "unit": "Gpairs/s", "pairs": pairs, "seconds": ts[-1],
@@ -391,7 +391,7 @@ SG_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m, 64 shots x 201 receivers (cmp=0, 10 m
 
 
 def surrogate_section(train_steps: int, steps: int, warmup: int):
-    """Table path vs learned-surrogate path on the same config-1 gathers:
+    """Table path vs learned-surrogate path on the same v(z) 201x401 gathers:
     throughput of each (device time per migration), the surrogate's training
     time and traveltime error on the tables, and the image error of the
     surrogate path (and of the straight-ray background alone, the method
@@ -399,7 +399,7 @@ def surrogate_section(train_steps: int, steps: int, warmup: int):
     import torch
     import kirch_datuming_b200 as kd
     from kirch_datuming_b200 import synth
-    vel, T1, D1, data1, g = synth.config1_workload(seed=4)
+    vel, T1, D1, data1, g = synth.vz_small_workload(seed=4)
     f = lambda v: float(np.float32(v))  # noqa: E731
     geom = kd.geometry(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds),
                        nz=g.nz, nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0,
@@ -575,8 +575,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
     ap.add_argument("--no-tables", action="store_true", help="skip the table-generator section")
     ap.add_argument("--no-stream", action="store_true", help="skip the host-resident-tables measurement")
-    ap.add_argument("--c5-sample", action="store_true",
-                    help="only the config-5 grid sample with host-resident tables (one JSON object)")
+    ap.add_argument("--large-grid-sample", action="store_true",
+                    help="only the 1201x4001 grid sample with host-resident tables (one JSON object)")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the uneven five-window workload and print its object (profiling)")
     ap.add_argument("--surrogate-steps", type=int, default=40000,
@@ -625,8 +625,8 @@ def main():
     import torch
     import kirch_datuming_b200 as kd
     torch.cuda.set_device(local)
-    if args.c5_sample:
-        print(json.dumps({"c5_sample": c5_sample_section()}), flush=True)
+    if args.large_grid_sample:
+        print(json.dumps({"large_grid_sample": large_grid_sample_section()}), flush=True)
         return 0
     if args.only_batched:
         print(json.dumps({"batched": batched_section(args.steps, args.warmup, small=args.size == "small")}),

@@ -32,8 +32,8 @@
 // wait other than the barriers and every loop has a fixed bound.
 //
 // Cost: a step gathers one anti-diagonal, one cache line per row, so the
-// passes run at about one L1 wavefront per row and step (c2: 400 sources of
-// 601 x 1601 in 83 ms for the time, 182 ms with tdl1/tds1).
+// passes run at about one L1 wavefront per row and step (400 sources of the
+// 601 x 1601 salt model in 83 ms for the time, 182 ms with tdl1/tds1).
 #include <float.h>
 #include <math.h>
 

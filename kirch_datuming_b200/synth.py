@@ -171,8 +171,8 @@ def reflectivities(n: int, seed: int) -> list:
     return [float(s * m) for s, m in zip(sign, mag)]
 
 
-def config1_workload(seed: int = 4, device: str = "cuda"):
-    """The CPU-runnable benchmark configuration: v(z) = 1.5 + 0.6 z km/s on a
+def vz_small_workload(seed: int = 4, device: str = "cuda"):
+    """The small survey the reference can migrate on a CPU: v(z) = 1.5 + 0.6 z km/s on a
     201 x 401 grid of 10 m; flat reflectors at 0.6 / 1.2 / 1.7 km with
     reflectivity +-U(0.05, 0.2); 64 shots evenly spaced over 0..4 km, 201
     receivers every 10 m from 1.0 to 3.0 km (cmp=0); nt=1001, dt=2 ms; 20 Hz

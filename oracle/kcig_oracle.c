@@ -9,7 +9,7 @@
  * Two builds come from this one source (see oracle/Makefile):
  *
  *   KCIG_ORACLE_FP64=1  liboracle64.so  every operation in IEEE double: the
- *                       FP64 judge every image is measured against.
+ *                       FP64 oracle every image is measured against.
  *   KCIG_ORACLE_FP64=0  liboracle32.so  the reference's own mixed rounding:
  *                       FP32 storage and arithmetic, with the few expressions
  *                       the reference evaluates in double (Hermite weights,

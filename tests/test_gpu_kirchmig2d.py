@@ -40,11 +40,11 @@ def test_gpu_kirchmig2d(name):
     stats = plan.stats()
     plan.close()
     assert stats["sum_launches"] >= 1
-    judge = oracle.migrate_kirchmig2d(op, data, T, D, T, D, fp64=True)
-    assert oracle.rel_l2(img, judge) <= 1e-5
+    o64 = oracle.migrate_kirchmig2d(op, data, T, D, T, D, fp64=True)
+    assert oracle.rel_l2(img, o64) <= 1e-5
     ref = GD.k2d_image(name)
     u = _cases.ub_columns(GD, name)
-    ref_err = oracle.rel_l2(ref[:, u:], judge[:, u:])
+    ref_err = oracle.rel_l2(ref[:, u:], o64[:, u:])
     assert oracle.rel_l2(img[:, u:], ref[:, u:]) <= 1.5 * ref_err + 1e-6
 
 

@@ -1,7 +1,7 @@
 """Parity of the CUDA path with the oracle and the reference, through the C ABI.
 
 Tolerances (relative L2, ||a-b||/||b|| in double as src/rsf_l2cmp.cpp:9-10):
-  * against the FP64 oracle: 1e-5 (the north-star bound for the table path);
+  * against the FP64 oracle: 1e-5 (the bound the table path is held to);
   * against the reference binary's FP32 image: 1.5x the distance between the
     reference and the FP64 oracle, plus 1e-6 (the reference's own rounding is
     the larger error; the GPU path must not add to it).

@@ -170,13 +170,13 @@ def test_surrogate_leg_fields_match_eval(golden):
 
 
 def test_surrogate_training_gain_and_migration():
-    # train on the config-1 tables (GPU eikonal, 401 positions), then migrate
-    # the config-1 gathers with the surrogate's leg fields.  What the network
+    # train on the v(z) 201x401 tables (GPU eikonal, 401 positions), then
+    # migrate its gathers with the surrogate's leg fields.  What the network
     # gains over the method without it (the straight-ray background T0 alone):
     # traveltime error on the tables and image error against the table path.
     import torch
     from kirch_datuming_b200 import synth
-    vel, T1, D1, data1, g = synth.config1_workload(seed=4)
+    vel, T1, D1, data1, g = synth.vz_small_workload(seed=4)
     net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
     losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, 6000, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
     assert np.all(np.isfinite(losses)) and losses[-50:].mean() < 1e-3 * losses[:50].mean()

@@ -3,7 +3,7 @@ against the reference kirchmig2d's own images (tests/golden/golden_k2d.npz,
 made by tests/golden/make_golden.py --kirchmig2d), and its parameter block.
 
 The FP32 mirror build follows the reference's arithmetic and must agree to
-rounding; the FP64 judge differs where the reference's FP32 pick position
+rounding; the FP64 oracle differs where the reference's FP32 pick position
 lands on a gate (a pick position of exactly the last sample in FP32 that is
 just below it in FP64 drops a pick in the reference only), which bounds it at
 1e-4 here."""
@@ -31,9 +31,9 @@ def test_oracle_matches_reference_kirchmig2d(name):
     u = _cases.ub_columns(GD, name)
     assert ref.shape[0] == axis[0]
     mirror = oracle.migrate_kirchmig2d(op, data, T, D, T, D, fp64=False)
-    judge = oracle.migrate_kirchmig2d(op, data, T, D, T, D, fp64=True)
+    o64 = oracle.migrate_kirchmig2d(op, data, T, D, T, D, fp64=True)
     assert oracle.rel_l2(mirror[:, u:], ref[:, u:]) < 1e-6
-    assert oracle.rel_l2(judge[:, u:], ref[:, u:]) < 1e-4
+    assert oracle.rel_l2(o64[:, u:], ref[:, u:]) < 1e-4
 
 
 def test_kirchmig2d_params():

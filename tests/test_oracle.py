@@ -1,6 +1,6 @@
 """The oracle is pinned to the reference: its FP32 build must reproduce the
 reference binary's images bit for bit on every golden case; its FP64 build is
-the precision judge of the GPU path."""
+the precision reference of the GPU path."""
 import numpy as np
 import pytest
 
