@@ -390,6 +390,92 @@ SG_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m, 64 shots x 201 receivers (cmp=0, 10 m
                "3 flat reflectors, 20 Hz; network trained on the 401-position GPU eikonal tables")
 
 
+STITCH_WINDOWS = [(0, 130), (110, 250), (230, 370), (350, 490), (470, 600)]
+STITCH_WORKLOAD = ("ADCIG stitching (layercom_cig): five depth windows, rows 0-130 / 110-250 / 230-370 / "
+                   "350-490 / 470-600, of a 601 x 1601 image with 61 angle bins (235 MB out), stitch_blend=15, "
+                   "lateral taper scalex_aper=50 scalex_scale=1.5")
+
+
+def stitch_section(steps: int, warmup: int, threads: int):
+    """ADCIG stitching: the device calls (kcig_stitch_window) timed with CUDA
+    events against the HBM peak, and the drop-in CLI and the reference tool
+    (oracle/_ref/layercom_cig, all host threads) timed on the same RSF files
+    (wall time: both read and write the files)."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import rsf
+    n1, n2, n3 = NZ, NX, 61
+    g = torch.Generator(device="cuda").manual_seed(5)
+    vols = [torch.randn((n3, n2, e - s + 1), device="cuda", generator=g) for s, e in STITCH_WINDOWS]
+    scales = [1.0, 1.1, 0.9, 1.2, 0.8]
+    out = torch.empty((n3, n2, n1), dtype=torch.float32, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def once():
+        out.zero_()
+        prev = -1
+        for k, ((s, e), v) in enumerate(zip(STITCH_WINDOWS, vols)):
+            kd.stitch_window(out, v, s, e, prev, 15, scales[k], k > 0, 50, 1.5)
+            prev = e
+
+    for _ in range(max(1, warmup)):
+        once()
+    ms = []
+    for _ in range(max(1, steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        once()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = statistics.median(ms)
+    # algorithmic bytes: every window sample read once and written once, the
+    # blended rows' output read once more, the zeroed output written once
+    win = sum((e - s + 1) for s, e in STITCH_WINDOWS) * n2 * n3
+    blend = sum(min(15, STITCH_WINDOWS[k - 1][1] - STITCH_WINDOWS[k][0] + 1) for k in range(1, 5)) * n2 * n3
+    algo = 4 * (2 * win + blend + n1 * n2 * n3)
+    peak, peak_src = measured_peaks()
+    res = {"workload": STITCH_WORKLOAD, "device_ms": t, "samples_out": n1 * n2 * n3,
+           "roofline": {"bound": "hbm", "achieved": algo / (t / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": algo / (t / 1e3) / 1e9 / peak, "peak_source": peak_src,
+                        "note": "five kcig_stitch_window calls with the zeroing of the output; each call also "
+                                "copies its blend weights in and its non-finite count out and synchronises"}}
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "layercom_cig")
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/model.rsf", np.zeros((n2, n1), np.float32), [n1, n2], [0.0, 0.0], [DZ, DZ])
+        with open(f"{wd}/layers.txt", "w") as f:
+            f.write("".join("%d %d\n" % w for w in STITCH_WINDOWS))
+        for k, ((s, e), v) in enumerate(zip(STITCH_WINDOWS, vols)):
+            rsf.write(f"{wd}/adcig_{k + 1}.rsf", v.cpu().numpy(), [e - s + 1, n2, n3], [s * DZ, 0.0, 0.0],
+                      [DZ, DZ, 1.0])
+        args = ["full_model=model.rsf", "layer_image_base=adcig.rsf", "layer_txt=layers.txt", "stitch_blend=15",
+                "scale=1,1.1,0.9,1.2,0.8", "scalex_aper=50", "scalex_scale=1.5"]
+        walls = {}
+        for name, exe in (("kcig", kd.layercom_cig_cli_path), ("reference", ref_bin)):
+            if not os.path.exists(exe):
+                continue
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            wall = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                r = subprocess.run([exe] + args + ["output_file=out_%s.rsf" % name], cwd=wd, env=env,
+                                   capture_output=True, text=True)
+                wall.append((time.perf_counter() - t0) * 1e3)
+                if r.returncode != 0:
+                    raise RuntimeError(r.stderr)
+            walls[name] = min(wall)
+        same = None
+        if len(walls) == 2:
+            a = np.fromfile(f"{wd}/out_kcig.rsf@", dtype="<f4")
+            b = np.fromfile(f"{wd}/out_reference.rsf@", dtype="<f4")
+            same = bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
+    res["cli_wall_ms"] = walls
+    res["cli_outputs_identical"] = same
+    res["reference_threads"] = threads
+    return res
+
+
 def surrogate_section(train_steps: int, steps: int, warmup: int):
     """Table path vs learned-surrogate path on the same v(z) 201x401 gathers:
     throughput of each (device time per migration), the surrogate's training
@@ -573,6 +659,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
+    ap.add_argument("--no-stitch", action="store_true", help="skip the ADCIG stitching section")
+    ap.add_argument("--only-stitch", action="store_true", help="only the ADCIG stitching section (one JSON object)")
     ap.add_argument("--no-tables", action="store_true", help="skip the table-generator section")
     ap.add_argument("--no-stream", action="store_true", help="skip the host-resident-tables measurement")
     ap.add_argument("--large-grid-sample", action="store_true",
@@ -627,6 +715,10 @@ def main():
     torch.cuda.set_device(local)
     if args.large_grid_sample:
         print(json.dumps({"large_grid_sample": large_grid_sample_section()}), flush=True)
+        return 0
+    if args.only_stitch:
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        print(json.dumps({"stitch": stitch_section(args.steps, args.warmup, threads)}), flush=True)
         return 0
     if args.only_batched:
         print(json.dumps({"batched": batched_section(args.steps, args.warmup, small=args.size == "small")}),
@@ -751,6 +843,12 @@ def main():
         del T, D, data, image
         torch.cuda.empty_cache()
         line["batched"] = batched_section(args.steps, args.warmup, small=args.size == "small")
+    if dist is None and not args.no_stitch and args.size == "full":
+        torch.cuda.empty_cache()
+        try:  # an extra object: its failure is recorded, the line still prints
+            line["stitch"] = stitch_section(args.steps, args.warmup, threads)
+        except Exception as e:  # noqa: BLE001
+            line["stitch"] = {"workload": STITCH_WORKLOAD, "error": str(e)[-400:]}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

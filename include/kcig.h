@@ -354,6 +354,33 @@ float kcig_plan_last_prelude_ms(const kcig_plan *plan);
  * tables).  The surrogates must outlive the plan's migrations. */
 int kcig_plan_set_surrogate(kcig_plan *plan, kcig_surrogate *src, kcig_surrogate *rcv);
 
+/* ---- ADCIG stitching of depth windows (src/layercom_cig.cpp) ------------ */
+
+/* One depth window of layercom_cig's stitch loop (src/layercom_cig.cpp:
+ * 473-533), on the device.  out: full-depth volume [n3][n2][n1] (device);
+ * layer: the window's volume [n3][n2][end-start+1] (device), covering depth
+ * rows start..end.  Every sample is scaled by layer_scale, times the
+ * lateral taper of scalex_aper / scalex_scale when use_lateral (:455-466,
+ * applied to every window but the first); non-finite products become 0 and
+ * are counted in *nonfinite (host).  previous_end: last row of the window
+ * above (-1 for the first window).  Rows shared with it keep the upper value
+ * for the first overlap - blend rows and are blended over the other blend
+ * rows with complementary raised-cosine weights, where blend =
+ * min(stitch_blend, overlap) (stitch_blend = -1: the whole overlap).  The
+ * other rows are written.  Synchronous on `stream`; the result equals the
+ * reference's float arithmetic bit for bit. */
+int kcig_stitch_window(float *out, int n1, int n2, int n3, const float *layer, int start, int end,
+                       int previous_end, int stitch_blend, float layer_scale, int use_lateral, int scalex_aper,
+                       double scalex_scale, long long *nonfinite, void *stream);
+
+/* The drop-in layercom_cig (src/layercom_cig.cpp:412-556): the same keys
+ * (full_model= layer_image_base= layer_txt= output_file= nlayers= nangle=
+ * scale= stitch_blend= scalex_aper= scalex_scale=), layer file rules,
+ * checks, INFO lines, "ERROR: ..." texts and output header; the windows are
+ * stitched on the device by kcig_stitch_window.  Returns 0 or KCIG_ERR_ARG
+ * (the message printed to stderr). */
+int kcig_run_layercom_cig_cli(int argc, char **argv);
+
 #ifdef __cplusplus
 }
 #endif

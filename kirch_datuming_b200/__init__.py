@@ -16,13 +16,15 @@ import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
            "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "eikods", "library_path",
-           "cli_path", "eikods_cli_path", "kirchmig2d_cli_path", "params_kirchmig2d"]
+           "cli_path", "eikods_cli_path", "kirchmig2d_cli_path", "layercom_cig_cli_path", "params_kirchmig2d",
+           "stitch_window"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 library_path = os.path.join(_HERE, "libkcig.so")
 cli_path = os.path.join(_HERE, "bin", "kirchmig2d_cig")
 kirchmig2d_cli_path = os.path.join(_HERE, "bin", "kirchmig2d")
 eikods_cli_path = os.path.join(_HERE, "bin", "eikods2d")
+layercom_cig_cli_path = os.path.join(_HERE, "bin", "layercom_cig")
 
 MEM_HOST = 0
 MEM_DEVICE = 1
@@ -138,6 +140,10 @@ def lib():
         L.kcig_graph_destroy.restype = None
         L.kcig_shots_pairs.argtypes = [vp]
         L.kcig_shots_pairs.restype = ctypes.c_longlong
+        L.kcig_stitch_window.argtypes = ([fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.POINTER(ctypes.c_longlong), vp])
+        L.kcig_run_layercom_cig_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
         L.kcig_plan_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.kcig_plan_last_prelude_ms.argtypes = [vp]
         L.kcig_plan_last_prelude_ms.restype = ctypes.c_float
@@ -344,6 +350,28 @@ def doubint_device(traces, isdiff: int = 0, dt: float = 1.0, stream=None):
                                      ctypes.c_void_p(st)))
     torch.cuda.current_stream().synchronize()
     return out
+
+
+def stitch_window(out, layer, start: int, end: int, previous_end: int = -1, stitch_blend: int = 15,
+                  layer_scale: float = 1.0, use_lateral: bool = False, scalex_aper: int = 0,
+                  scalex_scale: float = 1.0, stream=None) -> int:
+    """One depth window of layercom_cig's stitching on the device
+    (kcig_stitch_window): out [n3][n2][n1] and layer [n3][n2][end-start+1],
+    contiguous CUDA float32 tensors; out is updated in place.  Returns the
+    number of non-finite scaled samples (written as 0)."""
+    import torch
+    for t in (out, layer):
+        if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous() and t.dim() == 3):
+            raise ValueError("expects contiguous 3-D CUDA float32 tensors")
+    n3, n2, n1 = out.shape
+    if tuple(layer.shape) != (n3, n2, end - start + 1):
+        raise ValueError("layer shape %s does not match rows %d..%d" % (tuple(layer.shape), start, end))
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    bad = ctypes.c_longlong()
+    _check(lib().kcig_stitch_window(out.data_ptr(), n1, n2, n3, layer.data_ptr(), int(start), int(end),
+                                    int(previous_end), int(stitch_blend), float(layer_scale), int(bool(use_lateral)),
+                                    int(scalex_aper), float(scalex_scale), ctypes.byref(bad), ctypes.c_void_p(st)))
+    return bad.value
 
 
 def leg_fields_device(plan: Plan, is_source: int, pos: float):

@@ -7,6 +7,7 @@ produces, in-tree,
     kirch_datuming_b200/bin/kirchmig2d_cig  the drop-in migration / modelling tool
     kirch_datuming_b200/bin/eikods2d        the drop-in table generator
     kirch_datuming_b200/bin/kirchmig2d      the drop-in plain Kirchhoff migration
+    kirch_datuming_b200/bin/layercom_cig    the drop-in ADCIG stitching of depth windows
 compiled for sm_100a only (nvcc cross-compiles; no GPU needed to build).
 """
 from __future__ import annotations
@@ -23,9 +24,10 @@ LIB = os.path.join(PKG, "libkcig.so")
 CLI = os.path.join(PKG, "bin", "kirchmig2d_cig")
 EIK_CLI = os.path.join(PKG, "bin", "eikods2d")
 K2D_CLI = os.path.join(PKG, "bin", "kirchmig2d")
+STITCH_CLI = os.path.join(PKG, "bin", "layercom_cig")
 
 SOURCES = ["kcig_kernels.cu", "kcig_plan.cu", "kcig_eikods.cu", "kcig_mlp.cu", "kcig_params.cpp", "kcig_rsf.cpp", "kcig_cli.cpp",
-           "kcig_eikods_cli.cpp"]
+           "kcig_eikods_cli.cpp", "kcig_stitch.cu", "kcig_stitch_cli.cpp"]
 HEADERS = ["kcig_common.h", "kcig_tc.h", "kcig_aperture.h", "kcig_par.h", "kcig_rsf.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -61,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> None:
         if verbose:
             sys.stderr.write(r.stderr)
     for exe, src in ((CLI, "kirchmig2d_cig_main.cpp"), (EIK_CLI, "eikods2d_main.cpp"),
-                     (K2D_CLI, "kirchmig2d_main.cpp")):
+                     (K2D_CLI, "kirchmig2d_main.cpp"), (STITCH_CLI, "layercom_cig_main.cpp")):
         main = os.path.join(CSRC, src)
         if force or _stale(exe, [LIB, main]):
             os.makedirs(os.path.dirname(exe), exist_ok=True)

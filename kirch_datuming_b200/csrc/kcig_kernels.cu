@@ -26,7 +26,6 @@
 
 namespace kcig {
 
-static constexpr double kPi = 3.14159265358979323846;
 
 // =============================================================== K1 prelude ==
 // One warp per trace.  The trace is staged in shared memory as double, muted

@@ -11,6 +11,7 @@ container); the tests only read the committed outputs.
     python tests/golden/make_golden.py --forward  # only the adj=0 fixtures
     python tests/golden/make_golden.py --eikods   # only the table-generator fixtures
     python tests/golden/make_golden.py --kirchmig2d  # only the plain-tool fixtures
+    python tests/golden/make_golden.py --stitch   # only the ADCIG stitching fixtures
 """
 from __future__ import annotations
 
@@ -266,8 +267,83 @@ def kirchmig2d():
     print("wrote", os.path.join(HERE, "golden_k2d.npz"))
 
 
+# ADCIG stitching (layercom_cig): three depth windows of a 60 x 24 model with
+# 7 angles; the layer file mixes every separator the tool accepts
+STITCH_MODEL = dict(n=[60, 24], o=[0.0, 0.5], d=[0.01, 0.02])
+STITCH_ANGLES = dict(n=7, o=0.0, d=10.0)
+STITCH_LAYERS = "# depth windows of the test model\nSTART,25\n18\uff0c45   # middle\n\n40;END\n"
+STITCH_WINDOWS = [(0, 25), (18, 45), (40, 59)]
+STITCH = {
+    "default": [],
+    "blend3_scales": ["stitch_blend=3", "scale=1.5,0.5;2"],
+    "keep_upper": ["stitch_blend=0"],
+    "full_overlap": ["stitch_blend=-1", "nlayers=3", "nangle=7"],
+    "lateral": ["scalex_aper=5", "scalex_scale=2.5", "scale=0.8"],
+    "blend1_lateral1": ["stitch_blend=1", "scalex_aper=1", "scalex_scale=0.5"],
+}
+STITCH_ERRORS = {
+    "nonfinite": ["layer_image_base=bad.rsf"],
+    "nlayers": ["nlayers=4"],
+    "scale_count": ["scale=1,2"],
+    "blend": ["stitch_blend=-2"],
+    "bad_argument": ["foo"],
+    "missing_key": ["layer_txt="],
+}
+
+
+def stitch():
+    """layercom_cig fixtures (golden_stitch.npz, cases.json "stitch")."""
+    with open(os.path.join(HERE, "cases.json")) as f:
+        meta = json.load(f)
+    rng = np.random.default_rng(2024)
+    m, a = STITCH_MODEL, STITCH_ANGLES
+    out = {}
+    vols = []
+    for k, (s0, s1) in enumerate(STITCH_WINDOWS):
+        v = rng.standard_normal((a["n"], m["n"][1], s1 - s0 + 1)).astype(np.float32)
+        vols.append(v)
+        out["window_%d" % (k + 1)] = v
+    labels = {"label1": "Depth", "label2": "Lateral", "label3": "Scattering angle", "unit1": "km",
+              "unit3": "degree"}
+    info = dict(model=m, angles=a, layers=STITCH_LAYERS, windows=STITCH_WINDOWS, labels=labels, cases={},
+                errors={})
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/model.rsf", np.zeros(m["n"][::-1], np.float32), m["n"], m["o"], m["d"])
+        with open(f"{wd}/layers.txt", "w", encoding="utf-8") as f:
+            f.write(STITCH_LAYERS)
+        for base in ("adcig", "bad"):
+            for k, ((s0, s1), v) in enumerate(zip(STITCH_WINDOWS, vols)):
+                v = v.copy()
+                if base == "bad" and k == 1:
+                    v[3, 5, 2] = np.inf
+                rsf.write(f"{wd}/{base}_{k + 1}.rsf", v, [s1 - s0 + 1, m["n"][1], a["n"]],
+                          [m["o"][0] + s0 * m["d"][0], m["o"][1], a["o"]], [m["d"][0], m["d"][1], a["d"]],
+                          extra=labels)
+        common = ["full_model=model.rsf", "layer_image_base=adcig.rsf", "layer_txt=layers.txt",
+                  "output_file=out.rsf"]
+        for name, extra in STITCH.items():
+            r = subprocess.run([f"{REF}/layercom_cig"] + common + extra, cwd=wd, capture_output=True, text=True)
+            assert r.returncode == 0, r.stderr
+            h, img = rsf.read(f"{wd}/out.rsf")
+            out["out_" + name] = img.reshape(h.n[2], h.n[1], h.n[0])
+            with open(f"{wd}/out.rsf") as f:
+                header = f.read()
+            info["cases"][name] = dict(args=extra, header=header, stdout=r.stdout)
+        for name, extra in STITCH_ERRORS.items():
+            r = subprocess.run([f"{REF}/layercom_cig"] + common + extra, cwd=wd, capture_output=True, text=True)
+            assert r.returncode != 0
+            info["errors"][name] = dict(args=extra, stderr=r.stderr, returncode=r.returncode)
+    meta["stitch"] = info
+    np.savez_compressed(os.path.join(HERE, "golden_stitch.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_stitch.npz"))
+
+
 if __name__ == "__main__":
-    if "--forward" in sys.argv:
+    if "--stitch" in sys.argv:
+        stitch()
+    elif "--forward" in sys.argv:
         forward()
     elif "--kirchmig2d" in sys.argv:
         kirchmig2d()
