@@ -4,15 +4,18 @@
 // window above keep the upper values for the first rows of the overlap and are
 // blended with complementary raised-cosine weights over the rest.
 //
-// One pass over the window's samples, one thread per sample in a grid-stride
-// loop along the contiguous depth axis: 4 B read from the window, 4 B read
-// and 4 B written in the output (HBM-bound).  The blend weights and the
+// One pass over the window's samples: 4 B read from the window and 4 B
+// written in the output per sample, 4 B more read in the blended rows
+// (HBM-bound).  The blend weights and the
 // lateral taper are formed on the host in double exactly as the reference
 // forms them (:455-466, :522-528) and rounded once to float; the kernel keeps
 // the reference's float operations separate (no fused multiply-add), so the
 // output is the reference's, bit for bit.
 #include <math.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "kcig_common.h"
@@ -29,36 +32,45 @@ struct StitchArgs {
     float layer_scale;
 };
 
+// One warp per depth column (i3, i2) of the window, its lanes along the
+// contiguous depth rows: the column's scale is formed once, every access is
+// coalesced, and no index is divided per sample.
 __global__ void __launch_bounds__(256) k_stitch_layer(const StitchArgs a)
 {
-    const size_t total = (size_t)a.n1w * a.n2 * a.n3;
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int ncol = a.n2 * a.n3;  // < 2^31 (checked on the host)
     unsigned long long bad = 0;
-    for (size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (size_t)gridDim.x * blockDim.x) {
-        const int i1 = (int)(idx % a.n1w);
-        const size_t col = idx / a.n1w;  // i3 * n2 + i2
-        const int i2 = (int)(col % a.n2);
+    for (int col = blockIdx.x * warps + (threadIdx.x >> 5); col < ncol; col += gridDim.x * warps) {
+        const int i2 = col % a.n2;
         const float sx = a.lateral ? a.lateral[i2] : 1.0f;
         const float scale = __fmul_rn(a.layer_scale, sx);
-        float v = __fmul_rn(a.layer[idx], scale);
-        if (!isfinite(v)) {
-            ++bad;
-            v = 0.0f;
-        }
-        const int g1 = a.start + i1;
-        float *o = a.out + col * a.n1 + g1;
-        if (a.overlap > 0 && g1 <= a.previous_end) {
-            if (i1 < a.keep_upper || a.blend_count == 0) continue;
-            const float w = a.blend_w[i1 - a.keep_upper];
-            *o = __fadd_rn(__fmul_rn(*o, __fsub_rn(1.0f, w)), __fmul_rn(v, w));
-        } else {
-            *o = v;
+        const float *src = a.layer + (size_t)col * a.n1w;
+        float *dst = a.out + (size_t)col * a.n1 + a.start;
+        for (int i1 = lane; i1 < a.n1w; i1 += 32) {
+            float v = __fmul_rn(src[i1], scale);
+            if (!isfinite(v)) {
+                ++bad;
+                v = 0.0f;
+            }
+            if (a.overlap > 0 && a.start + i1 <= a.previous_end) {
+                if (i1 < a.keep_upper || a.blend_count == 0) continue;
+                const float w = a.blend_w[i1 - a.keep_upper];
+                dst[i1] = __fadd_rn(__fmul_rn(dst[i1], __fsub_rn(1.0f, w)), __fmul_rn(v, w));
+            } else {
+                dst[i1] = v;
+            }
         }
     }
     // one atomic per warp at most
     for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
-    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.nonfinite, bad);
+    if (lane == 0 && bad) atomicAdd(a.nonfinite, bad);
 }
+
+// Device scratch of the calls (counter + weights), one per device, grown on
+// demand and kept for the life of the process: a call allocates nothing once
+// warm.  Calls hold the lock until they have synchronised.
+static std::mutex g_scratch_mu;
+static std::map<int, std::pair<void *, size_t>> g_scratch;
 
 }  // namespace kcig
 
@@ -70,6 +82,7 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
 {
     if (!out || !layer || !nonfinite || n1 <= 0 || n2 <= 0 || n3 <= 0)
         return set_error(KCIG_ERR_ARG, "kcig_stitch_window: bad arguments");
+    if ((long long)n2 * n3 > 0x7fffffffLL) return set_error(KCIG_ERR_ARG, "kcig_stitch_window: n2*n3 too large");
     if (start < 0 || end < start || end >= n1)
         return set_error(KCIG_ERR_ARG, "Invalid layer range [%d,%d]", start, end);
     if (stitch_blend < -1) return set_error(KCIG_ERR_ARG, "stitch_blend must be -1 or nonnegative");
@@ -106,9 +119,18 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
     }
     cudaStream_t st = (cudaStream_t)stream;
     // device scratch: the counter first (8-byte aligned), then the weights
-    void *scratch = nullptr;
     const size_t bytes = sizeof(unsigned long long) + host.size() * sizeof(float);
-    KCIG_CUDA(cudaMalloc(&scratch, bytes));
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    std::pair<void *, size_t> &buf = g_scratch[dev];
+    if (buf.second < bytes) {
+        if (buf.first) cudaFree(buf.first);
+        buf = {nullptr, 0};
+        KCIG_CUDA(cudaMalloc(&buf.first, std::max<size_t>(bytes, 64 << 10)));
+        buf.second = std::max<size_t>(bytes, 64 << 10);
+    }
+    void *scratch = buf.first;
     unsigned long long *d_bad = (unsigned long long *)scratch;
     float *d_w = (float *)(d_bad + 1);
     int rc = KCIG_OK;
@@ -132,11 +154,10 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
         a.blend_count = blend_count;
         a.overlap = overlap;
         a.layer_scale = layer_scale;
-        const size_t total = (size_t)n1w * n2 * n3;
-        int sms = 148, dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t want = (total + 255) / 256;
-        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 8));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t want = ((size_t)n2 * n3 + 7) / 8;  // 8 columns (warps) per block
+        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 16));
         k_stitch_layer<<<grid, 256, 0, st>>>(a);
         e = cudaGetLastError();
     }
@@ -144,7 +165,6 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
     if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_error(e, "kcig_stitch_window");
-    cudaFree(scratch);
     *nonfinite = (long long)bad;
     return rc;
 }
