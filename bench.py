@@ -460,7 +460,7 @@ def stitch_section(steps: int, warmup: int, threads: int):
             for _ in range(2):
                 t0 = time.perf_counter()
                 r = subprocess.run([exe] + args + ["output_file=out_%s.rsf" % name], cwd=wd, env=env,
-                                   capture_output=True, text=True)
+                                   capture_output=True, text=True, timeout=120)
                 wall.append((time.perf_counter() - t0) * 1e3)
                 if r.returncode != 0:
                     raise RuntimeError(r.stderr)
