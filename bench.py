@@ -143,6 +143,24 @@ def profiled_traffic():
         return None
 
 
+def issue_ceiling(pairs_per_s: float, sm_mhz):
+    """The summation's instruction-issue ceiling next to its HBM roofline:
+    148 SMs x 4 schedulers x one warp instruction per cycle, divided by the
+    thread instructions per pair of the committed ncu summary; with that
+    summary's L2 hit rate.  None without the summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_sum_traffic.json")) as f:
+            p = json.load(f)
+        ipp = float(p["thread_instructions_per_pair"])
+        mhz = float(sm_mhz) if sm_mhz else 1965.0
+        ceiling = 148 * 4 * 32 * mhz * 1e6 / ipp / 1e9
+        return {"thread_instructions_per_pair": ipp, "sm_mhz": mhz, "ceiling_gpairs": ceiling,
+                "frac": pairs_per_s / 1e9 / ceiling, "issue_active_pct_ncu": p.get("issue_active_pct"),
+                "l2_sector_hit_rate_pct_ncu": p.get("l2_sector_hit_rate_pct")}
+    except Exception:
+        return None
+
+
 # ----------------------------------------------------------- reference (CPU) --
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "kirchmig2d_cig")
 REF_EIK = os.path.join(ROOT, "oracle", "_ref", "eikods2d")
@@ -818,6 +836,7 @@ def main():
                      "peak_source": peak_src, "kernel": "k_sum", "kernel_ms": ksum_ms,
                      "algorithmic_bytes_per_pair": B_PAIR,
                      "traffic": (tpp * pairs) if tpp is not None else None,
+                     "issue": issue_ceiling(pairs / (ksum_ms / 1e3), (clk or {}).get("sm_mhz")),
                      "note": "16 B/pair counts the receiver leg's fields once per pair; k_sum loads each "
                              "receiver leg once per block of 4 shots, so its DRAM traffic (ncu, 'traffic') is "
                              "below the algorithmic bytes and frac can pass 1: the kernel is issue-bound"},
