@@ -1,6 +1,7 @@
 #include "kcig_rsf.h"
 
 #include <ctype.h>
+#include <errno.h>
 #include <limits.h>
 #include <math.h>
 #include <pwd.h>
@@ -12,6 +13,7 @@
 
 #include <fstream>
 #include <sstream>
+#include <vector>
 
 #include "kcig_common.h"
 
@@ -54,13 +56,55 @@ static bool parse_double_str(const std::string &s, double *v)
     return true;
 }
 
+// The SEP layer names a file by its absolute path (se_uri.cpp:67-150): a
+// relative name is resolved against the working directory, "." components
+// are dropped and ".." removes the component before it.
+static std::string current_dir()
+{
+    char cwd[PATH_MAX] = ".";
+    if (!getcwd(cwd, sizeof cwd)) strcpy(cwd, ".");
+    return cwd;
+}
+
+static std::string sep_absolute(const std::string &path)
+{
+    std::vector<std::string> parts;
+    auto add = [&parts](const std::string &p) {
+        std::istringstream items(p);
+        for (std::string item; std::getline(items, item, '/');) {
+            if (item.empty() || item == ".") continue;
+            if (item == "..") {
+                if (!parts.empty()) parts.pop_back();
+            } else {
+                parts.push_back(item);
+            }
+        }
+    };
+    if (path.empty() || path[0] != '/') add(current_dir());
+    add(path);
+    std::string out = "/";
+    for (size_t i = 0; i < parts.size(); i++) out += (i ? "/" : "") + parts[i];
+    return out;
+}
+
+// se_fs_sep.cpp:740-745: the message of a header file that cannot be opened
+static int sep_open_error(const std::string &path, int err)
+{
+    return set_error(KCIG_ERR_IO, "Cannot open SEP file '%s': current dir is %s, error code is %d - %s",
+                     sep_absolute(path).c_str(), current_dir().c_str(), err, strerror(err));
+}
+
 int rsf_open(const std::string &path, RsfFile *f)
 {
     *f = RsfFile();
     f->path = path;
+    {
+        FILE *probe = fopen(path.c_str(), "rb");
+        if (!probe) return sep_open_error(path, errno);
+        fclose(probe);
+    }
     std::ifstream in(path, std::ios::binary);
-    if (!in)
-        return set_error(KCIG_ERR_IO, "Cannot open SEP file '%s'", path.c_str());
+    if (!in) return sep_open_error(path, errno ? errno : EIO);
     std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
     const size_t eot = text.find('\x04');
     if (eot != std::string::npos) text.resize(eot);
@@ -180,7 +224,7 @@ int rsf_write(const std::string &path, int ndim, const int *n, const double *o, 
     }
     fclose(fb);
     FILE *fh = fopen(path.c_str(), "w");
-    if (!fh) return set_error(KCIG_ERR_IO, "Cannot open SEP file '%s'", path.c_str());
+    if (!fh) return sep_open_error(path, errno);
     char cwd[PATH_MAX] = ".";
     if (!getcwd(cwd, sizeof cwd)) strcpy(cwd, ".");
     char host[256] = "unknown_host";

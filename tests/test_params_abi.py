@@ -105,7 +105,8 @@ def test_cli_errors_without_gpu(tmp_path):
     assert r.returncode == 1 and "ERROR:Need rderiv=" in r.stderr
     r = _cli(["seismic_data=nope.rsf", "migration=m.rsf", "stable=t.rsf", "sderiv=t.rsf", "rtable=t.rsf",
               "rderiv=t.rsf"], tmp_path)
-    assert r.returncode == 1 and "Cannot open SEP file 'nope.rsf'" in r.stderr
+    assert r.returncode == 1 and "Cannot open SEP file '%s': current dir is %s, error code is 2 - " % (
+        os.path.join(os.path.realpath(tmp_path), "nope.rsf"), os.path.realpath(tmp_path)) in r.stderr
     rsf.write(str(tmp_path / "d2.rsf"), np.zeros((4, 3), np.float32), [4, 3])
     r = _cli(["seismic_data=d2.rsf", "migration=m.rsf", "stable=t.rsf", "sderiv=t.rsf", "rtable=t.rsf",
               "rderiv=t.rsf"], tmp_path)
