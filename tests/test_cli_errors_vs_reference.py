@@ -52,3 +52,22 @@ def test_same_error_as_reference(tmp_path, name):
         out.append((r.returncode, _error_text(r.stderr)))
     assert out[0][0] != 0 and out[0][1]
     assert out[1] == out[0]
+
+
+K2D_REF = os.path.join(os.path.dirname(REF), "kirchmig2d")
+K2D_CASES = {k: CASES[k] for k in ("no_data", "no_rderiv", "missing_file", "data_2d")}
+K2D_CASES["interp_type"] = BASE + ["type=cubic"]
+
+
+@pytest.mark.skipif(not os.path.exists(K2D_REF), reason="reference kirchmig2d not built")
+@pytest.mark.parametrize("name", sorted(K2D_CASES))
+def test_kirchmig2d_same_error_as_reference(tmp_path, name):
+    rsf.write(str(tmp_path / "d.rsf"), np.zeros((2, 3, 4), np.float32), [4, 3, 2])
+    rsf.write(str(tmp_path / "d2.rsf"), np.zeros((4, 3), np.float32), [4, 3])
+    rsf.write(str(tmp_path / "t.rsf"), np.zeros((2, 5, 5), np.float32), [5, 5, 2])
+    out = []
+    for exe in (K2D_REF, kd.kirchmig2d_cli_path):
+        r = subprocess.run([exe] + K2D_CASES[name], cwd=tmp_path, capture_output=True, text=True)
+        out.append((r.returncode, _error_text(r.stderr)))
+    assert out[0][0] != 0 and out[0][1]
+    assert out[1] == out[0]
