@@ -1,7 +1,8 @@
-"""layercom_cig drop-in against the reference tool (oracle/_ref/layercom_cig,
-built from its source) on malformed inputs: exit code, INFO lines and ERROR
-text must be the same.  Every case fails before any device work, so this runs
-without a GPU."""
+"""layercom_cig against the reference tool (oracle/_ref/layercom_cig, built
+from its source), on the CPU: the drop-in on malformed inputs (exit code, INFO
+lines and ERROR text must be the same; every case fails before any device
+work), and the oracle on random window layouts, blends, tapers and scales (the
+volume must be the same bit for bit)."""
 import os
 import subprocess
 
@@ -78,3 +79,53 @@ def test_same_failure_as_reference(tmp_path, name):
     ref, got = results
     assert ref[0] != 0 and ref[2].startswith("ERROR: ")
     assert got == ref
+
+
+def _random_setup(rng):
+    n1 = int(rng.integers(30, 90))
+    nwin = int(rng.integers(2, 5))
+    # window ends increase; each window starts inside the one above
+    ends = sorted(rng.choice(np.arange(8, n1 - 1), size=nwin - 1, replace=False).tolist()) + [n1 - 1]
+    wins, prev_end = [], None
+    for k, e in enumerate(ends):
+        s = 0 if k == 0 else int(rng.integers(max(1, prev_end - 25), prev_end + 1))
+        wins.append((s, int(e)))
+        prev_end = int(e)
+    args = []
+    blend = int(rng.choice([-1, 0, 1, 2, 5, 15, 40]))
+    if blend != 15:
+        args.append("stitch_blend=%d" % blend)
+    aper = int(rng.integers(0, 7))
+    sxs = float(np.round(rng.uniform(0.2, 3.0), 3))
+    if aper:
+        args += ["scalex_aper=%d" % aper, "scalex_scale=%g" % sxs]
+    scales = None
+    if rng.random() < 0.7:
+        scales = [float(np.float32(np.round(rng.uniform(0.1, 3.0), 4))) for _ in wins]
+        args.append("scale=" + ",".join("%g" % x for x in scales))
+    return n1, wins, blend, aper, sxs if aper else 1.0, scales, args
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_oracle_vs_reference_random_layouts(tmp_path, seed):
+    # random window layouts, blends, tapers and scales through the reference
+    # tool: the oracle must give its volume bit for bit
+    import stitch as so
+    from kirch_datuming_b200 import rsf
+    rng = np.random.default_rng(1000 + seed)
+    n1, wins, blend, aper, sxs, scales, args = _random_setup(rng)
+    n2, n3 = int(rng.integers(3, 20)), int(rng.integers(1, 6))
+    rsf.write(str(tmp_path / "model.rsf"), np.zeros((n2, n1), np.float32), [n1, n2], [0.0, 0.0], [0.01, 0.02])
+    with open(tmp_path / "layers.txt", "w") as f:
+        f.write("".join("%d %d\n" % w for w in wins))
+    vols = []
+    for k, (s, e) in enumerate(wins):
+        v = (rng.standard_normal((n3, n2, e - s + 1)) * 10 ** rng.uniform(-3, 3)).astype(np.float32)
+        vols.append(v)
+        rsf.write(str(tmp_path / ("adcig_%d.rsf" % (k + 1))), v, [e - s + 1, n2, n3], [s * 0.01, 0.0, 0.0],
+                  [0.01, 0.02, 1.0])
+    r = subprocess.run([REF] + COMMON + args, cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    ref = np.fromfile(tmp_path / "out.rsf@", dtype="<f4").reshape(n3, n2, n1)
+    got = so.stitch(n1, wins, vols, scales, blend, aper, sxs)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
