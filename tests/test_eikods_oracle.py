@@ -102,3 +102,50 @@ def test_sweeps_stop_at_a_fixed_point():
     np.testing.assert_array_equal(r["time"], r2["time"])
     with pytest.raises(RuntimeError):
         O.eikods(g["vel"], meta["d"], meta["d"], g["shots"], method=1, max_iter=1)
+
+
+REF_EIK = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "eikods2d")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_EIK), reason="reference eikods2d not built (make -C oracle ref)")
+@pytest.mark.parametrize("seed", range(6))
+def test_random_models_vs_reference(tmp_path, seed):
+    # random layered models with a slow or fast body, sources on and off the
+    # grid nodes and below the surface, orders 1 and 2, through the reference
+    # binary (one thread): the marching restatement reproduces every output
+    # bit for bit, and so do the sweeps at order 1
+    import subprocess
+    from kirch_datuming_b200 import rsf
+    rng = np.random.default_rng(500 + seed)
+    nz, nx, d = int(rng.integers(24, 48)), int(rng.integers(30, 70)), 0.01
+    z = np.arange(nz)[:, None] * np.ones((1, nx))
+    v = np.full((nz, nx), rng.uniform(1.4, 2.0))
+    for _ in range(int(rng.integers(2, 5))):
+        depth = rng.uniform(0.2, 0.9) * nz + rng.uniform(-3, 3) * np.sin(np.arange(nx) / rng.uniform(4, 12))
+        v = np.where(z > depth[None, :], v + rng.uniform(0.2, 0.8), v)
+    cz, cx, r = rng.uniform(0.3, 0.7) * nz, rng.uniform(0.2, 0.8) * nx, rng.uniform(3, 8)
+    body = (z - cz) ** 2 + (np.arange(nx)[None, :] - cx) ** 2 < r * r
+    v = np.where(body, rng.choice([1.2, 4.5]), v).astype(np.float32)
+    ns = int(rng.integers(2, 5))
+    shots = np.zeros((ns, 3), np.float32)
+    shots[:, 0] = rng.choice([0.0, 0.05, 0.123], ns)                     # depth
+    shots[:, 1] = rng.uniform(0.0, (nx - 1) * d, ns).astype(np.float32)  # lateral, mostly off-node
+    velt = np.ascontiguousarray(v.T)                                     # [nx][nz] as the file
+    rsf.write(str(tmp_path / "vel.rsf"), velt, [nz, nx], [0, 0], [d, d])
+    rsf.write(str(tmp_path / "sht.rsf"), shots, [3, ns], [0, 0], [1, 1])
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    for order in (1, 2):
+        r = subprocess.run([REF_EIK, "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf",
+                            "tds1=tds.rsf", "gradz=gz.rsf", "gradx=gx.rsf", "b1=2", "b2=2", "order=%d" % order],
+                           cwd=tmp_path, env=env, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        ref = {k: rsf.read(str(tmp_path / (f + ".rsf")))[1].reshape(ns, nx, nz)
+               for f, k in (("time", "time"), ("tdl", "tdl1"), ("tds", "tds1"), ("gz", "gradz"), ("gx", "gradx"))}
+        assert ref["time"].max() > 0.01 and np.abs(ref["gradx"]).max() > 0 and np.abs(ref["tds1"]).max() > 0
+        got = O.eikods(velt, d, d, shots, order=order, b1=2, b2=2, method=0, grads=True)
+        for k in FIELDS:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg="order %d %s" % (order, k))
+        if order == 1:
+            sw = O.eikods(velt, d, d, shots, order=1, b1=2, b2=2, method=1, grads=True)
+            for k in FIELDS:
+                np.testing.assert_array_equal(sw[k], ref[k], err_msg="sweeps %s" % k)
