@@ -1,6 +1,8 @@
 """The oracle is pinned to the reference: its FP32 build must reproduce the
 reference binary's images bit for bit on every golden case; its FP64 build is
 the precision reference of the GPU path."""
+import os
+
 import numpy as np
 import pytest
 
@@ -98,3 +100,78 @@ def test_oracle_forward_is_adjoint_of_migration(golden, name):
     lhs = float(np.dot(Fm.ravel(), d.astype(np.float64).ravel()))
     rhs = float(np.dot(m.astype(np.float64).ravel(), Ftd.ravel()))
     assert abs(lhs - rhs) <= 1e-10 * (np.linalg.norm(Fm) * np.linalg.norm(d))
+
+
+REF_MIG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "kirchmig2d_cig")
+
+
+def _random_tokens(rng):
+    t = ["cig=%d" % rng.integers(0, 2), "mode=%s" % rng.choice(["angle", "offset"]),
+         "cmp=%d" % rng.integers(0, 2), "half_angle=%d" % rng.integers(0, 2),
+         "type=%s" % rng.choice(["h", "l", "p"]), "antialias=%g" % rng.choice([0.5, 1.0, 2.0]),
+         "tau=%g" % rng.choice([0.0, 0.004]), "diff=%d" % rng.integers(0, 2),
+         "aperture=%g" % rng.choice([30.0, 60.0, 90.0]), "aperture_taper=%g" % rng.choice([5.0, 10.0]),
+         "angle_interp=%d" % rng.integers(0, 2)]
+    if rng.random() < 0.5:
+        t += ["angle_min=0", "angle_max=%g" % rng.choice([40.0, 60.0, 90.0]), "angle_step=%g" % rng.choice([1.0, 2.5])]
+    if rng.random() < 0.5:
+        t += ["oazmin=%g" % rng.choice([70.0, 80.0]), "oazmax=%g" % rng.choice([40.0, 50.0]),
+              "oaztaper=%g" % rng.choice([0.0, 10.0])]
+    if rng.random() < 0.4:
+        t += ["angle_taper_start=%g" % rng.choice([20.0, 30.0]), "angle_taper_end=%g" % rng.choice([45.0, 55.0])]
+    if rng.random() < 0.4:
+        t += ["direct_mute=1", "direct_mute_slope=%g" % rng.choice([0.3, 0.6]),
+              "direct_mute_intercept=%g" % rng.choice([0.0, 0.02]), "direct_mute_taper=%g" % rng.choice([0.02, 0.05])]
+    if rng.random() < 0.3:
+        t += ["aperture_trace=%d" % rng.integers(4, 12), "aperture_trace_taper=%d" % rng.integers(0, 4)]
+    return t
+
+
+@pytest.mark.skipif(not os.path.exists(REF_MIG), reason="reference kirchmig2d_cig not built (make -C oracle ref)")
+@pytest.mark.parametrize("seed", range(16))
+def test_oracle_fp32_bitexact_random_configurations(golden, tmp_path, seed):
+    # random parameter sets and geometries on the fixture tables, through the
+    # reference binary (one thread): the FP32 mirror gives its image bit for bit
+    import subprocess
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import rsf
+    rng = np.random.default_rng(700 + seed)
+    t = golden.meta["table"]
+    T, D = golden.tables()
+    rsf.write(str(tmp_path / "time.rsf"), T, t["n"], t["o"], t["d"])
+    rsf.write(str(tmp_path / "tds.rsf"), D, t["n"], t["o"], t["d"])
+    toks = _random_tokens(rng)
+    cmp1 = "cmp=1" in toks
+    p0, dp, npos = t["o"][2], t["d"][2], t["n"][2]
+    span = (npos - 1) * dp
+    ns, nh = int(rng.integers(1, 4)), int(rng.integers(2, 7))
+    f = lambda v: float(np.float32(v))  # noqa: E731
+    ds = f(rng.choice([0.04, 0.06, 0.1]))
+    dh = f(rng.choice([0.02, 0.04, 0.05]))
+    if cmp1:   # receivers at s + h inside the tables
+        h0 = f(-(nh // 2) * dh)
+        s0 = f(p0 + (nh // 2) * dh + 0.02)
+        ns = max(1, min(ns, int((span - (nh - 1) * dh - 0.04) / ds)))
+    else:
+        h0 = f(p0 + rng.uniform(0.0, span - (nh - 1) * dh))
+        s0 = f(p0 + rng.uniform(0.0, span - (ns - 1) * ds))
+    nt, dt = golden.meta["nt"], golden.meta["dt"]
+    data = (rng.standard_normal((ns, nh, nt)) * 1e-2).astype(np.float32)
+    rsf.write(str(tmp_path / "d.rsf"), data, [nt, nh, ns], [0.0, h0, s0], [dt, dh, ds], extra={"unit1": "s"})
+    r = subprocess.run([REF_MIG, "seismic_data=d.rsf", "migration=m.rsf", "stable=time.rsf", "sderiv=tds.rsf",
+                        "rtable=time.rsf", "rderiv=tds.rsf"] + toks, cwd=tmp_path, capture_output=True, text=True,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert r.returncode == 0, r.stderr[-500:]
+    h, ref = rsf.read(str(tmp_path / "m.rsf"))
+    ref = ref.reshape(h.n[2], h.n[1], h.n[0])
+    geom = dict(nt=nt, nh=nh, ns=ns, t0=0.0, dt=f(dt), h0=h0, dh=dh, s0=s0, ds=ds, nz=golden.meta["nz"],
+                nx=golden.meta["nx"], z0=0.0, dz=f(golden.meta["dz"]), x0=0.0, dx=f(golden.meta["dz"]),
+                sny=npos, sy0=f(p0), sdy=f(dp), rny=npos, ry0=f(p0), rdy=f(dp))
+    kp = kd.params(*toks)
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    assert ref.shape == (axis[0], geom["nx"], geom["nz"])
+    img = oracle.migrate_adj(_cases.oracle_params(kp, geom, axis), data, T, D, T, D, fp64=False).astype(np.float32)
+    k = 3 if "type=p" in toks else 0
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(img[:, k:, :], ref[:, k:, :]), "max abs diff %g" % np.max(np.abs(img - ref))
