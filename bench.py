@@ -11,9 +11,11 @@ One step = one migration of all 160,000 traces: 1.54e11 image-point x trace
 pairs.  Every step reads inputs far larger than L2 (1.9 GB of traces, 3.1 GB
 of tables), so L2 holds nothing between steps.
 
-Prints one JSON line (rank 0).  Multi-GPU (torchrun): every rank migrates its
-own 400-shot survey (weak scaling) and the images are summed with one NCCL
-all-reduce inside the timed region.
+Prints one JSON line (rank 0).  Multi-GPU (torchrun): the one 400-shot survey
+is partitioned by shots over the ranks (each rank migrates its block at the
+shots' positions in the whole survey, kcig_plan_set_shot_range) and the
+ranks' images are summed with one NCCL all-reduce inside the timed region:
+the total work is fixed (strong scaling).
 """
 from __future__ import annotations
 
@@ -231,13 +233,10 @@ def run_sample(wd: str, threads: int, meta: dict):
         import _cases
         import kirch_datuming_b200 as kd
         from kirch_datuming_b200 import rsf
-        r0, nr = SAMPLE_RCV
         _, data = rsf.read(f"{wd}/data.rsf")
         _, T = rsf.read(f"{wd}/time.rsf")
         _, D = rsf.read(f"{wd}/tds.rsf")
-        f = lambda x: float(np.float32(x))  # noqa: E731
-        geom = dict(geometry_dict(1, nr), s0=f(SAMPLE_SHOT * DP), h0=f(r0 * DP), sny=meta["npos"],
-                    rny=meta["npos"], sy0=f(meta["p_lo"] * DP), ry0=f(meta["p_lo"] * DP))
+        geom = sample_geometry(meta)
         kp = kd.params(*TOKENS)
         axis = kd.output_axis(kp, kd.geometry(**geom))
         os.environ["OMP_NUM_THREADS"] = str(threads)
@@ -248,10 +247,68 @@ def run_sample(wd: str, threads: int, meta: dict):
             "seconds": round(el, 3), "sample": meta["sample"]}
 
 
-def cpu_sample(threads: int, tables=None):
+def sample_geometry(meta: dict) -> dict:
+    """Geometry of the bounded sample (one shot, 48 receivers, the table
+    positions it uses) as the library's geometry keys."""
+    r0, nr = SAMPLE_RCV
+    f = lambda x: float(np.float32(x))  # noqa: E731
+    return dict(geometry_dict(1, nr), s0=f(SAMPLE_SHOT * DP), h0=f(r0 * DP), sny=meta["npos"],
+                rny=meta["npos"], sy0=f(meta["p_lo"] * DP), ry0=f(meta["p_lo"] * DP))
+
+
+def sample_parity(wd: str, meta: dict, threads: int) -> dict:
+    """Image errors on the bounded sample of the production workload (one
+    shot x 48 receivers over the full 601x1601 grid): the GPU image against
+    the FP64 oracle and against the reference binary's own FP32 image, and
+    the reference against the FP64 oracle (relative L2 in double, as
+    src/rsf_l2cmp.cpp:9-10)."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    import _cases
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import rsf
+    _, data = rsf.read(f"{wd}/data.rsf")
+    _, T = rsf.read(f"{wd}/time.rsf")
+    _, D = rsf.read(f"{wd}/tds.rsf")
+    geom = sample_geometry(meta)
+    kp = kd.params(*TOKENS)
+    axis = kd.output_axis(kp, kd.geometry(**geom))
+    plan = kd.Plan(kp, kd.geometry(**geom))
+    dT = torch.from_numpy(np.ascontiguousarray(T, dtype=np.float32)).cuda()
+    dD = torch.from_numpy(np.ascontiguousarray(D, dtype=np.float32)).cuda()
+    plan.set_tables(dT, dD, dT, dD)
+    img = torch.zeros((plan.ng, NX, NZ), dtype=torch.float32, device="cuda")
+    plan.migrate(torch.from_numpy(np.ascontiguousarray(data, dtype=np.float32)).cuda(), img)
+    plan.close()
+    gpu = img.cpu().numpy().astype(np.float64)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    o64 = oracle.migrate_adj(_cases.oracle_params(kp, geom, axis), data, T, D, T, D, fp64=True)
+    out = {"sample": meta["sample"], "relL2_vs_fp64_oracle": oracle.rel_l2(gpu, o64),
+           "relL2_vs_reference": None, "reference_vs_fp64": None}
+    if os.path.exists(f"{wd}/mig.rsf"):
+        _, ref = rsf.read(f"{wd}/mig.rsf")
+        ref = np.asarray(ref, dtype=np.float64).reshape(o64.shape)
+        out["relL2_vs_reference"] = oracle.rel_l2(gpu, ref)
+        out["reference_vs_fp64"] = oracle.rel_l2(ref, o64)
+    return out
+
+
+def cpu_sample(threads: int, tables=None, parity: bool = False):
+    """cpu_baseline of the bounded sample; with parity=True also the image
+    errors of the same sample (sample_parity), as (baseline, parity)."""
     wd = tempfile.mkdtemp(prefix="kcig_cpu_")
     try:
-        return run_sample(wd, threads, prepare_sample(wd, threads, tables))
+        meta = prepare_sample(wd, threads, tables)
+        base = run_sample(wd, threads, meta)
+        if not parity:
+            return base
+        try:
+            par = sample_parity(wd, meta, threads)
+        except Exception as e:  # noqa: BLE001 -- reported, never required
+            par = {"error": str(e)[-300:]}
+        return base, par
     finally:
         shutil.rmtree(wd, ignore_errors=True)
 
@@ -747,20 +804,28 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    v, T, D, data = make_workload(seed=11 + rank)
+    from kirch_datuming_b200 import shard
+    v, T, D, data_all = make_workload(seed=11)  # the same survey on every rank
     kp = kd.params(*TOKENS)
     geom = geometry_dict()
     st = torch.cuda.current_stream()
     plan = kd.Plan(kp, kd.geometry(**geom), stream=st.cuda_stream)
     plan.set_tables(T, D, T, D)
+    # this rank's block of shots, at their positions in the whole survey
+    first, count = shard.shot_range(NPOS, rank, world)
+    if world > 1:
+        plan.set_shot_range(first, count)
+        data = data_all[first:first + count].contiguous()
+        del data_all
+    else:
+        data = data_all
     ng = plan.ng
     image = torch.zeros((ng, NX, NZ), dtype=torch.float32, device="cuda")
-    pairs = NPOS * NPOS * NZ * NX
+    pairs = NPOS * NPOS * NZ * NX  # the whole survey: every rank's share together
 
     def step():
         plan.migrate(data, image)
-        if dist is not None:
-            dist.all_reduce(image)
+        shard.reduce_image(image)
 
     for _ in range(args.warmup):
         step()
@@ -788,19 +853,39 @@ def main():
         ms = float(t.item())
         dist.barrier()
 
-    # end to end through the public C ABI with pinned host buffers
+    # end to end through the public C ABI with pinned host buffers: every
+    # step copies the tables and this rank's traces in and the image out; with
+    # several ranks the images are summed on the devices in between (device
+    # time on the plan's stream, the max over ranks)
     hT, hD = T.cpu().pin_memory(), D.cpu().pin_memory()
     hdata = data.cpu().pin_memory()
     himg = torch.zeros((ng, NX, NZ), dtype=torch.float32).pin_memory()
-    eplan = kd.Plan(kp, kd.geometry(**geom))
+    eplan = kd.Plan(kp, kd.geometry(**geom), stream=st.cuda_stream)
+    if world > 1:
+        eplan.set_shot_range(first, count)
     e2e_ms = []
     for i in range(args.e2e_steps + 1):
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         t0 = time.perf_counter()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st)
         eplan.set_tables(hT, hD, hT, hD)
         eplan.migrate(hdata, himg)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        if dist is not None:
+            image.copy_(himg, non_blocking=True)
+            shard.reduce_image(image)
+            himg.copy_(image, non_blocking=True)
+        a1.record(st)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        e2e_ms.append(max(wall, a0.elapsed_time(a1)))
     e2e_ms = statistics.median(e2e_ms[1:]) if len(e2e_ms) > 1 else e2e_ms[0]
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
     eplan.close()
     # the same call with the tables left in host memory (KCIG_MEM_HOST_STREAM):
     # only the slices each leg batch interpolates cross PCIe -- the mode for
@@ -822,25 +907,27 @@ def main():
 
     ksum_ms = statistics.median(sum_ms)
     peak, peak_src = measured_peaks()
-    achieved = pairs * B_PAIR / (ksum_ms / 1e3) / 1e9
+    pairs_rank = count * NPOS * NZ * NX  # the summation kernel's own share
+    achieved = pairs_rank * B_PAIR / (ksum_ms / 1e3) / 1e9
     tpp = profiled_traffic()
     line = {
-        "metric": metric, "value": world * pairs / (ms / 1e3) / 1e9, "unit": "Gpairs/s", "n_gpus": world,
+        "metric": metric, "value": pairs / (ms / 1e3) / 1e9, "unit": "Gpairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "pairs_per_gpu_step": pairs, "parallelism": "dp%d (shots per rank, "
-                   "image all-reduce)" % world if world > 1 else "single GPU",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_step": pairs,
+                   "parallelism": ("dp%d (one survey, shots %d..%d on rank 0 of %d, image all-reduce)"
+                                   % (world, first, first + count - 1, world)) if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (1.9 GB traces, 3.1 GB tables per step)",
                    "tables": "GPU eikods2d tables (kcig_eikods: order 2, tds1), 400 positions"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "kernel": "k_sum", "kernel_ms": ksum_ms,
                      "algorithmic_bytes_per_pair": B_PAIR,
-                     "traffic": (tpp * pairs) if tpp is not None else None,
-                     "issue": issue_ceiling(pairs / (ksum_ms / 1e3), (clk or {}).get("sm_mhz")),
+                     "traffic": (tpp * pairs_rank) if tpp is not None else None,
+                     "issue": issue_ceiling(pairs_rank / (ksum_ms / 1e3), (clk or {}).get("sm_mhz")),
                      "note": "16 B/pair counts the receiver leg's fields once per pair; k_sum loads each "
                              "receiver leg once per block of 4 shots, so its DRAM traffic (ncu, 'traffic') is "
                              "below the algorithmic bytes and frac can pass 1: the kernel is issue-bound"},
-        "e2e": {"value": world * pairs / (e2e_ms / 1e3) / 1e9 if world == 1 else None, "unit": "Gpairs/s",
+        "e2e": {"value": pairs / (e2e_ms / 1e3) / 1e9, "unit": "Gpairs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "streamed_tables": None if stream_ms is None else {
             "value": pairs / (stream_ms / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": stream_ms,
@@ -850,7 +937,8 @@ def main():
     }
     if rank == 0 and not args.no_cpu_baseline and args.size == "full":
         try:
-            line["cpu_baseline"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()))
+            line["cpu_baseline"], line["parity"] = cpu_sample(threads, tables=(T.cpu().numpy(), D.cpu().numpy()),
+                                                              parity=True)
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(e)[:300]}
     if dist is None and not args.no_tables and args.size == "full":

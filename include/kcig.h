@@ -35,7 +35,7 @@ extern "C" {
 /* Parameters of kirchmig2d_cig.  Field meanings and defaults are those of
  * src/kirchmig2d_cig.cpp:494-958; kcig_params_init() fills the defaults. */
 typedef struct kcig_params {
-    int adj;                 /* 1 = migration (only adj=1 is built)           :565-568 */
+    int adj;                 /* 1 = migration, 0 = forward modelling          :565-568 */
     int cig;                 /* 0 stack, 1 common-image gathers               :569-572 */
     int cig_is_angle;        /* mode=angle (1) or mode=offset (0)             :554-563 */
     int cmp;                 /* receiver position = s+h (1) or h (0)          :573-576 */
@@ -135,6 +135,23 @@ int kcig_plan_set_gradients(kcig_plan *plan, const float *sgradx, const float *s
  * device pointers (memory).  Replaces the shot/trace loop :979-1339. */
 int kcig_migrate(kcig_plan *plan, const float *data, float *image, int memory);
 
+/* Shot positions of the survey axis (s0 + is * ds, ds = 0 for one shot) for
+ * shots first .. first + count - 1, both as the migration uses them: in FP64
+ * for continuous quantities (pos) and in the reference's float expression
+ * s0 + (float)is * ds for its discrete decisions (posf, :980).  Host-only;
+ * either output may be NULL. */
+int kcig_shot_positions(const kcig_geometry *g, int first, int count, double *pos, float *posf);
+
+/* Restrict kcig_migrate to shots first .. first + count - 1 of the plan's
+ * survey (first = 0, count = -1: all).  The data then holds only those shots
+ * ([count][nh][nt]), while every shot keeps the position and antialias
+ * spacing it has in the whole survey (kcig_shot_positions), so images of a
+ * partition of the shots add up to the whole survey's image -- the shot
+ * sharding of one survey over ranks, whose images are then summed (one
+ * all-reduce).  The image is zeroed first as always.  No counterpart in the
+ * reference, which migrates a whole file. */
+int kcig_plan_set_shot_range(kcig_plan *plan, int first, int count);
+
 /* Number of summation-kernel launches and the device time (ms, CUDA events)
  * of the last kcig_migrate; either pointer may be NULL. */
 int kcig_plan_last_stats(const kcig_plan *plan, int *sum_launches, float *sum_ms, int *all_launches);
@@ -179,7 +196,8 @@ int kcig_leg_fields_device(kcig_plan *plan, int is_source, double pos, double *T
  * gradient volumes (both or NULL); outputs are caller-owned device arrays
  * [nx][nz] (any may be NULL).  The first call on a device looks up the
  * scratch array's device address, so make that first call before any stream
- * capture.  All calls share the one array and leave the last call's contents
+ * capture.  The address is kept for the life of the process: do not call
+ * this entry point again after cudaDeviceReset on that device.  All calls share the one array and leave the last call's contents
  * in it (every value is written before it is read, so nothing needs clearing);
  * calls that overlap on the GPU -- from other threads or other streams --
  * race and must be serialised by the caller.  Runs on `stream` and returns
@@ -299,18 +317,24 @@ void kcig_graph_destroy(kcig_graph *graph);
 
 /* ---------------------------------------------------------------------------
  * Learned traveltime surrogate (no counterpart in the reference, which reads
- * eikods2d tables).  A network T(xs, z, x) = T0 * tau(xs, z, x) with T0 the
- * straight-ray time |(x, z) - (xs, zsrc)| / vref and tau a 4x128 SiLU MLP on
- * 64-frequency Fourier features of the normalised inputs, BF16 tensor-core
- * GEMMs with FP32 accumulation.  Trained on a table volume by the library's
- * own forward and backward kernels (Adam, loss mean((1000 (T - T_table))^2)
- * in ms^2); plugged into a plan it replaces the table interpolation and the
- * finite-difference gradients of every leg. */
+ * eikods2d tables).  A network T(xs, z, x) = Tb + residual_ms * 1e-3 * out
+ * (or Tb * (1 + out) when residual_ms = 0), with Tb the closed-form first
+ * arrival of the background medium v(z) = vref + vgrad * (z - zsrc) (straight
+ * rays |(x, z) - (xs, zsrc)| / vref when vgrad = 0) and out a 4x128 SiLU MLP
+ * on 64-frequency Fourier features of the normalised inputs, BF16
+ * tensor-core GEMMs with FP32 accumulation.  Trained on a table volume by the
+ * library's own forward and backward kernels (Adam, loss
+ * mean((1000 (T - T_table))^2) in ms^2, fixed-order gradient sums: a run is
+ * reproducible bit for bit); plugged into a plan it replaces the table
+ * interpolation of every leg (kcig_plan_set_surrogate_options says which
+ * leg quantities it supplies). */
 typedef struct kcig_surrogate kcig_surrogate;
 typedef struct {
     float lo[3], hi[3]; /* domain of (xs, z, x) in km, mapped to [-1, 1]      */
     float fmax;         /* highest Fourier frequency (half-waves over the domain) */
-    float vref, zsrc;   /* background velocity (km/s) and source depth (km)    */
+    float vref, zsrc;   /* background velocity at the source depth (km/s) and source depth (km) */
+    float vgrad;        /* background velocity gradient (1/s): 0 = constant velocity */
+    float residual_ms;  /* > 0: T = Tb + residual_ms * 1e-3 * out; 0: T = Tb * (1 + out) */
 } kcig_surrogate_config;
 
 int kcig_surrogate_nparams(void);
@@ -353,6 +377,21 @@ float kcig_plan_last_prelude_ms(const kcig_plan *plan);
  * surrogates instead of tables (either may be NULL: that side uses its
  * tables).  The surrogates must outlive the plan's migrations. */
 int kcig_plan_set_surrogate(kcig_plan *plan, kcig_surrogate *src, kcig_surrogate *rcv);
+/* Which leg quantities a plan's surrogates supply (the traveltime always):
+ *   angle KCIG_SG_ANGLE_FD (default): the gradient direction comes from the
+ *     surrogate traveltime field by the tables' own centred differences and
+ *     triangle smoothing (src/kirchmig2d_cig.cpp:130-152, :424-492), so a
+ *     surrogate that matches the tables gives the tables' angles;
+ *     KCIG_SG_ANGLE_NETWORK: from the network's input gradient dT/dz, dT/dx.
+ *   tx KCIG_SG_TX_NETWORK (default): the source-position derivative (the
+ *     antialias width, :1264-1266) from the network's backward pass;
+ *     KCIG_SG_TX_TABLE: from the plan's sderiv/rderiv tables, interpolated as
+ *     the table path does (the tables must be set and on the device). */
+#define KCIG_SG_ANGLE_FD 0
+#define KCIG_SG_ANGLE_NETWORK 1
+#define KCIG_SG_TX_NETWORK 0
+#define KCIG_SG_TX_TABLE 1
+int kcig_plan_set_surrogate_options(kcig_plan *plan, int angle, int tx);
 
 /* ---- ADCIG stitching of depth windows (src/layercom_cig.cpp) ------------ */
 

@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
-           "run_cli", "doubint_device", "leg_fields_device", "eikonal_tables", "eikods", "library_path",
+           "run_cli", "doubint_device", "leg_fields_device", "shot_positions", "eikonal_tables", "eikods", "library_path",
            "cli_path", "eikods_cli_path", "kirchmig2d_cli_path", "layercom_cig_cli_path", "params_kirchmig2d",
            "stitch_window"]
 
@@ -40,7 +40,8 @@ class KcigError(RuntimeError):
 
 class SurrogateConfig(ctypes.Structure):
     _fields_ = [("lo", ctypes.c_float * 3), ("hi", ctypes.c_float * 3), ("fmax", ctypes.c_float),
-                ("vref", ctypes.c_float), ("zsrc", ctypes.c_float)]
+                ("vref", ctypes.c_float), ("zsrc", ctypes.c_float), ("vgrad", ctypes.c_float),
+                ("residual_ms", ctypes.c_float)]
 
 
 class EikodsOpts(ctypes.Structure):
@@ -129,6 +130,9 @@ def lib():
                                            [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_ulonglong, fp, vp])
         L.kcig_plan_set_surrogate.argtypes = [vp, vp, vp]
+        L.kcig_plan_set_shot_range.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.kcig_shot_positions.argtypes = [ctypes.POINTER(Geometry), ctypes.c_int, ctypes.c_int, vp, vp]
+        L.kcig_plan_set_surrogate_options.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.kcig_shots_prepare.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Shot), ctypes.c_int]
         L.kcig_migrate_prepared.argtypes = [vp, fp, ctypes.c_int]
         L.kcig_migrate_shots.argtypes = [vp, ctypes.c_int, ctypes.POINTER(Shot), fp, ctypes.c_int]
@@ -234,16 +238,29 @@ class Plan:
         self._keep += [stable, sderiv, rtable, rderiv]
         _check(lib().kcig_plan_set_tables(self._h, *[p for p, _ in ptrs], mem))
 
+    def set_shot_range(self, first: int = 0, count: int = -1):
+        """Migrate only shots first .. first + count - 1 of the survey, at
+        their positions in the whole survey (kcig_plan_set_shot_range); the
+        data passed to migrate() then holds just those shots."""
+        _check(lib().kcig_plan_set_shot_range(self._h, int(first), int(count)))
+
     def set_gradients(self, sgradx, sgradz, rgradx, rgradz):
         ptrs = [_ptr(x) for x in (sgradx, sgradz, rgradx, rgradz)]
         self._keep += [sgradx, sgradz, rgradx, rgradz]
         _check(lib().kcig_plan_set_gradients(self._h, *[p for p, _ in ptrs], ptrs[0][1]))
 
-    def set_surrogate(self, src=None, rcv=None):
+    def set_surrogate(self, src=None, rcv=None, angle: str = "fd", tx: str = "network"):
         """Leg fields of the source / receiver legs from Surrogate objects
-        instead of the tables (None: that side uses its tables)."""
+        instead of the tables (None: that side uses its tables).  angle:
+        "fd" (the tables' finite-difference gradient of the surrogate's
+        traveltime) or "network" (its input gradient); tx: the antialias
+        derivative from the "network" or from the "table"
+        (kcig_plan_set_surrogate_options)."""
         self._keep += [src, rcv]
         _check(lib().kcig_plan_set_surrogate(self._h, src.handle if src else None, rcv.handle if rcv else None))
+        a = {"fd": 0, "network": 1}[angle]
+        t = {"network": 0, "table": 1}[tx]
+        _check(lib().kcig_plan_set_surrogate_options(self._h, a, t))
 
     def prepare_shots(self, shots):
         """Upload ragged shots (include/kcig.h kcig_shot): a list of dicts with
@@ -374,6 +391,16 @@ def stitch_window(out, layer, start: int, end: int, previous_end: int = -1, stit
     return bad.value
 
 
+def shot_positions(g: Geometry, first: int = 0, count: int = None):
+    """(FP64, FP32) shot positions of the survey axis as the migration uses
+    them (kcig_shot_positions); host-only."""
+    import numpy as np
+    count = g.ns - first if count is None else count
+    pos, posf = np.empty(count, np.float64), np.empty(count, np.float32)
+    _check(lib().kcig_shot_positions(ctypes.byref(g), int(first), int(count), pos.ctypes.data, posf.ctypes.data))
+    return pos, posf
+
+
 def leg_fields_device(plan: Plan, is_source: int, pos: float):
     """(T float64, Tx float32, phi float64, w float32) device tensors [nx*nz] of one leg."""
     import torch
@@ -461,15 +488,19 @@ def tc_selftest(X, W):
 
 
 class Surrogate:
-    """Learned traveltime surrogate T(xs, z, x) = T0 * tau (include/kcig.h,
+    """Learned traveltime surrogate T(xs, z, x) = Tb + residual_ms * 1e-3 * out
+    (or Tb * (1 + out) with residual_ms = 0), Tb the first arrival of the
+    background medium vref + vgrad * (z - zsrc) (include/kcig.h,
     kcig_surrogate_*): trained and evaluated by the library's tensor-core
     kernels on the current CUDA device.  lo/hi: domain of (xs, z, x) in km."""
 
-    def __init__(self, lo, hi, fmax: float = 8.0, vref: float = 1.5, zsrc: float = 0.0, seed: int = 0):
+    def __init__(self, lo, hi, fmax: float = 8.0, vref: float = 1.5, zsrc: float = 0.0, seed: int = 0,
+                 vgrad: float = 0.0, residual_ms: float = 0.0):
         c = SurrogateConfig()
         for i in range(3):
             c.lo[i], c.hi[i] = float(lo[i]), float(hi[i])
         c.fmax, c.vref, c.zsrc = float(fmax), float(vref), float(zsrc)
+        c.vgrad, c.residual_ms = float(vgrad), float(residual_ms)
         self.config = c
         h = ctypes.c_void_p()
         _check(lib().kcig_surrogate_create(ctypes.byref(c), int(seed), ctypes.byref(h)))

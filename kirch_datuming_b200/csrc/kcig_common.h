@@ -77,12 +77,26 @@ struct FieldArgs {
 
 // Workspace for the gradient pipeline: 4 double planes per position.
 int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches = nullptr);
+// The two stages of launch_leg_fields: the table interpolation (T, Tx, w;
+// with gradient volumes also their interpolation into the work planes), and
+// the traveltime gradient of the T already in out.TP -- centred differences
+// of radius a.radius, triangle smoothing of radius a.smooth -- into its
+// direction phi (out.TP[].y).  launches (if given) is incremented.
+int launch_leg_interp(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches);
+int launch_leg_grad(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches);
+// Whether launch_leg_grad uses the work planes (gradient volumes, or a halo
+// too wide for the fused kernel): 4 * nzx doubles per leg.
+bool leg_grad_needs_work(const FieldArgs &a);
 
 // Leg fields from a traveltime surrogate (kcig_mlp.cu): one launch for all
-// `nlegs` legs (only .pos and .scale of each are read).  The surrogate's
-// status flag is cleared by sg_reset_status and read by sg_check_status.
+// `nlegs` legs (only .pos and .scale of each are read).  mode 0: the
+// traveltime only (TP[].x; the rest from the tables and the
+// finite-difference pass); 1: also its source-position derivative and the
+// aperture weight (XW); 2: also the direction phi from the network's own
+// input gradient.  The surrogate's status flag is cleared by sg_reset_status
+// and read by sg_check_status.
 int launch_surrogate_fields(kcig_surrogate *s, const LegInterp *legs, int nlegs, const kcig_geometry &g,
-                            const kcig_params &p, LegFields out, cudaStream_t st);
+                            const kcig_params &p, LegFields out, int mode, cudaStream_t st);
 int sg_reset_status(kcig_surrogate *s, cudaStream_t st);
 int sg_check_status(kcig_surrogate *s, cudaStream_t st);
 

@@ -499,21 +499,27 @@ size_t leg_grad_fused_smem(int radius, int smooth)
     return (4 * (size_t)W * W + 2 * smooth + 1 + 2 * (2 * r + 1)) * sizeof(double);
 }
 
-int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
+int launch_leg_interp(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
 {
+    if (a.n <= 0) return KCIG_OK;
+    const int nzx = a.nz * a.nx;
+    k_leg_interp<<<dim3((nzx + 255) / 256, a.n), dim3(256), 0, st>>>(a, out, work);
+    KCIG_CUDA(cudaGetLastError());
+    if (launches) (*launches)++;
+    return KCIG_OK;
+}
+
+int launch_leg_grad(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
+{
+    if (a.n <= 0 || !a.angle) return KCIG_OK;
     int nl = 0;
     struct Count {
         int *dst;
         int &n;
-        ~Count() { if (dst) *dst = n; }
+        ~Count() { if (dst) *dst += n; }
     } count{launches, nl};
-    if (a.n <= 0) return KCIG_OK;
     const int nzx = a.nz * a.nx;
     const dim3 blk(256), grd((nzx + 255) / 256, a.n);
-    k_leg_interp<<<grd, blk, 0, st>>>(a, out, work);
-    nl++;
-    KCIG_CUDA(cudaGetLastError());
-    if (!a.angle) return KCIG_OK;
     const size_t fsm = leg_grad_fused_smem(a.radius, a.smooth);
     if (!a.use_grad && fsm <= 200 * 1024) {
         KCIG_TRY(set_dyn_smem((const void *)k_leg_grad_fused, (int)fsm));
@@ -543,6 +549,24 @@ int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStrea
     nl++;
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
+}
+
+bool leg_grad_needs_work(const FieldArgs &a)
+{
+    return a.angle && (a.use_grad || leg_grad_fused_smem(a.radius, a.smooth) > 200 * 1024);
+}
+
+int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
+{
+    int nl = 0;
+    const int rc = launch_leg_interp(a, out, work, st, &nl);
+    if (rc == KCIG_OK && a.angle) {
+        const int rc2 = launch_leg_grad(a, out, work, st, &nl);
+        if (launches) *launches = nl;
+        return rc2;
+    }
+    if (launches) *launches = nl;
+    return rc;
 }
 
 // ============================================================ K3 summation ==

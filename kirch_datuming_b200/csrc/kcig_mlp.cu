@@ -6,13 +6,20 @@
 //   f   = interleaved [sin th_ik, cos th_ik], th_ik = (k+1) * fstep * u_i,
 //         k < 64, fstep = pi * fmax / 64                 -> 384 features
 //   h_1 = SiLU(W_1 f + b_1), h_l = SiLU(W_l h_{l-1} + b_l), l = 2..4 (128 wide)
-//   tau = 1 + w_o . h_4 + b_o,   T = T0 * tau,   T0 = |(x, z) - (xs, zsrc)| / vref
-// BF16 operands (weights, features, activations, backpropagated gradients)
-// with FP32 accumulation in TMEM; biases, output layer and the traveltime
-// algebra in FP32.  Input gradients (dT/dxs for the antialias width, dT/dz,
-// dT/dx for the scattering angle) come from the backward pass of the same
-// network.  A 128-point tile is one M=128 MMA row block; a thread pair owns a
-// row (one TMEM lane), each thread half of its 128 columns.
+//   out = w_o . h_4 + b_o
+//   T   = Tb + rscale * out   (additive residual, rscale > 0), or
+//   T   = Tb * (1 + out)      (factored form, rscale = 0)
+// with Tb the first-arrival time of a background medium vref + vgrad (z -
+// zsrc) (closed form; straight rays at vgrad = 0): the network learns what
+// the background misses.  BF16 operands (weights, features, activations,
+// backpropagated gradients) with FP32 accumulation in TMEM; biases, output
+// layer and the traveltime algebra in FP32 (FP64 for the traveltime a leg
+// field stores).  Input gradients come from the backward pass of the same
+// network: dT/dxs for the antialias width, and -- on request -- dT/dz, dT/dx
+// for the scattering angle; by default a plan takes the angle from the
+// traveltime's finite-difference gradient, as with tables.  A 128-point tile
+// is one M=128 MMA row block; each TMEM lane (row) is shared by the threads
+// of the warps that read it, each taking a share of its 128 columns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -103,6 +110,8 @@ struct SgNet {
     const float *P;          // [NPARAM] FP32 parameters
     float lo[3], sc[3];      // u = (v - lo) * sc - 1
     float fstep, vref, zsrc;
+    float vgrad;             // background velocity vref + vgrad * (z - zsrc)
+    float rscale;            // > 0: T = Tb + rscale * out (s); 0: T = Tb * (1 + out)
 };
 
 __device__ __forceinline__ float sg_sig(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
@@ -113,17 +122,45 @@ __device__ __forceinline__ float sg_dsilu(float z)
     return s * (1.0f + z * (1.0f - s));
 }
 
-// straight-ray background: T0 and its derivatives in (xs, z, x)
-__device__ __forceinline__ void sg_background(const SgNet &n, float xs, float z, float x, float &T0, float &dxs,
-                                              float &dz, float &dx)
+// Background traveltime Tb(xs, z, x) and its derivatives: the first arrival
+// in the medium v(z) = vref + vgrad (z - zsrc) from a source at (xs, zsrc),
+// the closed form for a constant velocity gradient g,
+//     Tb = acosh(1 + eps) / g,   eps = g^2 r^2 / (2 vs vp),
+// vs = vref at the source, vp = v at the point, r the distance; written as
+//     Tb = r / sqrt(vs vp) * log1p(eps + sqrt(eps (2 + eps))) / sqrt(2 eps)
+// so that it tends to the straight-ray time r / vref as g -> 0 without
+// cancellation.  Its gradient, from dTb/dA = 1 / (g sqrt(A^2 - 1)) with
+// A = 1 + eps:  dTb/dx = (x - xs) k,  dTb/dz = (z - zsrc - r^2 g / (2 vp)) k,
+// k = sqrt(2 / (vs vp (2 + eps))) / r,  dTb/dxs = -dTb/dx (0 at r = 0).
+template <typename F>
+__device__ __forceinline__ void sg_background(const SgNet &n, F xs, F z, F x, F &Tb, F &dxs, F &dz, F &dx)
 {
-    const float ex = x - xs, ez = z - n.zsrc;
-    const float dist = sqrtf(ex * ex + ez * ez);
-    T0 = dist / n.vref;
-    const float inv = dist > 0.0f ? 1.0f / (dist * n.vref) : 0.0f;
-    dxs = -ex * inv;
-    dz = ez * inv;
-    dx = ex * inv;
+    const F ex = x - xs, ez = z - (F)n.zsrc, g = (F)n.vgrad, vs = (F)n.vref;
+    const F r2 = ex * ex + ez * ez, r = sqrt(r2);
+    F vp = vs + g * ez;
+    vp = vp > (F)1e-3 * vs ? vp : (F)1e-3 * vs;
+    const F q = vs * vp, eps = g * g * r2 / ((F)2 * q);
+    const F fac = eps < (F)1e-6 ? (F)1 - eps / (F)12 : log1p(eps + sqrt(eps * ((F)2 + eps))) / sqrt((F)2 * eps);
+    Tb = r * fac / sqrt(q);
+    if (r > (F)0) {
+        const F k = sqrt((F)2 / (q * ((F)2 + eps))) / r;
+        dx = ex * k;
+        dxs = -dx;
+        dz = (ez - r2 * g / ((F)2 * vp)) * k;
+    } else {
+        dx = dxs = dz = (F)0;
+    }
+}
+
+// The network's output `out` (w_o . h_4 + b_o) and the background combine as
+// T = Tb + osc * out: osc = rscale for an additive residual, osc = Tb for the
+// factored form T = Tb (1 + out).  dT/dv = dTb/dv (1 + m out) + osc dout/dv
+// with m = 0 (additive) or 1 (factored).
+template <typename F>
+__device__ __forceinline__ F sg_out_scale(const SgNet &n, F Tb, F &m)
+{
+    m = n.rscale > 0.0f ? (F)0 : (F)1;
+    return n.rscale > 0.0f ? (F)n.rscale : Tb;
 }
 
 // 128x128 block of a row-major BF16 matrix (rows = outputs, row stride ld,
@@ -213,7 +250,10 @@ __device__ __forceinline__ void sg_epi_silu(uint32_t tacc, const float *bias, un
 }
 
 // backward epilogue: g = G * SiLU'(z + bias) as BF16 into dst; returns the
-// sum over the thread's columns of bf16(g) * vdot (vdot may be null)
+// sum over the thread's columns of bf16(g) * vdot (vdot may be null).
+// colsum (may be null): this warp's column sums over its 32 rows, stored
+// (not added) at colsum[c] -- one slot array per row group, so every slot
+// has one writer and the caller adds the groups in a fixed order
 __device__ __forceinline__ float sg_epi_back(uint32_t tG, uint32_t tZ, const float *bias, unsigned char *dst, int r,
                                              int cb, int nq, const float *vdot, float *colsum)
 {
@@ -241,7 +281,7 @@ __device__ __forceinline__ float sg_epi_back(uint32_t tG, uint32_t tZ, const flo
                 x += __shfl_xor_sync(0xffffffffu, x, 4);
                 x += __shfl_xor_sync(0xffffffffu, x, 2);
                 x += __shfl_xor_sync(0xffffffffu, x, 1);
-                if ((threadIdx.x & 31) == 0) atomicAdd(colsum + c0 + j, x);
+                if ((threadIdx.x & 31) == 0) colsum[c0 + j] = x;
             }
         }
 #pragma unroll
@@ -287,7 +327,15 @@ struct SgFieldArgs {
     int *status;
 };
 constexpr int kSgFieldSmem = 7 * sg::TB;
+// what a launch computes: the traveltime only (its position derivative and
+// the aperture weight come from the tables, its direction from the
+// finite-difference pass), the traveltime and its source-position
+// derivative from the network's backward pass (direction from the
+// finite-difference pass), or also the direction from the network's input
+// gradient in depth and lateral position
+enum { SGF_T = 0, SGF_TX = 1, SGF_ALL = 2 };
 
+template <int MODE>
 __global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
 {
     using namespace sg;
@@ -401,8 +449,8 @@ __global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
             tc::commit(&bar);
         }
         if (!(ok = sg_wait(&bar, phase))) break;
-        float out_part;
-        {   // output layer and the start of the backward pass (d tau / d out = 1)
+        float out_part, xs_part = 0.0f, gz_part = 0.0f, gx_part = 0.0f;
+        {   // output layer and the start of the backward pass (d out / d out = 1)
             float part = 0.0f, v[32];
             const int c0 = 32 * h;
             tc::tmem_ld32(D4 + c0, v);
@@ -412,44 +460,50 @@ __global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
                 part += sg_silu(z) * wo[c0 + jj];
                 v[jj] = wo[c0 + jj] * sg_dsilu(z);
             }
+            if (MODE != SGF_T) {
 #pragma unroll
-            for (int g = 0; g < 4; g++) sg_store8(actB, r, c0 + 8 * g, v + 8 * g);
+                for (int g = 0; g < 4; g++) sg_store8(actB, r, c0 + 8 * g, v + 8 * g);
+            }
             out_part = part;
         }
-        sg_sync_for_mma();
-        if (warp == 0 && tc::elect_one()) {
-            tc::gemm(T4, aB, LBO_K, SBO_K, aW4, LBO_M, SBO_M, 128, ID_KM, false);
-            tc::commit(&bar);
+        if (MODE != SGF_T) {
+            sg_sync_for_mma();
+            if (warp == 0 && tc::elect_one()) {
+                tc::gemm(T4, aB, LBO_K, SBO_K, aW4, LBO_M, SBO_M, 128, ID_KM, false);
+                tc::commit(&bar);
+            }
+            if (!(ok = sg_wait(&bar, phase))) break;
+            sg_epi_back(D4, D3, bias3, actA, r, 32 * h, 1, nullptr, nullptr);
+            sg_sync_for_mma();
+            if (warp == 0 && tc::elect_one()) {
+                tc::gemm(T3, aA, LBO_K, SBO_K, aW3, LBO_M, SBO_M, 128, ID_KM, false);
+                tc::commit(&bar);
+            }
+            if (!(ok = sg_wait(&bar, phase))) break;
+            sg_epi_back(D3, D2, bias2, actB, r, 32 * h, 1, nullptr, nullptr);
+            sg_sync_for_mma();
+            if (warp == 0 && tc::elect_one()) {
+                tc::gemm(T2, aB, LBO_K, SBO_K, aW2, LBO_M, SBO_M, 128, ID_KM, false);
+                tc::commit(&bar);
+            }
+            if (!(ok = sg_wait(&bar, phase))) break;
+            xs_part = sg_epi_back(D2, D1, b1p, actA, r, 32 * h, 1, vleg, nullptr);
         }
-        if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_back(D4, D3, bias3, actA, r, 32 * h, 1, nullptr, nullptr);
-        sg_sync_for_mma();
-        if (warp == 0 && tc::elect_one()) {
-            tc::gemm(T3, aA, LBO_K, SBO_K, aW3, LBO_M, SBO_M, 128, ID_KM, false);
-            tc::commit(&bar);
+        if (MODE == SGF_ALL) {
+            sg_sync_for_mma();
+            if (warp == 0 && tc::elect_one()) {
+                tc::gemm(T3, aA, LBO_K, SBO_K, aW1z, LBO_M, SBO_M, 128, ID_KM, false);
+                tc::gemm(T4, aA, LBO_K, SBO_K, aW1x, LBO_M, SBO_M, 128, ID_KM, false);
+                tc::commit(&bar);
+            }
+            if (!(ok = sg_wait(&bar, phase))) break;
+            // each column quarter: its part of d out/d u_z (G0z) and d out/d u_x (G0x)
+            gz_part = sg_feature_grad(D3, 32 * h, 1, uz, n.fstep);
+            gx_part = sg_feature_grad(D4, 32 * h, 1, ux, n.fstep);
         }
-        if (!(ok = sg_wait(&bar, phase))) break;
-        sg_epi_back(D3, D2, bias2, actB, r, 32 * h, 1, nullptr, nullptr);
-        sg_sync_for_mma();
-        if (warp == 0 && tc::elect_one()) {
-            tc::gemm(T2, aB, LBO_K, SBO_K, aW2, LBO_M, SBO_M, 128, ID_KM, false);
-            tc::commit(&bar);
-        }
-        if (!(ok = sg_wait(&bar, phase))) break;
-        const float xs_part = sg_epi_back(D2, D1, b1p, actA, r, 32 * h, 1, vleg, nullptr);
-        sg_sync_for_mma();
-        if (warp == 0 && tc::elect_one()) {
-            tc::gemm(T3, aA, LBO_K, SBO_K, aW1z, LBO_M, SBO_M, 128, ID_KM, false);
-            tc::gemm(T4, aA, LBO_K, SBO_K, aW1x, LBO_M, SBO_M, 128, ID_KM, false);
-            tc::commit(&bar);
-        }
-        if (!(ok = sg_wait(&bar, phase))) break;
-        // each column quarter: its part of d tau/d u_z (G0z) and d tau/d u_x
-        // (G0x); the four partials of each quantity meet in actB, which no
-        // MMA reads any more in this item
+        // the four column quarters' partials of each quantity meet in actB,
+        // which no MMA reads any more in this item
         {
-            const float gz_part = sg_feature_grad(D3, 32 * h, 1, uz, n.fstep);
-            const float gx_part = sg_feature_grad(D4, 32 * h, 1, ux, n.fstep);
             float *xq = reinterpret_cast<float *>(actB);  // [quantity][quarter][row]
             xq[(0 * 4 + h) * 128 + r] = out_part;
             xq[(1 * 4 + h) * 128 + r] = xs_part;
@@ -465,22 +519,30 @@ __global__ void __launch_bounds__(512, 1) k_sg_fields(SgFieldArgs a)
             for (int k = 0; k < 4; k++)
                 sum[k] = (xq[(k * 4) * 128 + r] + xq[(k * 4 + 1) * 128 + r]) +
                          (xq[(k * 4 + 2) * 128 + r] + xq[(k * 4 + 3) * 128 + r]);
-            const float tau = 1.0f + sum[0] + bo;
-            const float gxs = sum[1] * n.sc[0];
-            const float gz = sum[2] * n.sc[1];
-            const float gx = sum[3] * n.sc[2];
-            float T0, bxs, bz, bx;
-            sg_background(n, xs, zf, xf, T0, bxs, bz, bx);
-            const float T = T0 * tau;
-            const float Txs = bxs * tau + T0 * gxs, Tz = bz * tau + T0 * gz, Tx = bx * tau + T0 * gx;
-            const double phi = (sqrt((double)Tx * Tx + (double)Tz * Tz) <= 1.0e-12)
-                                   ? __longlong_as_double(0x7ff8000000000000ll)
-                                   : atan2((double)Tz, (double)Tx);
-            const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin,
-                                                 a.rtaper);
+            const float out = sum[0] + bo;
+            // the traveltime in FP64: background plus the network's term
+            double Tb, bxs, bz, bx, m;
+            sg_background<double>(n, (double)L.pos, (double)zf, (double)xf, Tb, bxs, bz, bx);
+            const double osc = sg_out_scale<double>(n, Tb, m);
+            const double T = Tb + osc * (double)out;
             const size_t o = (size_t)j * nzx + i;
-            a.out.TP[o] = make_double2((double)T, phi);
-            a.out.XW[o] = make_float2(Txs * L.scale, (float)w);
+            if (MODE == SGF_T) {
+                a.out.TP[o].x = T;  // Tx and w come from the tables, phi from the traveltime's gradient
+            } else {
+                const double gxs = (double)(sum[1] * n.sc[0]);
+                const double Txs = bxs * (1.0 + m * out) + osc * gxs;
+                double phi = 0.0;  // MODE SGF_TX: written by the finite-difference pass
+                if (MODE == SGF_ALL) {
+                    const double Tz = bz * (1.0 + m * out) + osc * (double)(sum[2] * n.sc[1]);
+                    const double Tx = bx * (1.0 + m * out) + osc * (double)(sum[3] * n.sc[2]);
+                    phi = (sqrt(Tx * Tx + Tz * Tz) <= 1.0e-12) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                               : atan2(Tz, Tx);
+                }
+                const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin,
+                                                     a.rtaper);
+                a.out.TP[o] = make_double2(T, phi);
+                a.out.XW[o] = make_float2((float)Txs * L.scale, (float)w);
+            }
         }
         __syncthreads();
     }
@@ -536,8 +598,10 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
     extern __shared__ __align__(1024) unsigned char dsm[];
     unsigned char *wbuf = dsm, *fbuf = dsm + TB, *H1 = dsm + 2 * TB, *H2 = dsm + 3 * TB, *H3 = dsm + 4 * TB;
     unsigned char *gbuf = dsm + 5 * TB;
-    __shared__ float bias[4][H], wo[H], colsum[4][H], cwo[H], red[4][2][H];
-    __shared__ float sc_loss, sc_dbo;
+    __shared__ float bias[4][H], wo[H], red[4][2][H];
+    // per row group (32 samples each) partial sums, added in a fixed order
+    // at the end so that a tile's gradient is the same on every run
+    __shared__ float colpart[4][4][H], cwopart[4][H], lpart[4], dpart[4];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tslot;
     const SgNet &n = a.net;
@@ -547,18 +611,11 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
     const int sc = valid ? s_idx : a.n - 1;
 
     if (warp == 0) tc::tmem_alloc(&tslot, 512);
-    if (tid == 0) {
-        tc::mbar_init(&bar, 1);
-        sc_loss = 0.0f;
-        sc_dbo = 0.0f;
-    }
+    if (tid == 0) tc::mbar_init(&bar, 1);
+    const int rg = warp & 3;  // row group of this warp
     for (int q = tid; q < H; q += blockDim.x) {
-        for (int l = 0; l < 4; l++) {
-            bias[l][q] = n.P[OFF_B1 + l * H + q];
-            colsum[l][q] = 0.0f;
-        }
+        for (int l = 0; l < 4; l++) bias[l][q] = n.P[OFF_B1 + l * H + q];
         wo[q] = n.P[OFF_WO + q];
-        cwo[q] = 0.0f;
     }
     const float vxs = a.xs[sc], vz = a.z[sc], vx = a.x[sc];
     const float u0 = (vxs - n.lo[0]) * n.sc[0] - 1.0f, u1 = (vz - n.lo[1]) * n.sc[1] - 1.0f;
@@ -630,16 +687,25 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
             red[0][h][r] = part_out;
         }
         __syncthreads();
-        const float tau = 1.0f + red[0][0][r] + red[0][1][r] + n.P[OFF_BO];
-        float T0, bxs, bz, bx;
-        sg_background(n, vxs, vz, vx, T0, bxs, bz, bx);
-        float gout = 1.0f;  // EVAL: d tau / d out
+        const float out = red[0][0][r] + red[0][1][r] + n.P[OFF_BO];
+        float Tb, bxs, bz, bx, mfac;
+        sg_background<float>(n, vxs, vz, vx, Tb, bxs, bz, bx);
+        const float osc = sg_out_scale<float>(n, Tb, mfac);
+        float gout = 1.0f;  // EVAL: d out / d out
         if (MODE == SG_TRAIN) {
-            const float res = valid ? 1000.0f * (T0 * tau - a.Ttrue[sc]) : 0.0f;
-            gout = 2.0f * res * 1000.0f * T0 / (float)a.ntotal;
+            const float res = valid ? 1000.0f * (Tb + osc * out - a.Ttrue[sc]) : 0.0f;
+            gout = 2.0f * res * 1000.0f * osc / (float)a.ntotal;
             if (h == 0) {
-                atomicAdd(&sc_loss, res * res / (float)a.ntotal);
-                atomicAdd(&sc_dbo, gout);
+                float l = res * res / (float)a.ntotal, d = gout;
+#pragma unroll
+                for (int m = 16; m >= 1; m >>= 1) {
+                    l += __shfl_xor_sync(0xffffffffu, l, m);
+                    d += __shfl_xor_sync(0xffffffffu, d, m);
+                }
+                if ((tid & 31) == 0) {
+                    lpart[rg] = l;
+                    dpart[rg] = d;
+                }
             }
         }
         // g4 = gout * wo * SiLU'(z4) -> gbuf; TRAIN: d wo, d b4 column sums
@@ -659,8 +725,8 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
                         gb += __shfl_xor_sync(0xffffffffu, gb, m);
                     }
                     if ((tid & 31) == 0) {
-                        atomicAdd(&cwo[c], hw);
-                        atomicAdd(&colsum[3][c], gb);
+                        cwopart[rg][c] = hw;
+                        colpart[3][rg][c] = gb;
                     }
                 }
             }
@@ -704,7 +770,7 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
                 sg_dump_tile(a.stages + 6 * 16384, wbuf);
             }
             sg_epi_back(Dk, Dpk, bias[2 - k], gbuf, r, 64 * h, 2, nullptr,
-                        MODE == SG_TRAIN ? colsum[2 - k] : nullptr);
+                        MODE == SG_TRAIN ? colpart[2 - k][rg] : nullptr);
         }
         if (!ok) break;
         // layer 1: weight gradient per feature chunk (TRAIN) or input gradient (EVAL)
@@ -743,21 +809,22 @@ __global__ void __launch_bounds__(256, 1) k_sg_tile(SgTileArgs a)
         __syncthreads();
         if (MODE == SG_TRAIN) {
             for (int q = tid; q < H; q += blockDim.x) {
-                for (int l = 0; l < 4; l++) part[OFF_B1 + l * H + q] = colsum[l][q];
-                part[OFF_WO + q] = cwo[q];
+                for (int l = 0; l < 4; l++)
+                    part[OFF_B1 + l * H + q] = ((colpart[l][0][q] + colpart[l][1][q]) + colpart[l][2][q]) + colpart[l][3][q];
+                part[OFF_WO + q] = ((cwopart[0][q] + cwopart[1][q]) + cwopart[2][q]) + cwopart[3][q];
             }
             if (tid == 0) {
-                part[OFF_BO] = sc_dbo;
-                part[NPARAM] = sc_loss;
+                part[OFF_BO] = ((dpart[0] + dpart[1]) + dpart[2]) + dpart[3];
+                part[NPARAM] = ((lpart[0] + lpart[1]) + lpart[2]) + lpart[3];
             }
         } else if (h == 0 && valid) {
             const float gxs = (red[1][0][r] + red[1][1][r]) * n.sc[0];
             const float gz = (red[2][0][r] + red[2][1][r]) * n.sc[1];
             const float gx = (red[3][0][r] + red[3][1][r]) * n.sc[2];
-            a.T[s_idx] = T0 * tau;
-            a.Txs[s_idx] = bxs * tau + T0 * gxs;
-            a.Tz[s_idx] = bz * tau + T0 * gz;
-            a.Tx[s_idx] = bx * tau + T0 * gx;
+            a.T[s_idx] = Tb + osc * out;
+            a.Txs[s_idx] = bxs * (1.0f + mfac * out) + osc * gxs;
+            a.Tz[s_idx] = bz * (1.0f + mfac * out) + osc * gz;
+            a.Tx[s_idx] = bx * (1.0f + mfac * out) + osc * gx;
         }
     } while (false);
     if (!ok && tid == 0) atomicExch(a.status, 1);
@@ -822,7 +889,7 @@ __global__ void k_sg_sample(const float *table, int npos, float p0, float dp, in
 }
 
 static int launch_sg_fields(const SgNet &net, const LegInterp *legs, int nlegs, const kcig_geometry &g,
-                            const kcig_params &p, LegFields out, int *status, cudaStream_t st)
+                            const kcig_params &p, LegFields out, int *status, int mode, cudaStream_t st)
 {
     if (nlegs <= 0) return KCIG_OK;
     static int sms = 0;
@@ -849,8 +916,16 @@ static int launch_sg_fields(const SgNet &net, const LegInterp *legs, int nlegs, 
     a.status = status;
     const long long items = (long long)nlegs * ((g.nz * g.nx + 127) / 128);
     const int grid = (int)std::min<long long>(sms, items);
-    KCIG_TRY(set_dyn_smem((const void *)k_sg_fields, kSgFieldSmem));
-    k_sg_fields<<<grid, 512, kSgFieldSmem, st>>>(a);
+    if (mode == SGF_T) {
+        KCIG_TRY(set_dyn_smem((const void *)k_sg_fields<SGF_T>, kSgFieldSmem));
+        k_sg_fields<SGF_T><<<grid, 512, kSgFieldSmem, st>>>(a);
+    } else if (mode == SGF_TX) {
+        KCIG_TRY(set_dyn_smem((const void *)k_sg_fields<SGF_TX>, kSgFieldSmem));
+        k_sg_fields<SGF_TX><<<grid, 512, kSgFieldSmem, st>>>(a);
+    } else {
+        KCIG_TRY(set_dyn_smem((const void *)k_sg_fields<SGF_ALL>, kSgFieldSmem));
+        k_sg_fields<SGF_ALL><<<grid, 512, kSgFieldSmem, st>>>(a);
+    }
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
@@ -892,9 +967,9 @@ namespace kcig {
 static SgNet sg_net(const kcig_surrogate *s);
 
 int launch_surrogate_fields(kcig_surrogate *s, const LegInterp *legs, int nlegs, const kcig_geometry &g,
-                            const kcig_params &p, LegFields out, cudaStream_t st)
+                            const kcig_params &p, LegFields out, int mode, cudaStream_t st)
 {
-    return launch_sg_fields(sg_net(s), legs, nlegs, g, p, out, s->status, st);
+    return launch_sg_fields(sg_net(s), legs, nlegs, g, p, out, s->status, mode, st);
 }
 
 int sg_reset_status(kcig_surrogate *s, cudaStream_t st)
@@ -915,6 +990,8 @@ static SgNet sg_net(const kcig_surrogate *s)
     n.fstep = 3.14159265358979f * s->cfg.fmax / (float)sg::NF;
     n.vref = s->cfg.vref;
     n.zsrc = s->cfg.zsrc;
+    n.vgrad = s->cfg.vgrad;
+    n.rscale = s->cfg.residual_ms * 1e-3f;
     return n;
 }
 
@@ -987,6 +1064,8 @@ extern "C" int kcig_surrogate_create(const kcig_surrogate_config *cfg, unsigned 
     for (int i = 0; i < 3; i++)
         if (!(cfg->hi[i] > cfg->lo[i])) return set_error(KCIG_ERR_ARG, "kcig_surrogate_create: need hi > lo on every input");
     if (!(cfg->vref > 0.0f) || !(cfg->fmax > 0.0f)) return set_error(KCIG_ERR_ARG, "kcig_surrogate_create: need vref > 0 and fmax > 0");
+    if (!std::isfinite(cfg->vgrad) || !(cfg->residual_ms >= 0.0f))
+        return set_error(KCIG_ERR_ARG, "kcig_surrogate_create: need a finite vgrad and residual_ms >= 0");
     kcig_surrogate *s = new kcig_surrogate();
     s->cfg = *cfg;
     int rc = KCIG_OK;

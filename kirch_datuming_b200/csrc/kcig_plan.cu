@@ -67,6 +67,8 @@ struct kcig_plan {
     int sum_launches = 0, all_launches = 0;
     float sum_ms = 0.f, fields_ms = 0.f, prelude_ms = 0.f;
     kcig_surrogate *sg_src = nullptr, *sg_rcv = nullptr;  // leg fields from surrogates instead of tables
+    int sg_angle = KCIG_SG_ANGLE_FD, sg_tx = KCIG_SG_TX_NETWORK;  // what the surrogates supply
+    int shot_first = 0, shot_count = -1;  // kcig_plan_set_shot_range: shots of the survey kcig_migrate takes
     struct ShotsPrepared *shots = nullptr;                 // ragged shots uploaded by kcig_shots_prepare
     int use_graph = 0;                                     // replay kcig_migrate_prepared as a CUDA graph
     int tile = 0;                                          // summation tile variant (kcig_plan_autotune)
@@ -224,14 +226,57 @@ int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int
     const kcig_geometry &g = P->g;
     const size_t nzx = (size_t)g.nz * g.nx;
     if (n <= 0) return KCIG_OK;
+    const int angle = P->p.cig && P->p.cig_is_angle;
     if (kcig_surrogate *sgt = is_source ? P->sg_src : P->sg_rcv) {
-        KCIG_TRY(launch_surrogate_fields(sgt, d_legs, n, g, P->p, LegFields{TP, XW}, P->st));
+        // the surrogate's traveltime; its source-position derivative from the
+        // network or the tables; its direction from the network or, as with
+        // tables, from the finite-difference gradient of the traveltime field
+        const bool tx_table = P->sg_tx == KCIG_SG_TX_TABLE;
+        const bool fd_angle = angle && P->sg_angle == KCIG_SG_ANGLE_FD;
+        FieldArgs a;
+        memset(&a, 0, sizeof a);
+        a.tab = is_source ? P->stab : P->rtab;
+        a.der = is_source ? P->sder : P->rder;
+        a.nz = g.nz;
+        a.nx = g.nx;
+        a.dz = g.dz;
+        a.dx = g.dx;
+        a.x0 = g.x0;
+        a.radius = P->p.angle_grad_radius;
+        a.smooth = P->p.angle_smooth;
+        a.angle = angle;
+        a.aper = P->p.aperture;
+        a.aper_taper = P->p.aperture_taper;
+        a.rmin = P->p.aperture_rmin;
+        a.rtaper = P->p.aperture_rtaper;
+        if (tx_table) {
+            if (!a.tab || !a.der || P->stream_tables)
+                return set_error(KCIG_ERR_ARG, "surrogate with table derivatives: the plan needs device tables");
+            a.legs = d_legs;
+            a.n = n;
+            int nl = 0;
+            KCIG_TRY(launch_leg_interp(a, LegFields{TP, XW}, nullptr, P->st, &nl));
+            P->all_launches += nl;
+        }
+        const int mode = tx_table ? 0 : (angle && !fd_angle ? 2 : 1);
+        KCIG_TRY(launch_surrogate_fields(sgt, d_legs, n, g, P->p, LegFields{TP, XW}, mode, P->st));
         P->all_launches += 1;
+        if (fd_angle) {
+            const int FB = leg_grad_needs_work(a) ? field_batch(P, (size_t)n) : n;
+            if (leg_grad_needs_work(a)) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
+            for (int j0 = 0; j0 < n; j0 += FB) {
+                a.legs = d_legs + j0;
+                a.n = std::min(FB, n - j0);
+                int nl = 0;
+                KCIG_TRY(launch_leg_grad(a, LegFields{TP + (size_t)j0 * nzx, XW + (size_t)j0 * nzx},
+                                         P->d_work.as<double>(), P->st, &nl));
+                P->all_launches += nl;
+            }
+        }
         return KCIG_OK;
     }
     if (P->stream_tables && !tab)
         return set_error(KCIG_ERR_UNSUPPORTED, "tables kept in host memory need the host-side leg path");
-    const int angle = P->p.cig && P->p.cig_is_angle;
     const int FB = field_batch(P, (size_t)n);
     if (angle) KCIG_TRY(P->d_work.ensure((size_t)FB * 4 * nzx * sizeof(double)));
     for (int j0 = 0; j0 < n; j0 += FB) {
@@ -523,7 +568,8 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     // data and image on the device
     const float *d_data = data;
     float *d_img = image;
-    const size_t data_bytes = (size_t)g.ns * g.nh * g.nt * sizeof(float);
+    const int ns = P->shot_count > 0 ? P->shot_count : ns;  // shots of this call (kcig_plan_set_shot_range)
+    const size_t data_bytes = (size_t)ns * g.nh * g.nt * sizeof(float);
     if (memory == KCIG_MEM_HOST) {
         KCIG_TRY(upload(P->d_data, data, data_bytes, st));
         d_data = P->d_data.as<float>();
@@ -534,28 +580,26 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     // per-trace scalars (:1054-1105), all in double
     const double ds = g.ns == 1 ? 0.0 : (double)g.ds, dh = g.nh == 1 ? 0.0 : (double)g.dh;
     // positions in FP64 for every continuous use, and as the reference's
-    // float expressions (:980, :1055, :1061) for its discrete decisions
-    std::vector<double> sx(g.ns), hx(g.nh);
-    std::vector<float> sxf(g.ns), hxf(g.nh);
-    for (int is = 0; is < g.ns; is++) {
-        sx[is] = (double)g.s0 + (double)is * ds;
-        sxf[is] = g.s0 + (float)is * (float)ds;
-    }
+    // float expressions (:980, :1055, :1061) for its discrete decisions; a
+    // shot range takes its shots' positions from the whole survey's axis
+    std::vector<double> sx(ns), hx(g.nh);
+    std::vector<float> sxf(ns), hxf(g.nh);
+    kcig_shot_positions(&g, P->shot_first, ns, sx.data(), sxf.data());
     for (int ih = 0; ih < g.nh; ih++) {
         hx[ih] = (double)g.h0 + (double)ih * dh;
         hxf[ih] = g.h0 + (float)ih * (float)dh;
     }
-    std::vector<LegInterp> slegs(g.ns);
-    std::vector<int> ist(g.ns);
-    for (int is = 0; is < g.ns; is++) {
+    std::vector<LegInterp> slegs(ns);
+    std::vector<int> ist(ns);
+    for (int is = 0; is < ns; is++) {
         ist[is] = leg_interp(P, 1, sxf[is], sx[is], &slegs[is]);
         slegs[is].scale = (float)ds;
     }
-    const size_t ntr_all = (size_t)g.ns * g.nh;
+    const size_t ntr_all = (size_t)ns * g.nh;
     std::vector<float> trw(ntr_all);
     std::vector<int> igo(ntr_all, 0);
     std::vector<double> msx(ntr_all), mrx(ntr_all);
-    for (int is = 0; is < g.ns; is++)
+    for (int is = 0; is < ns; is++)
         for (int ih = 0; ih < g.nh; ih++) {
             const size_t t = (size_t)is * g.nh + ih;
             const double rpos = p.cmp ? sx[is] + hx[ih] : hx[ih];
@@ -612,7 +656,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     const unsigned long long fixed = (shared_r ? (unsigned long long)nhc * leg_bytes : 0) + work_bytes;
     long long room = (long long)budget - (long long)fixed;
     int nsb = (int)std::max<long long>(1, room / (long long)per_shot);
-    nsb = std::min(nsb, g.ns);
+    nsb = std::min(nsb, ns);
 
     if (shared_r) {
         KCIG_TRY(P->d_rT.ensure((size_t)nhc * nzx * sizeof(double2)));
@@ -663,8 +707,8 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             rc = fields(0, rl, P->d_rT.as<double2>(), P->d_rF.as<float2>());
             if (rc) break;
         }
-        for (int s0 = 0; s0 < g.ns && rc == KCIG_OK; s0 += nsb) {
-            const int nsh = std::min(nsb, g.ns - s0);
+        for (int s0 = 0; s0 < ns && rc == KCIG_OK; s0 += nsb) {
+            const int nsh = std::min(nsb, ns - s0);
             std::vector<LegInterp> sl(slegs.begin() + s0, slegs.begin() + s0 + nsh);
             rc = fields(1, sl, P->d_sT.as<double2>(), P->d_sF.as<float2>());
             if (rc) break;
@@ -799,7 +843,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             P->all_launches += nl + (sa.nsplit > 1 ? 1 : 0);
             first = false;
             // the host-side arrays are reused by the next batch
-            if (s0 + nsb < g.ns || r0 + nhc < g.nh) {
+            if (s0 + nsb < ns || r0 + nhc < g.nh) {
                 cudaError_t e = cudaStreamSynchronize(st);
                 if (e != cudaSuccess) {
                     rc = cuda_error(e, "cudaStreamSynchronize(batch)");
@@ -852,6 +896,46 @@ extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_s
     return KCIG_OK;
 }
 
+extern "C" int kcig_shot_positions(const kcig_geometry *g, int first, int count, double *pos, float *posf)
+{
+    if (!g || first < 0 || count < 0 || (long long)first + count > g->ns)
+        return set_error(KCIG_ERR_ARG, "kcig_shot_positions: shots [%d, %d) outside the axis of %d shots", first,
+                         first + count, g ? g->ns : 0);
+    const double ds = g->ns == 1 ? 0.0 : (double)g->ds;
+    for (int k = 0; k < count; k++) {
+        const int is = first + k;
+        if (pos) pos[k] = (double)g->s0 + (double)is * ds;
+        if (posf) posf[k] = g->s0 + (float)is * (float)ds;
+    }
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_set_shot_range(kcig_plan *P, int first, int count)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_shot_range: null plan");
+    if (count == -1 && first == 0) {
+        P->shot_first = 0;
+        P->shot_count = -1;
+        return KCIG_OK;
+    }
+    if (first < 0 || count < 1 || (long long)first + count > P->g.ns)
+        return set_error(KCIG_ERR_ARG, "kcig_plan_set_shot_range: shots [%d, %d) outside the survey's %d", first,
+                         first + count, P->g.ns);
+    P->shot_first = first;
+    P->shot_count = count;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_plan_set_surrogate_options(kcig_plan *P, int angle, int tx)
+{
+    if (!P) return set_error(KCIG_ERR_ARG, "kcig_plan_set_surrogate_options: null plan");
+    if ((angle != KCIG_SG_ANGLE_FD && angle != KCIG_SG_ANGLE_NETWORK) || (tx != KCIG_SG_TX_NETWORK && tx != KCIG_SG_TX_TABLE))
+        return set_error(KCIG_ERR_ARG, "kcig_plan_set_surrogate_options: angle %d / tx %d not known", angle, tx);
+    P->sg_angle = angle;
+    P->sg_tx = tx;
+    return KCIG_OK;
+}
+
 // ------------------------------------------------------- forward modelling --
 // kirchmig2d_cig adj=0: data [ns][nh][nt] from an image [ng][nx][nz] with the
 // plan's geometry, the exact adjoint of kcig_migrate without the direct mute
@@ -859,6 +943,8 @@ extern "C" int kcig_plan_set_surrogate(kcig_plan *P, kcig_surrogate *src, kcig_s
 // direct_mute=1).  Same per-trace gates as the migration.
 extern "C" int kcig_model(kcig_plan *P, const float *image, float *data, int memory)
 {
+    if (P && P->shot_count > 0)
+        return set_error(KCIG_ERR_UNSUPPORTED, "kcig_model: a shot range is not built for forward modelling");
     if (!P || !image || !data) return set_error(KCIG_ERR_ARG, "kcig_model: null argument");
     if (!(P->sg_src || P->stab) || !(P->sg_rcv || P->rtab)) return set_error(KCIG_ERR_ARG, "kcig_model: tables not set");
     const kcig_params &p = P->p;

@@ -17,8 +17,19 @@ def shot_slice(ns: int, rank: int, world: int) -> slice:
     return slice(start, start + base + (1 if rank < extra else 0))
 
 
+def shot_range(ns: int, rank: int, world: int) -> tuple:
+    """(first, count) of this rank's shots, for Plan.set_shot_range: the rank
+    keeps the whole survey's geometry, so its shots sit at exactly the
+    positions (and antialias spacing) a single-process run gives them."""
+    sl = shot_slice(ns, rank, world)
+    return sl.start, sl.stop - sl.start
+
+
 def shard_geometry(geom: dict, rank: int, world: int) -> dict:
-    """Geometry of this rank's shots: the shot axis origin moves, spacing stays."""
+    """Geometry of this rank's shots as a survey of its own: the shot axis
+    origin moves to the first shot and the spacing stays.  Positions are then
+    re-derived from the new origin and can round differently in FP32 from the
+    whole survey's; Plan.set_shot_range with shot_range() avoids that."""
     sl = shot_slice(geom["ns"], rank, world)
     g = dict(geom)
     g["ns"] = sl.stop - sl.start

@@ -12,10 +12,15 @@ Network (per leg position xs and image point (z, x), all in km):
     f     = [sin(th_ik), cos(th_ik)] interleaved, th_ik = (k+1) * fstep * u_i,
             k < 64, fstep = pi * fmax / 64            -> 384 features
     h_1   = SiLU(W_1 f + b_1),  h_l = SiLU(W_l h_{l-1} + b_l)  (l = 2..4, width 128)
-    tau   = 1 + w_o . h_4 + b_o
-    T     = T0 * tau,  T0 = sqrt((x - xs)^2 + (z - zsrc)^2) / vref
-(the factored form T = T0 * tau keeps the source singularity out of the
-network, as in factored-eikonal learning, e.g. EikoNet).
+    out   = w_o . h_4 + b_o
+    T     = Tb + rscale * out   (additive residual, residual_ms > 0), or
+    T     = Tb * (1 + out)      (factored form, residual_ms = 0)
+with Tb the first arrival of the background medium v(z) = vref + vgrad (z -
+zsrc): acosh(1 + g^2 r^2 / (2 vs vp)) / g for a constant velocity gradient g
+(the straight-ray time r / vref at g = 0).  The factored form keeps the
+source singularity out of the network, as in factored-eikonal learning
+(e.g. EikoNet); the additive form lets it learn only what the background
+misses.
 
 Parameter vector layout (float32 on the device): W_1 [128][384], W_2, W_3,
 W_4 [128][128] (row = output), b_1..b_4 [128], w_o [128], b_o.
@@ -73,10 +78,11 @@ def init_params(seed: int = 0, out_scale: float = 0.01):
 
 
 class Config:
-    def __init__(self, lo, hi, fmax=8.0, vref=1.5, zsrc=0.0):
+    def __init__(self, lo, hi, fmax=8.0, vref=1.5, zsrc=0.0, vgrad=0.0, residual_ms=0.0):
         self.lo = np.asarray(lo, np.float64)
         self.hi = np.asarray(hi, np.float64)
         self.fmax, self.vref, self.zsrc = float(fmax), float(vref), float(zsrc)
+        self.vgrad, self.residual_ms = float(vgrad), float(residual_ms)
 
     @property
     def scale(self):
@@ -117,13 +123,30 @@ def _features(cfg, u):
 
 
 def _background(cfg, xs, z, x):
+    """Tb and dTb/dxs, dTb/dz, dTb/dx of the linear-gradient medium
+    (constant velocity at vgrad = 0)."""
     dxv = x - xs
     dzv = z - cfg.zsrc
-    dist = np.sqrt(dxv * dxv + dzv * dzv)
-    T0 = dist / cfg.vref
+    g, vs = cfg.vgrad, cfg.vref
+    r2 = dxv * dxv + dzv * dzv
+    r = np.sqrt(r2)
+    vp = np.maximum(vs + g * dzv, 1e-3 * vs)
+    q = vs * vp
+    eps = g * g * r2 / (2.0 * q)
     with np.errstate(invalid="ignore", divide="ignore"):
-        inv = np.where(dist > 0, 1.0 / (dist * cfg.vref), 0.0)
-    return T0, -dxv * inv, dzv * inv, dxv * inv  # T0, dT0/dxs, dT0/dz, dT0/dx
+        fac = np.where(eps < 1e-12, 1.0 - eps / 12.0,
+                       np.log1p(eps + np.sqrt(eps * (2.0 + eps))) / np.sqrt(2.0 * np.maximum(eps, 1e-300)))
+        Tb = r * fac / np.sqrt(q)
+        k = np.where(r > 0, np.sqrt(2.0 / (q * (2.0 + eps))) / np.where(r > 0, r, 1.0), 0.0)
+    dx = dxv * k
+    return Tb, -dx, (dzv - r2 * g / (2.0 * vp)) * k, dx
+
+
+def _out_scale(cfg, Tb):
+    """(osc, m): T = Tb + osc * out and dT/dv = dTb/dv (1 + m out) + osc dout/dv."""
+    if cfg.residual_ms > 0:
+        return np.full_like(Tb, cfg.residual_ms * 1e-3), 0.0
+    return Tb, 1.0
 
 
 def forward(params, cfg: Config, xs, z, x, mirror: bool = False, keep: bool = False):
@@ -143,19 +166,20 @@ def forward(params, cfg: Config, xs, z, x, mirror: bool = False, keep: bool = Fa
         hl = _silu(zl)
         hs.append(rb(hl) if l < 3 else hl)
     out = hs[4] @ wo + bo
-    tau = 1.0 + out
-    # input gradient of tau: backpropagate d tau / d out = 1
+    # input gradient of out: backpropagate d out / d out = 1
     g = rb(wo[None, :] * _dsilu(zs[3]))
     for l in (3, 2, 1):
         g = rb((g @ Wq[l]) * _dsilu(zs[l - 1]))
-    G0 = g @ Wq[0]                                # d tau / d feature
-    dtau_du = np.stack([(G0 * df)[:, i * 2 * NF:(i + 1) * 2 * NF].sum(1) for i in range(NIN)], axis=1)
-    dtau_dv = dtau_du * cfg.scale
-    T0, dxs0, dz0, dx0 = _background(cfg, xs, z, x)
-    T = T0 * tau
-    res = (T, dxs0 * tau + T0 * dtau_dv[:, 0], dz0 * tau + T0 * dtau_dv[:, 1], dx0 * tau + T0 * dtau_dv[:, 2])
+    G0 = g @ Wq[0]                                # d out / d feature
+    dout_du = np.stack([(G0 * df)[:, i * 2 * NF:(i + 1) * 2 * NF].sum(1) for i in range(NIN)], axis=1)
+    dout_dv = dout_du * cfg.scale
+    Tb, dxs0, dz0, dx0 = _background(cfg, xs, z, x)
+    osc, m = _out_scale(cfg, Tb)
+    T = Tb + osc * out
+    f1 = 1.0 + m * out
+    res = (T, dxs0 * f1 + osc * dout_dv[:, 0], dz0 * f1 + osc * dout_dv[:, 1], dx0 * f1 + osc * dout_dv[:, 2])
     if keep:
-        return res, dict(a=a, zs=zs, hs=hs, T0=T0, tau=tau, Wq=Wq, wo=wo)
+        return res, dict(a=a, zs=zs, hs=hs, osc=osc, out=out, Wq=Wq, wo=wo)
     return res
 
 
@@ -167,7 +191,7 @@ def loss_grad(params, cfg: Config, xs, z, x, Ttrue, mirror: bool = False, ntotal
     n = len(T) if ntotal is None else ntotal
     r = 1000.0 * (T - np.asarray(Ttrue, np.float64))
     loss = float((r * r).sum() / n)
-    gout = 2.0 * r * 1000.0 * k["T0"] / n          # d loss / d out
+    gout = 2.0 * r * 1000.0 * k["osc"] / n         # d loss / d out
     W, b, wo, bo = unpack(params)
     grad = np.zeros(NPARAM)
     zs, hs, Wq = k["zs"], k["hs"], k["Wq"]

@@ -27,13 +27,18 @@ import surrogate as sgo  # oracle/surrogate.py: the float64 restatement of the n
 LO, HI = (0.0, 0.0, 0.0), (4.0, 2.0, 4.0)
 
 
-def _net(seed=5, out_scale=30.0, fmax=6.0):
-    s = kd.Surrogate(LO, HI, fmax=fmax, vref=1.5, zsrc=0.0, seed=seed)
+# the straight-ray factored form T = T0 (1 + out) and the linear-gradient
+# background with an additive residual T = Tb + 1 ms * out
+BACKGROUNDS = {"straight_factored": dict(vgrad=0.0, residual_ms=0.0), "lingrad_additive": dict(vgrad=0.6, residual_ms=1.0)}
+
+
+def _net(seed=5, out_scale=30.0, fmax=6.0, bg="straight_factored"):
+    s = kd.Surrogate(LO, HI, fmax=fmax, vref=1.5, zsrc=0.0, seed=seed, **BACKGROUNDS[bg])
     p = s.get_params()
-    p[sgo.OFF_WO:sgo.OFF_BO] *= out_scale  # tau visibly different from 1
+    p[sgo.OFF_WO:sgo.OFF_BO] *= out_scale  # the network's term visibly non-zero
     p[sgo.OFF_B1:sgo.OFF_WO] = np.random.default_rng(seed).uniform(-0.2, 0.2, 4 * sgo.H)
     s.set_params(p)
-    cfg = sgo.Config(LO, HI, fmax=fmax, vref=1.5, zsrc=0.0)
+    cfg = sgo.Config(LO, HI, fmax=fmax, vref=1.5, zsrc=0.0, **BACKGROUNDS[bg])
     return s, cfg, p
 
 
@@ -47,7 +52,8 @@ def _stats(e):
     return np.median(e), np.percentile(e, 95), e.max()
 
 
-def test_surrogate_eval_vs_oracle():
+@pytest.mark.parametrize("bg", sorted(BACKGROUNDS))
+def test_surrogate_eval_vs_oracle(bg):
     # forward value and input gradient through the tcgen05 kernels against the
     # float64 oracle with the same BF16 rounding points.  The GPU builds the
     # Fourier features by rotation (a few FP32 ulp off the exact sines), so a
@@ -55,14 +61,17 @@ def test_surrogate_eval_vs_oracle():
     # way (one BF16 ulp, 2^-8 relative) and moves that point by up to ~1e-3:
     # most points agree to FP32 accumulation order, a few percent carry a flip.
     # A wrong operand layout or TMEM mapping is off by O(1) everywhere.
-    s, cfg, p = _net()
+    # Errors are in units of the network's output (T - Tb) / osc.
+    s, cfg, p = _net(bg=bg)
     xs, z, x = _points(1000)
     got = [t.cpu().double().numpy() for t in s.eval(xs, z, x)]
-    ref = sgo.forward(p, cfg, xs.astype(np.float64), z.astype(np.float64), x.astype(np.float64), mirror=True)
-    T0 = np.hypot(x - xs, z) / 1.5
-    assert np.abs(ref[0] / T0 - 1).max() > 0.05  # the network does something
-    e = np.abs(got[0] - ref[0]) / T0
-    print("tau err median %.2e p95 %.2e max %.2e" % _stats(e))
+    v64 = [a.astype(np.float64) for a in (xs, z, x)]
+    ref = sgo.forward(p, cfg, *v64, mirror=True)
+    Tb = sgo._background(cfg, *v64)[0]
+    osc = np.maximum(sgo._out_scale(cfg, Tb)[0], 1e-4)
+    assert np.abs((ref[0] - Tb) / osc).max() > 0.05  # the network does something
+    e = np.abs(got[0] - ref[0]) / osc
+    print("out err median %.2e p95 %.2e max %.2e" % _stats(e))
     med, p95, mx = _stats(e)
     assert med < 1e-5 and p95 < 2e-3 and mx < 2e-2
     for k in (1, 2, 3):
@@ -124,6 +133,99 @@ def test_surrogate_eval_stages_vs_oracle():
 import _cases  # noqa: E402
 
 
+def _fd_direction(T, r, sm, dz, dx):
+    """Direction of the stabilised traveltime gradient of one field T[nx][nz]
+    as the table path forms it (float64): centred differences of radius r
+    clamped to the grid and divided by the actual span
+    (src/kirchmig2d_cig.cpp:130-152, :424-435), then two passes of a box
+    average of radius sm along depth and then lateral position, windows
+    clamped to the grid (:438-492); NaN where the gradient vanishes."""
+    nx, nz = T.shape
+    gx, gz = np.zeros_like(T), np.zeros_like(T)
+    for ix in range(nx):
+        il, ir = max(0, ix - r), min(nx - 1, ix + r)
+        if ir != il:
+            gx[ix] = (T[ir] - T[il]) / ((ir - il) * dx)
+    for iz in range(nz):
+        it, ib = max(0, iz - r), min(nz - 1, iz + r)
+        if ib != it:
+            gz[:, iz] = (T[:, ib] - T[:, it]) / ((ib - it) * dz)
+
+    def box(a, axis):
+        n = a.shape[axis]
+        out = np.empty_like(a)
+        for k in range(n):
+            lo, hi = max(0, k - sm), min(n - 1, k + sm)
+            sl = [slice(None)] * 2
+            sl[axis] = slice(lo, hi + 1)
+            o = [slice(None)] * 2
+            o[axis] = k
+            out[tuple(o)] = a[tuple(sl)].mean(axis=axis)
+        return out
+    for _ in range(2 if sm > 0 else 0):
+        gx, gz = box(box(gx, 1), 0), box(box(gz, 1), 0)
+    phi = np.arctan2(gz, gx)
+    phi[np.hypot(gx, gz) <= 1e-12] = np.nan
+    return phi
+
+
+def test_surrogate_fd_angle_and_table_derivative(golden):
+    # angle="fd": the direction is the table path's finite-difference
+    # gradient of the surrogate's own traveltime field; tx="table": the
+    # antialias derivative and the aperture weight are the table path's
+    kp, geom, axis, op, _ = _cases.case_setup(golden, "base")
+    T, Dt = golden.tables()
+    nz, nx, dz = geom["nz"], geom["nx"], geom["dz"]
+    s = kd.Surrogate((0.0, 0.0, 0.0), (0.8, 0.4, 0.8), fmax=4.0, vref=1.5, zsrc=0.0, seed=9, vgrad=0.6,
+                     residual_ms=1.0)
+    p = s.get_params()
+    p[sgo.OFF_WO:sgo.OFF_BO] *= 30.0
+    s.set_params(p)
+    ref_plan = kd.Plan(kp, kd.geometry(**geom))
+    ref_plan.set_tables(T, Dt, T, Dt)
+    for tx in ("network", "table"):
+        plan = kd.Plan(kp, kd.geometry(**geom))
+        plan.set_tables(T, Dt, T, Dt)
+        plan.set_surrogate(s, s, angle="fd", tx=tx)
+        net_plan = kd.Plan(kp, kd.geometry(**geom))
+        net_plan.set_tables(T, Dt, T, Dt)
+        net_plan.set_surrogate(s, s, angle="network", tx="network")
+        for is_source, pos in ((1, 0.05), (0, 0.4133)):
+            pos = float(np.float32(pos))
+            gT, gTx, gphi, gw = (t.cpu().numpy().reshape(nx, nz) for t in kd.leg_fields_device(plan, is_source, pos))
+            nT, nTx, _, nw = (t.cpu().numpy().reshape(nx, nz) for t in kd.leg_fields_device(net_plan, is_source, pos))
+            rT, rTx, _, rw = (t.cpu().numpy().reshape(nx, nz) for t in kd.leg_fields_device(ref_plan, is_source, pos))
+            assert np.array_equal(gT, nT)  # the same traveltime whichever quantities the network supplies
+            assert np.abs(gT - rT).max() > 1e-4  # ... and not the table's
+            ref_phi = _fd_direction(gT.astype(np.float64), kp.angle_grad_radius, kp.angle_smooth, dz, dz)
+            nan = np.isnan(ref_phi)
+            assert np.array_equal(np.isnan(gphi), nan)
+            assert np.abs(np.angle(np.exp(1j * (gphi[~nan] - ref_phi[~nan])))).max() < 1e-9
+            if tx == "table":
+                assert np.array_equal(gTx, rTx) and np.array_equal(gw, rw)
+            else:
+                assert np.array_equal(gTx, nTx) and np.array_equal(gw, nw)
+        plan.close()
+        net_plan.close()
+    ref_plan.close()
+    s.close()
+
+
+def test_surrogate_training_is_reproducible():
+    # fixed-order gradient sums: two runs from the same seed give the same
+    # parameters bit for bit
+    import torch
+    vol = torch.rand((6, 40, 30), device="cuda") + 0.5  # [npos][nx][nz]
+    out = []
+    for _ in range(2):
+        s = kd.Surrogate((0.0, 0.0, 0.0), (1.0, 0.3, 0.4), fmax=3.0, vref=1.5, zsrc=0.0, seed=2, vgrad=0.6,
+                         residual_ms=1.0)
+        s.train(vol, 0.0, 0.2, 0.0, 0.01, 0.0, 0.01, 50, batch=1024, lr=1e-3, lr_final=1e-4, seed=4)
+        out.append(s.get_params())
+        s.close()
+    assert np.array_equal(out[0], out[1])
+
+
 def test_surrogate_leg_fields_match_eval(golden):
     # the persistent leg-field kernel (resident weights, per-leg xs features)
     # against the general evaluation kernel at the same points, and the
@@ -140,7 +242,7 @@ def test_surrogate_leg_fields_match_eval(golden):
     plan.set_tables(T, Dt, T, Dt)
     ref_plan = kd.Plan(kp, kd.geometry(**geom))
     ref_plan.set_tables(T, Dt, T, Dt)
-    plan.set_surrogate(s, s)
+    plan.set_surrogate(s, s, angle="network")
     zz, xx = np.meshgrid(np.arange(nz) * dz, np.arange(nx) * dz)  # [nx][nz]
     for is_source, pos in ((1, 0.05), (0, 0.4133), (1, 0.7)):
         pos = float(np.float32(pos))
