@@ -73,6 +73,8 @@ struct FieldArgs {
     int radius, smooth, angle, use_grad;
     float aper, aper_taper, rmin, rtaper;
     int cone;  // kirchmig2d: the w field holds the leg's two cone flags (see k_leg_interp)
+    int *status;  // device flag a kernel sets when a bounded wait gives up (may be null)
+    int type_p;   // the legs use the partial-shift interpolation ('p')
 };
 
 // Workspace for the gradient pipeline: 4 double planes per position.

@@ -23,6 +23,7 @@
 
 #include "kcig_aperture.h"
 #include "kcig_common.h"
+#include "kcig_tc.h"
 
 namespace kcig {
 
@@ -188,15 +189,163 @@ static int prelude_block(int nt, int *warps)
     return -1;
 }
 
+// K1 with one CTA of PW warps per trace.  The trace is staged in shared
+// memory as FP64 with coalesced loads (the mute applied on the way).  Each
+// warp owns a contiguous segment of 32-sample rows and scans it row by row
+// with a 32-wide shuffle scan, carrying the running total from row to row;
+// the segments' totals are scanned across the warps first (in a fixed order),
+// so every running sum is FP64 and every shared-memory access is one
+// consecutive row (no bank conflicts).  Causal sum, then anticausal sum
+// (kirmig.cpp:8-24), then the optional centred difference (:381-394); the
+// {D[i], D[i+1]-D[i]} pairs leave with coalesced 16-byte stores.
+__device__ __forceinline__ double warp_incl_scan(double v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_incl_suffix_scan(double v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o < 32) v += y;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+constexpr int kPreludeWarps = 4;
+
+__global__ void __launch_bounds__(32 * kPreludeWarps) k_prelude_cta(PreludeArgs a)
+{
+    constexpr int PW = kPreludeWarps, PT = 32 * PW;
+    extern __shared__ double pd[];  // [nt] (+ [nt] of the differenced trace with diff=1)
+    __shared__ double wtot[PW], woff[PW];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+    const int tr = blockIdx.x;
+    const int k = tr / a.nhc, rr = tr % a.nhc;
+    const float *x = a.data + ((size_t)(a.shot0 + k) * a.nh + (a.rcv0 + rr)) * a.nt;
+    int nt = a.nt;
+    if (a.toff) {  // ragged shots: own samples, own length (padding traces are never read)
+        const long long off = a.toff[tr];
+        if (off < 0) return;
+        x = a.data + off;
+        nt = a.tnt[tr];
+    }
+    double boundary = 0.0;
+    const bool mute = a.mute_sx != nullptr;
+    if (mute) {
+        const double off = a.slope * fabs(a.mute_rx[tr] - a.mute_sx[tr]);
+        boundary = a.invert ? a.intercept - off : a.intercept + off;
+    }
+    for (int i = tid; i < nt; i += PT) {
+        double v = (double)__ldg(x + i);
+        if (mute) {
+            const double t = a.t0 + (double)i * a.dt;
+            double w = 0.0;
+            if (t >= boundary + a.taper) w = 1.0;
+            else if (t > boundary) w = 0.5 * (1.0 - cospi((t - boundary) / a.taper));
+            v *= w;
+        }
+        pd[i] = v;
+    }
+    __syncthreads();
+    const int rows = (nt + 31) >> 5, R = (rows + PW - 1) / PW;
+    const int i0 = min(nt, warp * R * 32), i1 = min(nt, (warp + 1) * R * 32);
+
+    // causal running sum
+    double sv = 0.0;
+    for (int i = i0 + lane; i < i1; i += 32) sv += pd[i];
+    sv = warp_sum(sv);
+    if (lane == 0) wtot[warp] = sv;
+    __syncthreads();
+    if (tid == 0) {
+        double acc = 0.0;
+        for (int w = 0; w < PW; w++) {
+            woff[w] = acc;
+            acc += wtot[w];
+        }
+    }
+    __syncthreads();
+    double carry = woff[warp];
+    for (int b = i0; b < i1; b += 32) {
+        const int i = b + lane;
+        const double v = warp_incl_scan(i < i1 ? pd[i] : 0.0) + carry;
+        if (i < i1) pd[i] = v;
+        carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+    __syncthreads();
+
+    // anticausal running sum of that: D[i] = sum over j >= i
+    sv = 0.0;
+    for (int i = i0 + lane; i < i1; i += 32) sv += pd[i];
+    sv = warp_sum(sv);
+    if (lane == 0) wtot[warp] = sv;
+    __syncthreads();
+    if (tid == 0) {
+        double acc = 0.0;
+        for (int w = PW - 1; w >= 0; w--) {
+            woff[w] = acc;
+            acc += wtot[w];
+        }
+    }
+    __syncthreads();
+    carry = woff[warp];
+    if (i1 > i0) {
+        for (int b = i0 + ((i1 - 1 - i0) & ~31); b >= i0; b -= 32) {
+            const int i = b + lane;
+            const double v = warp_incl_suffix_scan(i < i1 ? pd[i] : 0.0) + carry;
+            if (i < i1) pd[i] = v;
+            carry = __shfl_sync(0xffffffffu, v, 0);
+        }
+    }
+    __syncthreads();
+
+    const double *D = pd;
+    if (a.isdiff == 1 && nt >= 2) {
+        // central first derivative, one-sided at the ends, into the second half
+        double *q = pd + nt;
+        for (int i = tid; i < nt; i += PT) {
+            double v;
+            if (i == 0) v = (pd[1] - pd[0]) / a.dt;
+            else if (i == nt - 1) v = (pd[nt - 1] - pd[nt - 2]) / a.dt;
+            else v = (pd[i + 1] - pd[i - 1]) / (2.0 * a.dt);
+            q[i] = v;
+        }
+        __syncthreads();
+        D = q;
+    }
+    double2 *out = a.D + (size_t)tr * a.nt;
+    for (int i = tid; i < nt; i += PT) {
+        double2 e;
+        e.x = D[i];
+        e.y = (i + 1 < nt) ? D[i + 1] - D[i] : 0.0;
+        out[i] = e;
+    }
+}
+
 int launch_prelude(const PreludeArgs &a, cudaStream_t st)
 {
     if (a.ntr <= 0) return KCIG_OK;
-    int warps;
-    if (prelude_block(a.nt, &warps))
-        return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (25600)", a.nt);
-    const size_t sm = (size_t)warps * a.nt * sizeof(double);
-    KCIG_TRY(set_dyn_smem((const void *)k_prelude, (int)sm));
-    k_prelude<<<(a.ntr + warps - 1) / warps, 32 * warps, sm, st>>>(a);
+    const size_t sm = (size_t)(a.isdiff == 1 ? 2 : 1) * a.nt * sizeof(double);
+    if (sm > 200 * 1024)
+        return set_error(KCIG_ERR_UNSUPPORTED, "nt=%d exceeds the on-chip trace limit (%d, %d with diff=1)", a.nt,
+                         25600, 12800);
+    KCIG_TRY(set_dyn_smem((const void *)k_prelude_cta, (int)sm));
+    k_prelude_cta<<<a.ntr, 32 * kPreludeWarps, sm, st>>>(a);
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
 }
@@ -499,6 +648,176 @@ size_t leg_grad_fused_smem(int radius, int smooth)
     return (4 * (size_t)W * W + 2 * smooth + 1 + 2 * (2 * r + 1)) * sizeof(double);
 }
 
+// K2 in one pass from the tables: interpolation along the position axis
+// (tinterpsr.cpp:37-70, :142-188), the gradient with its smoothing and
+// direction (as k_leg_grad_fused), and the aperture weight, for one
+// kGradTile x kGradTile block of image points of one leg.  The table slices
+// the block and its halo need (p0, m0 and, between two positions, p1, m1)
+// are staged in shared memory by the TMA engine: one bulk copy per column
+// and slice, completing on an mbarrier's transaction count.  A table column
+// starts at ix*nz floats, which is 16-byte aligned only when nz is a multiple
+// of 4, so a tiled tensor map cannot describe the tables in general: each
+// column segment is placed in shared memory at the same 16-byte phase as in
+// global memory, its aligned interior goes by bulk copy and its ragged ends
+// (at most three floats each) by plain loads.  The staging buffer is then
+// reused for the gradient planes.  Every interpolated traveltime stays on
+// chip; only the block's own {T, phi} and {Tx*scale, w} are written.
+constexpr int kLegTileMaxW = 96;  // widest halo tile the host launches (one byte of phase per column)
+
+__host__ __device__ inline int leg_tile_pitch(int W) { return (W + 6) & ~3; }  // >= W + 3 floats, 16-byte rows
+
+size_t leg_tile_smem(int radius, int smooth)
+{
+    const int r = radius < 1 ? 1 : radius, W = kGradTile + 2 * (r + 2 * smooth);
+    const size_t stage = (size_t)4 * W * leg_tile_pitch(W) * sizeof(float);
+    const size_t planes = (size_t)3 * W * W * sizeof(double);
+    return (size_t)W * W * sizeof(double) + std::max(stage, planes) +
+           (size_t)(2 * smooth + 1 + 2 * (2 * r + 1)) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(256, 3) k_leg_tile(FieldArgs a, LegFields out)
+{
+    extern __shared__ __align__(16) unsigned char lsm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ unsigned char phs[4][kLegTileMaxW];  // 16-byte phase (in floats) of each staged column
+    const int nz = a.nz, nx = a.nx;
+    const size_t nzx = (size_t)nz * nx;
+    const int r = a.radius < 1 ? 1 : a.radius, s = a.smooth;
+    const int H = r + 2 * s, W = kGradTile + 2 * H, SW = leg_tile_pitch(W);
+    const int tiles_z = (nz + kGradTile - 1) / kGradTile;
+    const int gz0 = (int)(blockIdx.x % tiles_z) * kGradTile - H, gx0 = (int)(blockIdx.x / tiles_z) * kGradTile - H;
+    const int zlo = max(0, -gz0), zhi = min(W, nz - gz0), xlo = max(0, -gx0), xhi = min(W, nx - gx0);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+    const LegInterp &L = a.legs[blockIdx.y];
+    const int i0 = L.i0, i1 = L.i1;
+    const bool two = i1 >= 0;  // between two positions: p0, m0, p1, m1; else p0, m0
+    const int nsl = two ? 4 : 2;
+    double *P0 = reinterpret_cast<double *>(lsm);
+    unsigned char *regB = lsm + (size_t)W * W * sizeof(double);
+    float *stage = reinterpret_cast<float *>(regB);
+    double *P1 = reinterpret_cast<double *>(regB), *P2 = P1 + W * W, *P3 = P2 + W * W;
+    const size_t stage_bytes = (size_t)4 * W * SW * sizeof(float), plane_bytes = (size_t)3 * W * W * sizeof(double);
+    const size_t regB_bytes = stage_bytes > plane_bytes ? stage_bytes : plane_bytes;
+    double *rcpb = reinterpret_cast<double *>(regB + regB_bytes), *rcpx = rcpb + 2 * s + 1, *rcpz = rcpx + 2 * r + 1;
+
+    // ---- stage the slices' columns of the block and its halo
+    if (tid == 0) tc::mbar_init(&bar, 1);
+    __syncthreads();
+    const int ncol = xhi - xlo, nseg = zhi - zlo;
+    for (int j = tid; j < nsl * ncol; j += nthr) {
+        const int q = j / ncol, lx = xlo + j % ncol;
+        const float *base = (q & 1) ? a.der : a.tab;
+        const float *gp = base + (size_t)(q < 2 ? i0 : i1) * nzx + (size_t)(gx0 + lx) * nz + (gz0 + zlo);
+        const uintptr_t ad = reinterpret_cast<uintptr_t>(gp);
+        const bool aligned4 = (ad & 3) == 0;
+        const int ph = aligned4 ? (int)((ad >> 2) & 3) : 0;
+        const int head = aligned4 ? min(nseg, (4 - ph) & 3) : nseg;
+        const int nb = ((nseg - head) >> 2) << 2;
+        float *dp = stage + (size_t)(q * W + lx) * SW + ph;  // segment element k at dp[k]
+        phs[q][lx] = (unsigned char)ph;
+        for (int k = 0; k < head; k++) dp[k] = __ldg(gp + k);
+        for (int k = head + nb; k < nseg; k++) dp[k] = __ldg(gp + k);
+        if (nb > 0) {
+            tc::mbar_expect_tx(&bar, (uint32_t)nb * 4u);
+            tc::bulk_g2s(dp + head, gp + head, (uint32_t)nb * 4u, &bar);
+        }
+    }
+    for (int k = tid; k <= 2 * s; k += nthr) rcpb[k] = 1.0 / (double)(k + 1);
+    for (int k = tid; k <= 2 * r; k += nthr) {
+        rcpx[k] = k ? 1.0 / ((double)k * a.dx) : 0.0;
+        rcpz[k] = k ? 1.0 / ((double)k * a.dz) : 0.0;
+    }
+    __syncthreads();  // every transfer announced before the arrival
+    if (tid == 0) tc::mbar_arrive(&bar);
+    // bounded wait; a block whose copies did not land raises the flag, waits
+    // once more (bounded) for them and leaves
+    if (!__syncthreads_and(tc::mbar_wait(&bar, 0))) {
+        if (tid == 0 && a.status) atomicExch(a.status, 1);
+        tc::mbar_wait(&bar, 0);
+        return;
+    }
+
+    // ---- interpolated traveltime (FP64) on the block and its halo; the
+    // block's own points also get T, Tx and the aperture weight written
+    double2 *TPo = out.TP + (size_t)blockIdx.y * nzx;
+    const double hc0 = L.c[0], hc1 = L.c[1], hc2 = L.c[2], hc3 = L.c[3];
+    for (int lx = xlo + (int)threadIdx.y; lx < xhi; lx += blockDim.y) {
+        const float *c0 = stage + (size_t)(0 * W + lx) * SW + phs[0][lx] - zlo;
+        const float *c1 = stage + (size_t)(1 * W + lx) * SW + phs[1][lx] - zlo;
+        const float *c2 = two ? stage + (size_t)(2 * W + lx) * SW + phs[2][lx] - zlo : c0;
+        const float *c3 = two ? stage + (size_t)(3 * W + lx) * SW + phs[3][lx] - zlo : c1;
+        const bool xin = lx >= H && lx < H + kGradTile;
+        for (int lz = zlo + (int)threadIdx.x; lz < zhi; lz += blockDim.x) {
+            double T, Tx = 0.0;
+            if (!two) {
+                T = c0[lz];
+                Tx = c1[lz];
+            } else {
+                const double p0 = c0[lz], p1 = c2[lz];
+                const double m0 = c1[lz], m1 = c3[lz];
+                T = hc0 * p0 + hc1 * m0 + hc2 * p1 + hc3 * m1;
+            }
+            P0[lx * W + lz] = T;
+            if (xin && lz >= H && lz < H + kGradTile) {
+                if (two) {
+                    const double p0 = c0[lz], p1 = c2[lz];
+                    const double m0 = c1[lz], m1 = c3[lz];
+                    Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
+                }
+                const int iz = gz0 + lz, ix = gx0 + lx;
+                const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin,
+                                                     a.rtaper);
+                TPo[(size_t)ix * nz + iz].x = T;
+                out.XW[(size_t)blockIdx.y * nzx + (size_t)ix * nz + iz] = make_float2((float)Tx * L.scale, (float)w);
+            }
+        }
+    }
+    __syncthreads();  // the staging buffer is free: it becomes P1..P3
+
+    // ---- centred differences on [r, W-r)^2: gx -> P1, gz -> P2
+    const bool dox = nx > 1 && a.dx != 0.0f, doz = nz > 1 && a.dz != 0.0f;
+    for (int lx = max(r, xlo) + (int)threadIdx.y; lx < min(W - r, xhi); lx += blockDim.y)
+        for (int lz = max(r, zlo) + (int)threadIdx.x; lz < min(W - r, zhi); lz += blockDim.x) {
+            double vx = 0.0, vz = 0.0;
+            if (dox) {
+                const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
+                if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
+            }
+            if (doz) {
+                const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
+                if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
+            }
+            P1[lx * W + lz] = vx;
+            P2[lx * W + lz] = vz;
+        }
+    __syncthreads();
+    // ---- the four box passes (z, x, z, x; both components per pass), P0 and
+    // P3 as scratch (the block's traveltimes are already written)
+    if (s > 0) {
+        const int i1 = r + s, i2 = H;
+        box_tile<0>(P1, P0, P2, P3, W, s, max(i1, zlo), min(W - i1, zhi), max(r, xlo), min(W - r, xhi), zlo, zhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<1>(P0, P1, P3, P2, W, s, max(i1, zlo), min(W - i1, zhi), max(i1, xlo), min(W - i1, xhi), xlo, xhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<0>(P1, P0, P2, P3, W, s, max(i2, zlo), min(W - i2, zhi), max(i1, xlo), min(W - i1, xhi), zlo, zhi,
+                    rcpb);
+        __syncthreads();
+        box_tile<1>(P0, P1, P3, P2, W, s, max(i2, zlo), min(W - i2, zhi), max(i2, xlo), min(W - i2, xhi), xlo, xhi,
+                    rcpb);
+        __syncthreads();
+    }
+    // scattering_angle_deg_from_grad (:171-187) returns NaN for a vanishing gradient
+    for (int lx = max(H, xlo) + (int)threadIdx.y; lx < min(W - H, xhi); lx += blockDim.y)
+        for (int lz = max(H, zlo) + (int)threadIdx.x; lz < min(W - H, zhi); lz += blockDim.x) {
+            const double vx = P1[lx * W + lz], vz = P2[lx * W + lz];
+            const double phi = (sqrt(vx * vx + vz * vz) <= 1.0e-12) ? __longlong_as_double(0x7ff8000000000000ll)
+                                                                     : atan2(vz, vx);
+            TPo[(size_t)(gx0 + lx) * nz + (gz0 + lz)].y = phi;
+        }
+}
+
 int launch_leg_interp(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
 {
     if (a.n <= 0) return KCIG_OK;
@@ -556,9 +875,29 @@ bool leg_grad_needs_work(const FieldArgs &a)
     return a.angle && (a.use_grad || leg_grad_fused_smem(a.radius, a.smooth) > 200 * 1024);
 }
 
+// The one-pass kernel covers the default interpolations (Hermite and linear
+// between two positions, or a clamped end) with the angle on and no gradient
+// volumes; the partial-shift interpolation, gradient volumes, the kirchmig2d
+// cone flags and halos wider than its shared memory take the two-stage path.
+static bool leg_tile_applies(const FieldArgs &a)
+{
+    if (!a.angle || a.use_grad || a.cone || a.type_p) return false;
+    const int r = a.radius < 1 ? 1 : a.radius, W = kGradTile + 2 * (r + 2 * a.smooth);
+    return W <= kLegTileMaxW && leg_tile_smem(a.radius, a.smooth) <= 200 * 1024;
+}
+
 int launch_leg_fields(const FieldArgs &a, LegFields out, double *work, cudaStream_t st, int *launches)
 {
     int nl = 0;
+    if (a.n > 0 && leg_tile_applies(a)) {
+        const size_t sm = leg_tile_smem(a.radius, a.smooth);
+        KCIG_TRY(set_dyn_smem((const void *)k_leg_tile, (int)sm));
+        const int tiles = ((a.nz + kGradTile - 1) / kGradTile) * ((a.nx + kGradTile - 1) / kGradTile);
+        k_leg_tile<<<dim3(tiles, a.n), dim3(32, 8), sm, st>>>(a, out);
+        KCIG_CUDA(cudaGetLastError());
+        if (launches) *launches = 1;
+        return KCIG_OK;
+    }
     const int rc = launch_leg_interp(a, out, work, st, &nl);
     if (rc == KCIG_OK && a.angle) {
         const int rc2 = launch_leg_grad(a, out, work, st, &nl);
@@ -667,10 +1006,11 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
     const bool aal_pos = a.aal >= 0.0f;
     const float aal_abs = fabsf(a.aal), aal_sgn = aal_pos ? 1.0f : -1.0f;
 
+    // receiver streams: one shared by a block's KB shots (cmp=0), or one per
+    // shot (receivers not shared), so that KB independent (shot, receiver)
+    // gather chains are in flight per thread either way
+    constexpr int KR = SHARED_R ? 1 : KB;
     for (int sb = s_lo; sb < s_hi; sb += KB) {
-        // last usable sample of this shot's traces: ragged shots (receivers
-        // never shared, one shot per block) carry their own
-        const double topk = (!SHARED_R && a.stop) ? (double)__ldg(a.stop + sb) : top;
         double2 sTP[KB];
         float2 sXW[KB];
 #pragma unroll
@@ -687,41 +1027,62 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 sXW[k] = make_float2(0.f, 0.f);
             }
         }
-        // receivers of this block: all nh, or (ragged shots, one shot per
-        // block) the shot's own count; their fields are loaded one receiver
-        // ahead of use (through the trace's field index when not shared)
-        const int nr = (!SHARED_R && a.snh) ? __ldg(a.snh + sb) : a.nh;
-        double2 nTP = make_double2(0.0, 0.0);
-        float2 nXW = make_float2(0.f, 0.f);
-        // unshared receivers: field index of the receiver after next, so the
-        // index load does not stand in front of the field load
-        const int *rfi_s = a.rfi + (size_t)sb * a.nh;
-        int fnext = 0;
-        if (nr > 0) {
-            const size_t f0 = SHARED_R ? 0 : (size_t)__ldg(rfi_s);
-            nTP = __ldg(a.RTP + f0 * nzx + i);
-            nXW = __ldg(a.RXW + f0 * nzx + i);
-            if (!SHARED_R && nr > 1) fnext = __ldg(rfi_s + 1);
+        // per stream: the last usable sample of its traces and its receiver
+        // count (ragged shots carry their own), and its fields loaded one
+        // receiver ahead of use (through the trace's field index when not
+        // shared, with the index of the receiver after next loaded too, so
+        // the index load does not stand in front of the field load)
+        double topk[KR];
+        int nrk[KR], fnext[KR];
+        double2 nTP[KR];
+        float2 nXW[KR];
+        int nr = 0;
+#pragma unroll
+        for (int j = 0; j < KR; j++) {
+            const bool live = SHARED_R || sb + j < s_hi;
+            topk[j] = (!SHARED_R && a.stop && live) ? (double)__ldg(a.stop + sb + j) : top;
+            nrk[j] = !live ? 0 : ((!SHARED_R && a.snh) ? __ldg(a.snh + sb + j) : a.nh);
+            nr = max(nr, nrk[j]);
+            fnext[j] = 0;
+            nTP[j] = make_double2(0.0, 0.0);
+            nXW[j] = make_float2(0.f, 0.f);
+            if (nrk[j] > 0) {
+                const int *rfi_j = a.rfi + (size_t)(sb + j) * a.nh;
+                const size_t f0 = SHARED_R ? 0 : (size_t)__ldg(rfi_j);
+                nTP[j] = __ldg(a.RTP + f0 * nzx + i);
+                nXW[j] = __ldg(a.RXW + f0 * nzx + i);
+                if (!SHARED_R && nrk[j] > 1) fnext[j] = __ldg(rfi_j + 1);
+            }
         }
         for (int r = 0; r < nr; r++) {
-            double2 rTP = nTP;
-            float2 rXW = nXW;
-            // the receiver's share, once per receiver for the KB shots
-            rTP.x *= a.inv_dt;
-            rXW.x = fabsf(rXW.x) * aal_abs * inv_dt_f;
-            if (r + 1 < nr) {  // next receiver, one ahead of use
-                const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)fnext;
-                nTP = __ldg(a.RTP + f1 * nzx + i);
-                nXW = __ldg(a.RXW + f1 * nzx + i);
-                if (!SHARED_R && r + 2 < nr) fnext = __ldg(rfi_s + r + 2);
+            double2 rTP[KR];
+            float2 rXW[KR];
+#pragma unroll
+            for (int j = 0; j < KR; j++) {
+                rTP[j] = nTP[j];
+                rXW[j] = nXW[j];
+                // the receiver's share, once per receiver for the stream's shots
+                rTP[j].x *= a.inv_dt;
+                rXW[j].x = fabsf(rXW[j].x) * aal_abs * inv_dt_f;
+                if (r + 1 < nrk[j]) {  // next receiver, one ahead of use
+                    const size_t f1 = SHARED_R ? (size_t)(r + 1) : (size_t)fnext[j];
+                    nTP[j] = __ldg(a.RTP + f1 * nzx + i);
+                    nXW[j] = __ldg(a.RXW + f1 * nzx + i);
+                    if (!SHARED_R && r + 2 < nrk[j]) fnext[j] = __ldg(a.rfi + (size_t)(sb + j) * a.nh + r + 2);
+                }
             }
 #pragma unroll
             for (int k = 0; k < KB; k++) {
                 if (sb + k >= s_hi) break;
+                const int j = SHARED_R ? 0 : k;  // this shot's receiver stream
+                if (!SHARED_R && r >= nrk[j]) continue;
+                const double2 rTPk = rTP[j];
+                const float2 rXWk = rXW[j];
+                const double topj = topk[j];
                 const int trc = (sb + k) * a.nh + r;
                 const float tw = a.unit_tw ? 1.0f : __ldg(a.trw + trc);
                 if (tw == 0.0f) continue;  // trace removed by aperture_trace / offset bin
-                const float apw = sXW[k].y * rXW.y;
+                const float apw = sXW[k].y * rXWk.y;
                 if (!(apw > 0.0f)) continue;
                 int b0 = 0;
                 float w0 = 1.0f, w1 = 0.0f, aw;
@@ -729,7 +1090,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                     // kirchmig2d (:455-488): the trace weight's sign says
                     // whether the source is the left leg; each leg's w holds
                     // its cone flags (1: left side inside, 2: right side inside)
-                    const int sw = (int)sXW[k].y, rw = (int)rXW.y;
+                    const int sw = (int)sXW[k].y, rw = (int)rXWk.y;
                     const bool keep = tw > 0.0f ? ((sw & 1) && (rw & 2)) : ((rw & 1) && (sw & 2));
                     if (!keep) continue;
                     b0 = __ldg(a.igo + trc) - gc0;
@@ -742,7 +1103,7 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 } else {
                     // opening angle (:171-187): atan2(|s x r|, s.r) is the
                     // difference of the gradient directions folded to [0, pi]
-                    double th = fabs(sTP[k].y - rTP.y);
+                    double th = fabs(sTP[k].y - rTPk.y);
                     th = (th > kPiD) ? kTwoPi - th : th;
                     const double u = fma(th, uk, -ub);  // bin coordinate; NaN: vanishing gradient
                     double fl = 0.0;
@@ -782,8 +1143,8 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 // as 1 + sign(aal) * (max of the shares scaled by |aal| / dt):
                 // the scale is >= 0 and rounding is monotone, and negation is
                 // exact; in FP32: it only sets the window
-                const double ft0 = sTP[k].x + rTP.x;
-                const float shf = fmaf(aal_sgn, fmaxf(sXW[k].x, rXW.x), 1.0f);
+                const double ft0 = sTP[k].x + rTPk.x;
+                const float shf = fmaf(aal_sgn, fmaxf(sXW[k].x, rXWk.x), 1.0f);
                 const double sh = (double)shf;
                 const double ftm0 = ft0 - sh, ftp0 = ft0 + sh;
                 // the reference's six tests on the three floors (0 <= flm <=
@@ -791,10 +1152,10 @@ __global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum
                 // NaN, so fl0 lies between the other two and the tests reduce
                 // to ftm0 >= 0 and ftp0 < top (top is an integer; NaN fails)
                 if (aal_pos) {
-                    if (!(ftm0 >= 0.0 && ftp0 < topk)) continue;
+                    if (!(ftm0 >= 0.0 && ftp0 < topj)) continue;
                 } else {
                     const double fl0 = floor(ft0), flm = floor(ftm0), flp = floor(ftp0);
-                    if (!(fl0 >= 0.0 && fl0 < topk && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topk)) continue;
+                    if (!(fl0 >= 0.0 && fl0 < topj && flm >= 0.0 && flm <= fl0 && flp >= fl0 && flp < topj)) continue;
                 }
                 // all three positions are now in [0, nt - 1): floors by the
                 // shifted add, the sample indices from its low word
@@ -966,6 +1327,12 @@ static int launch_sum_t(const SumArgs &a, int nb, cudaStream_t st)
     return KCIG_OK;
 }
 
+// Shots per block when receivers are not shared (each shot its own receiver
+// stream): the independent gather chains a thread keeps in flight.
+#ifndef KCIG_KB_UNSHARED
+#define KCIG_KB_UNSHARED 2
+#endif
+
 template <int TZ, int TX, int KB>
 static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
 {
@@ -975,10 +1342,10 @@ static int launch_sum_mode(const SumArgs &a, int nb, cudaStream_t st)
         if (a.mode == 3) return launch_sum_t<TZ, TX, KB, true, 3>(a, nb, st);
         return launch_sum_t<TZ, TX, KB, true, 2>(a, nb, st);
     }
-    if (a.mode == 0) return launch_sum_t<TZ, TX, 1, false, 0>(a, nb, st);
-    if (a.mode == 1) return launch_sum_t<TZ, TX, 1, false, 1>(a, nb, st);
-    if (a.mode == 3) return launch_sum_t<TZ, TX, 1, false, 3>(a, nb, st);
-    return launch_sum_t<TZ, TX, 1, false, 2>(a, nb, st);
+    if (a.mode == 0) return launch_sum_t<TZ, TX, KCIG_KB_UNSHARED, false, 0>(a, nb, st);
+    if (a.mode == 1) return launch_sum_t<TZ, TX, KCIG_KB_UNSHARED, false, 1>(a, nb, st);
+    if (a.mode == 3) return launch_sum_t<TZ, TX, KCIG_KB_UNSHARED, false, 3>(a, nb, st);
+    return launch_sum_t<TZ, TX, KCIG_KB_UNSHARED, false, 2>(a, nb, st);
 }
 
 // Shots per block of the receiver-shared path (register-resident source
@@ -1036,7 +1403,7 @@ int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
     const long long tiles = (long long)((nz + 15) / 16) * ((nx + 7) / 8);
     const long long want = 2LL * sms * KCIG_SUM_MINB;  // two waves of resident CTAs
     if (tiles >= want) return 1;
-    const int blocks = shared_r ? (nsb + KCIG_KB - 1) / KCIG_KB : nsb;
+    const int blocks = shared_r ? (nsb + KCIG_KB - 1) / KCIG_KB : (nsb + KCIG_KB_UNSHARED - 1) / KCIG_KB_UNSHARED;
     long long ns = (want + tiles - 1) / tiles;
     ns = std::min<long long>(ns, std::min(blocks, 64));
     return (int)std::max<long long>(1, ns);

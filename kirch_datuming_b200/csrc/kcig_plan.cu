@@ -59,6 +59,7 @@ struct kcig_plan {
     DevBuf own_stab, own_sder, own_rtab, own_rder, own_sgx, own_sgz, own_rgx, own_rgz;
     DevBuf d_data, d_image, d_rT, d_rF, d_sT, d_sF, d_work, d_D, d_legs, d_tr;
     DevBuf d_part;  // partial images of a split summation (small grids)
+    DevBuf d_status;  // flag of the leg-field kernels' bounded waits (k_leg_tile)
     // tables left in host memory (KCIG_MEM_HOST_STREAM): the slices of each
     // leg batch are copied into d_stage
     int stream_tables = 0;
@@ -218,6 +219,25 @@ int field_batch(const kcig_plan *P, size_t nlegs)
     return std::max(1, std::min<int>((int)nlegs, (int)std::min<size_t>(64, (256ull << 20) / (nzx * 32) + 1)));
 }
 
+// The leg-field kernels' status flag: cleared before a migration's launches,
+// read after them (KCIG_ERR_DEVICE when a bounded wait gave up).
+int plan_status_reset(kcig_plan *P, cudaStream_t st)
+{
+    KCIG_TRY(P->d_status.ensure(sizeof(int)));
+    KCIG_CUDA(cudaMemsetAsync(P->d_status.p, 0, sizeof(int), st));
+    return KCIG_OK;
+}
+
+int plan_status_check(kcig_plan *P, cudaStream_t st)
+{
+    if (!P->d_status.p) return KCIG_OK;
+    int h = 0;
+    KCIG_CUDA(cudaMemcpyAsync(&h, P->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KCIG_CUDA(cudaStreamSynchronize(st));
+    if (h) return set_error(KCIG_ERR_DEVICE, "leg fields: a staged table copy did not complete");
+    return KCIG_OK;
+}
+
 // Leg fields of n legs whose LegInterp records are already on the device;
 // tab/der (device) replace the plan's tables when given (staged slices).
 int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int n, double2 *TP, float2 *XW,
@@ -249,6 +269,8 @@ int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int
         a.aper_taper = P->p.aperture_taper;
         a.rmin = P->p.aperture_rmin;
         a.rtaper = P->p.aperture_rtaper;
+        a.status = P->d_status.as<int>();
+        a.type_p = P->p.interp_type == 'p';
         if (tx_table) {
             if (!a.tab || !a.der || P->stream_tables)
                 return set_error(KCIG_ERR_ARG, "surrogate with table derivatives: the plan needs device tables");
@@ -301,6 +323,8 @@ int compute_fields_dev(kcig_plan *P, int is_source, const LegInterp *d_legs, int
         a.rmin = P->p.aperture_rmin;
         a.rtaper = P->p.aperture_rtaper;
         a.cone = P->p.tool == 1;
+        a.status = P->d_status.as<int>();
+        a.type_p = P->p.interp_type == 'p';
         LegFields out{TP + (size_t)j0 * nzx, XW + (size_t)j0 * nzx};
         int nl = 0;
         KCIG_TRY(launch_leg_fields(a, out, P->d_work.as<double>(), P->st, &nl));
@@ -522,6 +546,7 @@ extern "C" int kcig_leg_fields_device(kcig_plan *P, int is_source, double pos, d
     if (!rc) rc = xw.ensure(nzx * sizeof(float2));
     kcig_surrogate *sgt = is_source ? P->sg_src : P->sg_rcv;
     if (!rc && sgt) rc = sg_reset_status(sgt, P->st);
+    if (!rc) rc = plan_status_reset(P, P->st);
     if (!rc) rc = compute_fields(P, is_source, legs, tp.as<double2>(), xw.as<float2>());
     if (!rc && sgt) rc = sg_check_status(sgt, P->st);
     // unpack {T, phi} and {Tx, w} into the caller's planes
@@ -538,6 +563,7 @@ extern "C" int kcig_leg_fields_device(kcig_plan *P, int is_source, double pos, d
     }
     cudaError_t e = cudaStreamSynchronize(P->st);
     if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(leg fields)");
+    if (!rc) rc = plan_status_check(P, P->st);
     tp.release();
     xw.release();
     return rc;
@@ -564,11 +590,12 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     P->all_launches = 0;
     P->sum_ms = 0.f;
     cudaStream_t st = P->st;
+    KCIG_TRY(plan_status_reset(P, st));
 
     // data and image on the device
     const float *d_data = data;
     float *d_img = image;
-    const int ns = P->shot_count > 0 ? P->shot_count : ns;  // shots of this call (kcig_plan_set_shot_range)
+    const int ns = P->shot_count > 0 ? P->shot_count : g.ns;  // shots of this call (kcig_plan_set_shot_range)
     const size_t data_bytes = (size_t)ns * g.nh * g.nt * sizeof(float);
     if (memory == KCIG_MEM_HOST) {
         KCIG_TRY(upload(P->d_data, data, data_bytes, st));
@@ -873,6 +900,7 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     }
     for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
         if (s && rc == KCIG_OK) rc = sg_check_status(s, st);
+    if (rc == KCIG_OK) rc = plan_status_check(P, st);
     return rc;
 }
 
@@ -956,6 +984,7 @@ extern "C" int kcig_model(kcig_plan *P, const float *image, float *data, int mem
     cudaStream_t st = P->st;
     P->sum_launches = 0;
     P->all_launches = 0;
+    KCIG_TRY(plan_status_reset(P, st));
     const float *d_img = image;
     float *d_dat = data;
     const size_t img_bytes = (size_t)P->ng * nzx * sizeof(float);
@@ -1100,6 +1129,7 @@ extern "C" int kcig_model(kcig_plan *P, const float *image, float *data, int mem
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(model)");
+    if (!rc) rc = plan_status_check(P, st);
     return rc;
 }
 
@@ -1500,6 +1530,7 @@ extern "C" int kcig_migrate_prepared(kcig_plan *P, float *image, int memory)
     P->fields_ms = 0.f;
     for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
         if (s) KCIG_TRY(sg_reset_status(s, P->st));
+    KCIG_TRY(plan_status_reset(P, P->st));
     float *d_img = image;
     if (memory == KCIG_MEM_HOST) {
         KCIG_TRY(P->d_image.ensure(img_bytes));
@@ -1581,6 +1612,7 @@ extern "C" int kcig_migrate_prepared(kcig_plan *P, float *image, int memory)
     if (!rc && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(prepared)");
     for (kcig_surrogate *s : {P->sg_src, P->sg_rcv})
         if (s && rc == KCIG_OK) rc = sg_check_status(s, st);
+    if (rc == KCIG_OK) rc = plan_status_check(P, st);
     return rc;
 }
 
@@ -1712,7 +1744,7 @@ extern "C" long long kcig_shots_pairs(const kcig_plan *P)
 #define KCIG_NOALLOC_SCRATCH_BYTES (16u << 20)
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[KCIG_NOALLOC_SCRATCH_BYTES];
-static_assert(sizeof(LegInterp) <= 256, "descriptor slot");
+static_assert(sizeof(LegInterp) <= 248, "descriptor slot (the last 8 bytes hold the status flag)");
 static_assert(256 + (size_t)KCIG_NOALLOC_MAX_POINTS * 56 <= KCIG_NOALLOC_SCRATCH_BYTES, "scratch layout");
 
 namespace {
@@ -1758,6 +1790,7 @@ extern "C" int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry
     // scratch layout: [descriptor | {T,phi} | {Tx,w} | 4 gradient planes]
     char *s = (char *)base;
     LegInterp *d_leg = (LegInterp *)s;
+    int *d_status = (int *)(s + 248);  // the kernels' wait flag, in the descriptor slot's tail
     double2 *d_tp = (double2 *)(s + 256);
     float2 *d_xw = (float2 *)((char *)d_tp + (size_t)nzx * sizeof(double2));
     double *d_work = (double *)((char *)d_xw + (size_t)nzx * sizeof(float2));
@@ -1790,6 +1823,9 @@ extern "C" int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry
     a.rmin = p->aperture_rmin;
     a.rtaper = p->aperture_rtaper;
     a.cone = p->tool == 1;
+    a.status = d_status;
+    a.type_p = p->interp_type == 'p';
+    KCIG_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     KCIG_TRY(launch_leg_fields(a, LegFields{d_tp, d_xw}, d_work, st));
     struct Cp { void *dst; const char *src; size_t el, pitch; } cps[4] = {
         {T, (const char *)d_tp, sizeof(double), sizeof(double2)},
@@ -1800,6 +1836,9 @@ extern "C" int kcig_leg_fields_noalloc(const kcig_params *p, const kcig_geometry
         if (!c.dst) continue;
         KCIG_CUDA(cudaMemcpy2DAsync(c.dst, c.el, c.src, c.pitch, c.el, (size_t)nzx, cudaMemcpyDeviceToDevice, st));
     }
+    int flag = 0;
+    KCIG_CUDA(cudaMemcpyAsync(&flag, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     KCIG_CUDA(cudaStreamSynchronize(st));
+    if (flag) return set_error(KCIG_ERR_DEVICE, "kcig_leg_fields_noalloc: a staged table copy did not complete");
     return KCIG_OK;
 }

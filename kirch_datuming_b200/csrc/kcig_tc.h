@@ -120,6 +120,33 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
     return done != 0;
 }
 
+// Adds `bytes` to the transaction count the current phase of `bar` waits for
+// (no arrival): each thread that issues a bulk copy announces its bytes
+// before issuing it, then one thread arrives once all have announced.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Bulk asynchronous copy (the TMA engine, untiled form) of `bytes` from
+// global memory to this CTA's shared memory, completing on `bar`'s
+// transaction count.  Both addresses 16-byte aligned, bytes a multiple of
+// 16.  No cluster multicast: the source is this GPU's own memory.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
 // one lane of a converged warp (elect.sync): the issuer of MMAs and commits
 __device__ __forceinline__ bool elect_one()
 {
