@@ -390,7 +390,12 @@ def large_grid_sample_section():
     the 800 receiver positions (the full 1000 x 800 survey needs 4001 positions,
     154 GB of host tables; this sample needs 31 GB).  Tables from kcig_eikods
     on the device, copied to pinned host memory, freed on the device; then
-    one untimed and one timed migration through the C ABI with host data."""
+    one untimed and one timed migration through the C ABI with host data.
+    Beside it the surrogate path on the same sample: a network trained on the
+    sample's own tables (on the device, before they leave it) supplies every
+    leg's traveltime and source-position derivative (angle from the
+    finite-difference gradient of its traveltime), with no table read; its
+    image is compared with the streamed-table image."""
     import psutil
     import torch
     import kirch_datuming_b200 as kd
@@ -414,6 +419,24 @@ def large_grid_sample_section():
     t_tables = time.perf_counter() - t0
     T, D = r["time"], r["tds1"]
     del r["tdl1"]
+    # the surrogate: background gradient fitted to the model's mean velocity
+    # profile (v = 1.5 + g z), trained on the sample's tables
+    zs = np.arange(BIG_NZ) * dz
+    vbar = v.mean(axis=0).astype(np.float64)
+    vgrad = float(np.sum((vbar - 1.5) * zs) / np.sum(zs * zs))
+    sg_cfg = dict(lo=(float(pos[0]), 0.0, 0.0), hi=(float(pos[-1]) + dz, (BIG_NZ - 1) * dz, (BIG_NX - 1) * dz),
+                  fmax=6.0, vref=1.5, zsrc=0.0, vgrad=vgrad, residual_ms=20.0)
+    net = kd.Surrogate(seed=1, **sg_cfg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = net.train(T, float(pos[0]), dz, 0.0, dz, 0.0, dz, 40000, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    ip, iz, ix = rng.integers(0, BIG_NPOS, 200000), rng.integers(0, BIG_NZ, 200000), rng.integers(0, BIG_NX, 200000)
+    Tt = T[torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), torch.from_numpy(iz).cuda()].cpu().numpy()
+    Tg = net.eval(pos[ip], (iz * dz).astype(np.float32), (ix * dz).astype(np.float32))[0].cpu().numpy()
+    tt_err = 1000.0 * np.abs(Tg - Tt)
     ds_km = 1.0  # shots every 100 receivers
     g = synth.Geometry(nz=BIG_NZ, nx=BIG_NX, dz=dz, dx=dz, z0=0, x0=0, ns=BIG_NS, s0=float(pos[0]), ds=ds_km,
                        nh=BIG_NPOS, h0=float(pos[0]), dh=dz, cmp=0, nt=BIG_NT, dt=0.001, t0=0.0, npos=BIG_NPOS,
@@ -446,6 +469,20 @@ def large_grid_sample_section():
         ts.append(time.perf_counter() - t0)
     free1, _ = torch.cuda.mem_get_info()
     plan.close()
+    img_table = himg.clone()
+    splan = kd.Plan(kp, kd.geometry(**geom))
+    splan.set_surrogate(net, net, angle="fd", tx="network")
+    sts = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        splan.migrate(hdata, himg)
+        sts.append(time.perf_counter() - t0)
+    sfields = splan.timing()["fields_ms"]
+    splan.close()
+    net.close()
+    a_, b_ = himg.double(), img_table.double()
+    sg_rel = float((a_ - b_).norm() / b_.norm())
     pairs = BIG_NS * BIG_NPOS * nzx
     out = {"workload": "1201x4001@10m grid (five-layer salt), nt=4001 dt=1ms, 91 angle bins; sample of "
                        "8 shots x 800 receivers (cmp=0, 10 m); tables at the 800 receiver positions in pinned "
@@ -453,14 +490,30 @@ def large_grid_sample_section():
            "value": pairs / ts[-1] / 1e9, "unit": "Gpairs/s", "pairs": pairs, "seconds": ts[-1],
            "host_tables_gb": host_bytes / 1e9, "tables_seconds": t_tables,
            "device_used_gb_during_migration": (total - free1) / 1e9,
-           "image_finite": bool(torch.isfinite(himg).all().item()),
-           "image_rms": float(himg.double().pow(2).mean().sqrt().item())}
-    del hT, hD, hdata, himg
+           "image_finite": bool(torch.isfinite(img_table).all().item()),
+           "image_rms": float(img_table.double().pow(2).mean().sqrt().item()),
+           "surrogate": {"value": pairs / sts[-1] / 1e9, "unit": "Gpairs/s", "seconds": sts[-1],
+                         "fields_ms": sfields, "host_tables_gb": 0.0,
+                         "relL2_vs_streamed_table_image": sg_rel,
+                         "config": {k: list(v_) if isinstance(v_, tuple) else v_ for k, v_ in sg_cfg.items()},
+                         "training": {"steps": 40000, "batch": 16384, "seconds": t_train,
+                                      "final_loss_ms2": float(np.mean(losses[-50:])),
+                                      "traveltime_err_ms": {"rms": float(np.sqrt(np.mean(tt_err ** 2))),
+                                                            "p99": float(np.percentile(tt_err, 99)),
+                                                            "max": float(tt_err.max())}}}}
+    del hT, hD, hdata, himg, img_table
     return out
 
 
 # ------------------------------------------------------- surrogate section ---
-SG_FLOPS_EVAL = 2 * 128 * (256 + 3 * 128 + 3 * 128 + 256)  # tensor FLOPs per (leg, point) in k_sg_fields
+# tensor FLOPs per (leg, point) of k_sg_fields by what the network supplies
+# (the xs features folded into a per-leg bias): the traveltime only (layer 1
+# on the z and x features, layers 2-4), plus its source-position derivative
+# (the backward pass through layers 4-2), plus the depth and lateral input
+# gradient for the angle (the backward pass through layer 1)
+SG_FLOPS = {"t": 2 * 128 * (256 + 3 * 128), "tx": 2 * 128 * (256 + 3 * 128 + 3 * 128),
+            "all": 2 * 128 * (256 + 3 * 128 + 3 * 128 + 256)}
+SG_CONFIG = dict(lo=(0.0, 0.0, 0.0), hi=(4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, vgrad=0.6, residual_ms=1.0)
 SG_WORKLOAD = ("v(z)=1.5+0.6z 201x401@10m, 64 shots x 201 receivers (cmp=0, 10 m), nt=1001 dt=2ms, 61 angle bins, "
                "3 flat reflectors, 20 Hz; network trained on the 401-position GPU eikonal tables")
 
@@ -551,29 +604,44 @@ def stitch_section(steps: int, warmup: int, threads: int):
     return res
 
 
-def surrogate_section(train_steps: int, steps: int, warmup: int):
-    """Table path vs learned-surrogate path on the same v(z) 201x401 gathers:
-    throughput of each (device time per migration), the surrogate's training
-    time and traveltime error on the tables, and the image error of the
-    surrogate path (and of the straight-ray background alone, the method
-    without the network) against the table path."""
+def surrogate_section(train_steps: int, steps: int, warmup: int, threads: int):
+    """Table path vs learned-surrogate path on the same v(z) 201x401 gathers,
+    every image judged against the FP64 oracle of the table path (run on the
+    host cores): throughput of each (device time per migration), the
+    surrogate's training time and traveltime error on the tables, the image
+    error of each way the surrogate can supply the leg fields, of the
+    background alone (the method without the network), and the floor any
+    surrogate that supplies its own source-position derivative meets."""
     import torch
     import kirch_datuming_b200 as kd
     from kirch_datuming_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    import _cases
+    import surrogate as sgo
     vel, T1, D1, data1, g = synth.vz_small_workload(seed=4)
     f = lambda v: float(np.float32(v))  # noqa: E731
-    geom = kd.geometry(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds),
-                       nz=g.nz, nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0,
-                       sdy=f(g.dp), rny=g.npos, ry0=0.0, rdy=f(g.dp))
+    gd = dict(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds), nz=g.nz,
+              nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0, sdy=f(g.dp), rny=g.npos, ry0=0.0,
+              rdy=f(g.dp))
+    geom = kd.geometry(**gd)
     kp = kd.params(*TOKENS)
     pairs = g.nz * g.nx * g.ns * g.nh
     st = torch.cuda.current_stream()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    Th, Dh, dh_ = T1.cpu().numpy(), D1.cpu().numpy(), data1.cpu().numpy()
+    op = _cases.oracle_params(kp, gd, kd.output_axis(kp, geom))
+    t0 = time.perf_counter()
+    o64 = oracle.migrate_adj(op, dh_, Th, Dh, Th, Dh, fp64=True)
+    oracle_s = time.perf_counter() - t0
 
-    def run(src=None, rcv=None):
+    def run(sur=None, angle="fd", tx="network"):
         plan = kd.Plan(kp, geom, stream=st.cuda_stream)
         plan.set_tables(T1, D1, T1, D1)
-        if src is not None:
-            plan.set_surrogate(src, rcv)
+        if sur is not None:
+            plan.set_surrogate(sur, sur, angle=angle, tx=tx)
         img = torch.zeros((plan.ng, g.nx, g.nz), dtype=torch.float32, device="cuda")
         for _ in range(warmup):
             plan.migrate(data1, img)
@@ -590,11 +658,13 @@ def surrogate_section(train_steps: int, steps: int, warmup: int):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
         plan.close()
-        return img.cpu().double().numpy(), ms, statistics.median(fields), statistics.median(summ)
+        im = img.cpu().double().numpy()
+        return {"value": pairs / (ms / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms,
+                "fields_ms": statistics.median(fields), "k_sum_ms": statistics.median(summ),
+                "relL2_vs_fp64_oracle": rel(im, o64)}, im
 
-    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
-    img_t, ms_t, fl_t, sm_t = run()
-    net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    table, img_t = run()
+    net = kd.Surrogate(seed=1, **SG_CONFIG)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, train_steps, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
@@ -604,41 +674,70 @@ def surrogate_section(train_steps: int, steps: int, warmup: int):
     n = 200000
     ip, iz, ix = rng.integers(0, g.npos, n), rng.integers(0, g.nz, n), rng.integers(0, g.nx, n)
     Tt = T1[torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), torch.from_numpy(iz).cuda()].cpu().numpy()
-    Tg = net.eval((ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32),
-                  (ix * g.dx).astype(np.float32))[0].cpu().numpy()
-    err_ms = 1000.0 * np.abs(Tg - Tt)
-    img_s, ms_s, fl_s, sm_s = run(net, net)
-    background = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
+    pts = ((ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32), (ix * g.dx).astype(np.float32))
+
+    def tt_err(sur):
+        e = 1000.0 * np.abs(sur.eval(*pts)[0].cpu().numpy() - Tt)
+        return {"rms": float(np.sqrt(np.mean(e ** 2))), "p99": float(np.percentile(e, 99)), "max": float(e.max())}
+
+    variants = {}
+    for name, angle, tx in (("fd_angle_network_tx", "fd", "network"), ("fd_angle_table_tx", "fd", "table"),
+                            ("network_angle_network_tx", "network", "network")):
+        r, im = run(net, angle, tx)
+        r["relL2_vs_table_path"] = rel(im, img_t)
+        variants[name] = r
+    background = kd.Surrogate(seed=1, **SG_CONFIG)
     p = background.get_params()
-    p[-129:] = 0.0  # output weights and bias: tau = 1, T = straight-ray time
+    p[sgo.OFF_WO:] = 0.0  # output weights and bias: T = the background alone
     background.set_params(p)
-    img_b, _, _, _ = run(background, background)
+    bg_err = tt_err(background)
+    bg_fd, _ = run(background, "fd", "network")
+    bg_tab, _ = run(background, "fd", "table")
+    # the floor of a surrogate that supplies its own source-position
+    # derivative: the table path with dT/dxs replaced by the exact derivative
+    # of the table traveltime itself (central difference across the table
+    # positions) instead of eikods2d's tds1 -- 8 of the 64 shots (FP64 oracle)
+    sel = np.arange(0, g.ns, 8)
+    gd8 = dict(gd, ns=len(sel), ds=f(8 * g.ds))
+    op8 = _cases.oracle_params(kp, gd8, kd.output_axis(kp, kd.geometry(**gd8)))
+    sub = np.ascontiguousarray(dh_[sel])
+    Dfd = np.empty_like(Th)
+    Dfd[1:-1] = (Th[2:].astype(np.float64) - Th[:-2]) / (2 * g.dp)
+    Dfd[0], Dfd[-1] = (Th[1] - Th[0]) / g.dp, (Th[-1] - Th[-2]) / g.dp
+    ref8 = oracle.migrate_adj(op8, sub, Th, Dh, Th, Dh, fp64=True)
+    fd8 = oracle.migrate_adj(op8, sub, Th, Dfd, Th, Dfd, fp64=True)
     evals = (g.ns + g.nh) * g.nz * g.nx  # legs x points per migration
-    achieved = evals * SG_FLOPS_EVAL / (fl_s / 1e3) / 1e12
+    fl = variants["fd_angle_network_tx"]["fields_ms"]
+    achieved = evals * SG_FLOPS["tx"] / (fl / 1e3) / 1e12
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
             peak, peak_src = float(json.load(fh)["bf16_tflops"]), "of measured"
     except Exception:
         peak, peak_src = 1590.0, "of fallback"
-    net.close()
-    background.close()
-    return {
+    out = {
         "workload": SG_WORKLOAD, "pairs_per_step": pairs,
-        "table_path": {"value": pairs / (ms_t / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_t,
-                       "fields_ms": fl_t, "k_sum_ms": sm_t},
-        "surrogate_path": {"value": pairs / (ms_s / 1e3) / 1e9, "unit": "Gpairs/s", "ms_per_step": ms_s,
-                           "fields_ms": fl_s, "k_sum_ms": sm_s},
-        "image_rel_l2_vs_table_path": rel(img_s, img_t),
-        "image_rel_l2_background_only_vs_table_path": rel(img_b, img_t),
-        "meets_rel_l2_1e-3": rel(img_s, img_t) <= 1e-3,
+        "oracle": {"seconds": oracle_s, "threads": threads},
+        "network": {"config": {k: list(v) if isinstance(v, tuple) else v for k, v in SG_CONFIG.items()},
+                    "layers": "3 inputs, 64 Fourier frequencies each, 4 x 128 SiLU, BF16 operands, FP32 accumulation"},
+        "table_path": table,
+        "surrogate_path": variants,
+        "background_only": {"traveltime_err_ms": bg_err, "fd_angle_network_tx": bg_fd, "fd_angle_table_tx": bg_tab},
+        "derivative_floor": {
+            "what": "table path with dT/dxs = central difference of the table traveltime across positions instead "
+                    "of tds1 (the derivative a traveltime-only surrogate converges to); 8 of 64 shots, FP64 oracle",
+            "relL2_vs_fp64_oracle": rel(fd8, ref8)},
+        "meets_rel_l2_1e-3": {k: v["relL2_vs_fp64_oracle"] <= 1e-3 for k, v in variants.items()},
         "training": {"steps": train_steps, "batch": 16384, "seconds": train_s,
                      "samples_per_s": train_steps * 16384 / train_s, "final_loss_ms2": float(np.mean(losses[-50:])),
-                     "traveltime_err_ms": {"rms": float(np.sqrt(np.mean(err_ms ** 2))),
-                                           "p99": float(np.percentile(err_ms, 99)), "max": float(err_ms.max())}},
-        "roofline": {"bound": "tensor", "kernel": "k_sg_fields", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "peak_source": peak_src,
-                     "flops_per_eval": SG_FLOPS_EVAL, "evals_per_step": evals},
+                     "traveltime_err_ms": tt_err(net)},
+        "roofline": {"bound": "tensor", "kernel": "k_sg_fields (traveltime + source-position derivative)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": peak_src, "flops_per_eval": SG_FLOPS["tx"], "evals_per_step": evals,
+                     "note": "fields_ms also holds the finite-difference direction pass"},
     }
+    net.close()
+    background.close()
+    return out
 
 
 # --------------------------------------------------------- batched section ---
@@ -944,7 +1043,10 @@ def main():
     if dist is None and not args.no_tables and args.size == "full":
         line["tables"] = tables_section(args.steps, args.warmup, threads)
     if dist is None and args.surrogate_steps > 0:
-        line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup)
+        try:  # an extra object: its failure is recorded, the line still prints
+            line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup, threads)
+        except Exception as e:  # noqa: BLE001
+            line["surrogate"] = {"workload": SG_WORKLOAD, "error": str(e)[-400:]}
     if dist is None and not args.no_batched:
         plan.close()
         del T, D, data, image

@@ -54,13 +54,15 @@ def build(force: bool = False, verbose: bool = False) -> None:
     env["CXX"] = "g++"
     host = ["-ccbin", "g++"]
     if force or _stale(LIB, deps):
-        cmd = [nvcc(), *ARCH, *host, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
+        # a variable used before it is set is an error, not a warning
+        cmd = [nvcc(), *ARCH, *host, "-O3", "-lineinfo", "-std=c++17", "-Xcudafe", "--diag_error=549",
+               "-Xcompiler", "-fPIC,-O3,-Werror=uninitialized,-Werror=maybe-uninitialized",
                "-Xptxas", "-v" if verbose else "-O3", "-shared", "-o", LIB,
                *[os.path.join(CSRC, s) for s in SOURCES]]
         r = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True, env=env)
         if r.returncode != 0:
             raise RuntimeError("nvcc failed:\n" + r.stdout[-6000:] + r.stderr[-6000:])
-        if verbose:
+        if verbose or "warning" in r.stderr:
             sys.stderr.write(r.stderr)
     for exe, src in ((CLI, "kirchmig2d_cig_main.cpp"), (EIK_CLI, "eikods2d_main.cpp"),
                      (K2D_CLI, "kirchmig2d_main.cpp"), (STITCH_CLI, "layercom_cig_main.cpp")):
