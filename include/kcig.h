@@ -412,6 +412,22 @@ int kcig_stitch_window(float *out, int n1, int n2, int n3, const float *layer, i
                        int previous_end, int stitch_blend, float layer_scale, int use_lateral, int scalex_aper,
                        double scalex_scale, long long *nonfinite, void *stream);
 
+/* All nwin depth windows of one stitch in a single device pass (the loop of
+ * src/layercom_cig.cpp:473-535 over every window): window k is layers[k]
+ * [n3][n2][ends[k]-starts[k]+1] (device) covering depth rows
+ * starts[k]..ends[k] (host arrays), scaled by scales[k] and, for k > 0 when
+ * use_lateral, by the lateral taper; each window shares rows with the one
+ * before it, as in kcig_stitch_window.  Every output sample is formed from
+ * the windows covering its row in window order, so out equals nwin calls of
+ * kcig_stitch_window on a zeroed volume bit for bit (rows no window covers
+ * are 0); each window sample is read once and each output sample written
+ * once, with one weight upload and one counter read-back for the whole
+ * stitch.  nonfinite: host long long[nwin], the non-finite products of each
+ * window.  Synchronous on `stream`. */
+int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin, const float *const *layers, const int *starts,
+                        const int *ends, int stitch_blend, const float *scales, int use_lateral, int scalex_aper,
+                        double scalex_scale, long long *nonfinite, void *stream);
+
 /* The drop-in layercom_cig (src/layercom_cig.cpp:412-556): the same keys
  * (full_model= layer_image_base= layer_txt= output_file= nlayers= nangle=
  * scale= stitch_blend= scalex_aper= scalex_scale=), layer file rules,

@@ -15,7 +15,7 @@ import os
 import numpy as np
 
 __all__ = ["lib", "KcigError", "Params", "Geometry", "params", "geometry", "output_axis", "Plan",
-           "run_cli", "doubint_device", "leg_fields_device", "shot_positions", "eikonal_tables", "eikods", "library_path",
+           "run_cli", "doubint_device", "leg_fields_device", "shot_positions", "stitch_windows", "eikonal_tables", "eikods", "library_path",
            "cli_path", "eikods_cli_path", "kirchmig2d_cli_path", "layercom_cig_cli_path", "params_kirchmig2d",
            "stitch_window"]
 
@@ -144,6 +144,8 @@ def lib():
         L.kcig_graph_destroy.restype = None
         L.kcig_shots_pairs.argtypes = [vp]
         L.kcig_shots_pairs.restype = ctypes.c_longlong
+        L.kcig_stitch_windows.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
+                                          ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, vp, vp]
         L.kcig_stitch_window.argtypes = ([fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, fp, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.POINTER(ctypes.c_longlong), vp])
@@ -389,6 +391,35 @@ def stitch_window(out, layer, start: int, end: int, previous_end: int = -1, stit
                                     int(previous_end), int(stitch_blend), float(layer_scale), int(bool(use_lateral)),
                                     int(scalex_aper), float(scalex_scale), ctypes.byref(bad), ctypes.c_void_p(st)))
     return bad.value
+
+
+def stitch_windows(out, layers, windows, stitch_blend: int = 15, scales=None, use_lateral: bool = False,
+                   scalex_aper: int = 0, scalex_scale: float = 1.0, stream=None):
+    """Every depth window of one stitch in a single device pass
+    (kcig_stitch_windows): out [n3][n2][n1] (overwritten; rows no window
+    covers become 0), layers[k] [n3][n2][e-s+1] for windows[k] = (s, e),
+    contiguous CUDA float32 tensors.  Returns the non-finite count per window."""
+    import torch
+    n3, n2, n1 = out.shape
+    nw = len(windows)
+    if len(layers) != nw or nw < 1:
+        raise ValueError("one layer per window")
+    for t, (s0, e0) in zip([out] + list(layers), [(0, n1 - 1)] + list(windows)):
+        if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous() and t.dim() == 3):
+            raise ValueError("expects contiguous 3-D CUDA float32 tensors")
+        if tuple(t.shape) != (n3, n2, e0 - s0 + 1):
+            raise ValueError("layer shape %s does not match rows %d..%d" % (tuple(t.shape), s0, e0))
+    scales = [1.0] * nw if scales is None else list(scales)
+    ptrs = (ctypes.c_void_p * nw)(*[t.data_ptr() for t in layers])
+    starts = (ctypes.c_int * nw)(*[int(w[0]) for w in windows])
+    ends = (ctypes.c_int * nw)(*[int(w[1]) for w in windows])
+    sc = (ctypes.c_float * nw)(*[float(x) for x in scales])
+    bad = (ctypes.c_longlong * nw)()
+    st = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    _check(lib().kcig_stitch_windows(out.data_ptr(), n1, n2, n3, nw, ptrs, starts, ends, int(stitch_blend), sc,
+                                     int(bool(use_lateral)), int(scalex_aper), float(scalex_scale), bad,
+                                     ctypes.c_void_p(st)))
+    return [int(b) for b in bad]
 
 
 def shot_positions(g: Geometry, first: int = 0, count: int = None):

@@ -12,6 +12,7 @@
 // the reference's float operations separate (no fused multiply-add), so the
 // output is the reference's, bit for bit.
 #include <math.h>
+#include <string.h>
 
 #include <map>
 #include <mutex>
@@ -167,4 +168,179 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
     if (e != cudaSuccess) rc = cuda_error(e, "kcig_stitch_window");
     *nonfinite = (long long)bad;
     return rc;
+}
+
+// ------------------------------------------------- all windows, one pass --
+// The windows of one stitch in a single kernel: every output sample is
+// formed from the windows that cover its depth row, taken in window order
+// with exactly the per-window rule above (write; keep the upper value; or
+// blend), so the result equals the window-by-window calls bit for bit.  Each
+// window sample is read once and each output sample written once (rows no
+// window covers are written as 0): no read of the output, one launch, one
+// upload of the weights and one read-back of the counters.
+namespace kcig {
+
+struct StitchWin {
+    const float *layer;  // [n3][n2][n1w]
+    int start, n1w, keep_upper, blend_count, overlap, previous_end, lateral, woff;
+    float scale;
+};
+
+struct StitchAllArgs {
+    float *out;
+    const StitchWin *win;     // [nwin]
+    const int *row_ptr;       // [n1 + 1]: windows covering row r are row_win[row_ptr[r] .. row_ptr[r+1])
+    const int *row_win;
+    const float *weights;     // blend weights of every window (at win.woff), then the lateral taper [n2]
+    const float *lateral;
+    unsigned long long *nonfinite;  // [nwin]
+    int n1, n2, n3, nwin;
+};
+
+__global__ void __launch_bounds__(256) k_stitch_all(const StitchAllArgs a)
+{
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int ncol = a.n2 * a.n3;
+    for (int col = blockIdx.x * warps + (threadIdx.x >> 5); col < ncol; col += gridDim.x * warps) {
+        const int i2 = col % a.n2;
+        const float sx = a.lateral ? a.lateral[i2] : 1.0f;
+        float *dst = a.out + (size_t)col * a.n1;
+        for (int r = lane; r < a.n1; r += 32) {
+            float val = 0.0f;
+            for (int q = a.row_ptr[r]; q < a.row_ptr[r + 1]; q++) {
+                const int k = a.row_win[q];
+                const StitchWin &w = a.win[k];
+                const int i1 = r - w.start;
+                const float scale = __fmul_rn(w.scale, w.lateral ? sx : 1.0f);
+                float v = __fmul_rn(w.layer[(size_t)col * w.n1w + i1], scale);
+                if (!isfinite(v)) {
+                    atomicAdd(a.nonfinite + k, 1ull);
+                    v = 0.0f;
+                }
+                if (w.overlap > 0 && r <= w.previous_end) {
+                    if (i1 < w.keep_upper || w.blend_count == 0) continue;
+                    const float bw = a.weights[w.woff + i1 - w.keep_upper];
+                    val = __fadd_rn(__fmul_rn(val, __fsub_rn(1.0f, bw)), __fmul_rn(v, bw));
+                } else {
+                    val = v;
+                }
+            }
+            dst[r] = val;
+        }
+    }
+}
+
+}  // namespace kcig
+
+extern "C" int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin, const float *const *layers,
+                                   const int *starts, const int *ends, int stitch_blend, const float *scales,
+                                   int use_lateral, int scalex_aper, double scalex_scale, long long *nonfinite,
+                                   void *stream)
+{
+    if (!out || !layers || !starts || !ends || !scales || !nonfinite || n1 <= 0 || n2 <= 0 || n3 <= 0 || nwin < 1)
+        return set_error(KCIG_ERR_ARG, "kcig_stitch_windows: bad arguments");
+    if ((long long)n2 * n3 > 0x7fffffffLL) return set_error(KCIG_ERR_ARG, "kcig_stitch_windows: n2*n3 too large");
+    if (stitch_blend < -1) return set_error(KCIG_ERR_ARG, "stitch_blend must be -1 or nonnegative");
+    if (scalex_aper < 0) return set_error(KCIG_ERR_ARG, "scalex_aper must be nonnegative");
+    std::vector<StitchWin> win(nwin);
+    std::vector<float> wts;
+    for (int k = 0; k < nwin; k++) {
+        const int start = starts[k], end = ends[k];
+        if (!layers[k] || start < 0 || end < start || end >= n1)
+            return set_error(KCIG_ERR_ARG, "Invalid layer range [%d,%d]", start, end);
+        const int previous_end = k > 0 ? ends[k - 1] : -1;
+        int overlap = 0;
+        if (previous_end >= 0) {
+            overlap = previous_end - start + 1;
+            if (overlap <= 0) return set_error(KCIG_ERR_ARG, "no overlap with the window above");
+        }
+        int blend_count = overlap;
+        if (overlap > 0 && stitch_blend >= 0) blend_count = std::min(stitch_blend, overlap);
+        StitchWin &w = win[k];
+        w.layer = layers[k];
+        w.start = start;
+        w.n1w = end - start + 1;
+        w.keep_upper = overlap - blend_count;
+        w.blend_count = blend_count;
+        w.overlap = overlap;
+        w.previous_end = previous_end;
+        w.lateral = use_lateral && k > 0;
+        w.scale = scales[k];
+        w.woff = (int)wts.size();
+        // complementary cosine weights (:522-528), in double, rounded once
+        for (int bi = 0; bi < blend_count; bi++) {
+            const double u = blend_count > 1 ? (double)bi / (double)(blend_count - 1) : 1.0;
+            wts.push_back((float)(0.5 * (1.0 - cos(3.14159265358979323846 * u))));
+        }
+    }
+    const int lat_off = (int)wts.size();
+    if (use_lateral) {  // lateral taper towards both edges (:455-466)
+        for (int i2 = 0; i2 < n2; i2++) {
+            float v = 1.0f;
+            const int edge = std::min(i2, n2 - 1 - i2);
+            if (scalex_aper > 0 && edge < scalex_aper) {
+                const double taper = scalex_aper == 1 ? 1.0 : 1.0 - (double)edge / (double)(scalex_aper - 1);
+                v = (float)(1.0 + (scalex_scale - 1.0) * taper);
+            }
+            wts.push_back(v);
+        }
+    }
+    // the windows covering each depth row, in window order
+    std::vector<int> row_ptr(n1 + 1, 0), row_win;
+    for (int r = 0; r < n1; r++) {
+        row_ptr[r] = (int)row_win.size();
+        for (int k = 0; k < nwin; k++)
+            if (r >= win[k].start && r < win[k].start + win[k].n1w) row_win.push_back(k);
+    }
+    row_ptr[n1] = (int)row_win.size();
+    // one staging upload: counters, window records, row lists, weights
+    const size_t o_bad = 0, o_win = o_bad + (((size_t)nwin * 8 + 15) & ~(size_t)15);
+    const size_t o_ptr = o_win + (((size_t)nwin * sizeof(StitchWin) + 15) & ~(size_t)15);
+    const size_t o_rw = o_ptr + (((size_t)(n1 + 1) * 4 + 15) & ~(size_t)15);
+    const size_t o_w = o_rw + (((size_t)std::max<size_t>(1, row_win.size()) * 4 + 15) & ~(size_t)15);
+    const size_t bytes = o_w + std::max<size_t>(1, wts.size()) * 4;
+    std::vector<unsigned char> host(bytes, 0);
+    memcpy(host.data() + o_win, win.data(), nwin * sizeof(StitchWin));
+    memcpy(host.data() + o_ptr, row_ptr.data(), (n1 + 1) * 4);
+    if (!row_win.empty()) memcpy(host.data() + o_rw, row_win.data(), row_win.size() * 4);
+    if (!wts.empty()) memcpy(host.data() + o_w, wts.data(), wts.size() * 4);
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    std::pair<void *, size_t> &buf = g_scratch[dev];
+    if (buf.second < bytes) {
+        if (buf.first) cudaFree(buf.first);
+        buf = {nullptr, 0};
+        KCIG_CUDA(cudaMalloc(&buf.first, std::max<size_t>(bytes, 64 << 10)));
+        buf.second = std::max<size_t>(bytes, 64 << 10);
+    }
+    unsigned char *d = (unsigned char *)buf.first;
+    cudaError_t e = cudaMemcpyAsync(d, host.data(), bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        StitchAllArgs a;
+        a.out = out;
+        a.win = (const StitchWin *)(d + o_win);
+        a.row_ptr = (const int *)(d + o_ptr);
+        a.row_win = (const int *)(d + o_rw);
+        a.weights = (const float *)(d + o_w);
+        a.lateral = use_lateral ? a.weights + lat_off : nullptr;
+        a.nonfinite = (unsigned long long *)(d + o_bad);
+        a.n1 = n1;
+        a.n2 = n2;
+        a.n3 = n3;
+        a.nwin = nwin;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const size_t want = ((size_t)n2 * n3 + 7) / 8;
+        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 16));
+        k_stitch_all<<<grid, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    std::vector<unsigned long long> bad(nwin, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bad.data(), d + o_bad, nwin * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(e, "kcig_stitch_windows");
+    for (int k = 0; k < nwin; k++) nonfinite[k] = (long long)bad[k];
+    return KCIG_OK;
 }

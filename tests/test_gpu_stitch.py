@@ -95,3 +95,38 @@ def test_stitch_window_counts_nonfinite():
     out2 = torch.zeros_like(out)
     big = np.full((2, 3, 10), 3e38, np.float32)
     assert kd.stitch_window(out2, torch.from_numpy(big).cuda(), 0, 9, layer_scale=10.0) == 60
+
+
+@pytest.mark.parametrize("blend,aper,sxs", [(15, 0, 1.0), (3, 4, 1.7), (0, 0, 1.0), (-1, 2, 0.6), (40, 7, 0.25)])
+def test_stitch_windows_one_pass_equals_the_window_calls(blend, aper, sxs):
+    # the one-pass kernel over all windows against the oracle (bit for bit),
+    # with a window whose overlap reaches two windows back and a row range
+    # no window covers (written as zeros)
+    import torch
+    rng = np.random.default_rng(blend + 7 * aper)
+    n1, n2, n3 = 140, 29, 4
+    wins = [(0, 50), (37, 90), (45, 120), (100, 131)]
+    vols = [rng.standard_normal((n3, n2, e - s + 1)).astype(np.float32) for s, e in wins]
+    scales = [1.0, 0.75, 1.25, 0.5]
+    vols[1][1, 3, 5] = 0.0  # the oracle refuses non-finite windows: 0 there, NaN on the device
+    ref = so.stitch(n1, wins, vols, scales, blend, aper, sxs)
+    vols[1][1, 3, 5] = np.nan  # counted, and written as 0
+    out = torch.full((n3, n2, n1), 7.0, dtype=torch.float32, device="cuda")  # overwritten everywhere
+    bad = kd.stitch_windows(out, [torch.from_numpy(v).cuda() for v in vols], wins, blend, scales, True, aper, sxs)
+    got = out.cpu().numpy()
+    assert bad == [0, 1, 0, 0]
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert not got[:, :, 132:].any()
+
+
+def test_stitch_windows_full_image_size():
+    import torch
+    rng = np.random.default_rng(8)
+    n1, n2, n3 = 601, 1601, 61
+    wins = [(0, 130), (110, 250), (230, 370), (350, 490), (470, 600)]
+    vols = [rng.standard_normal((n3, n2, e - s + 1), dtype=np.float32) for s, e in wins]
+    scales = [1.0, 1.1, 0.9, 1.2, 0.8]
+    ref = so.stitch(n1, wins, vols, scales, 15, 50, 1.5)
+    out = torch.empty((n3, n2, n1), dtype=torch.float32, device="cuda")
+    kd.stitch_windows(out, [torch.from_numpy(v).cuda() for v in vols], wins, 15, scales, True, 50, 1.5)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
