@@ -73,7 +73,13 @@ def test_surrogate_eval_vs_oracle(bg):
     e = np.abs(got[0] - ref[0]) / osc
     print("out err median %.2e p95 %.2e max %.2e" % _stats(e))
     med, p95, mx = _stats(e)
-    assert med < 1e-5 and p95 < 2e-3 and mx < 2e-2
+    if BACKGROUNDS[bg]["residual_ms"] > 0:
+        # T = Tb + 1 ms * out comes back in FP32: at 1-2 s its rounding
+        # (~1e-7 s) is ~1e-4 of the residual scale, which bounds the median
+        ea = np.abs(got[0] - ref[0])
+        assert np.median(ea) < 2e-7 and np.percentile(ea, 95) < 2e-6 and ea.max() < 2e-5
+    else:
+        assert med < 1e-5 and p95 < 2e-3 and mx < 2e-2
     for k in (1, 2, 3):
         e = np.abs(got[k] - ref[k]) / np.sqrt(np.mean(ref[k] ** 2))
         print("dT/d%s err median %.2e p95 %.2e max %.2e" % (("xs", "z", "x")[k - 1], *_stats(e)))

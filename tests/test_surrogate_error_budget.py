@@ -5,11 +5,12 @@ GPU).  These are properties of the summation, independent of any network:
 * a coherent traveltime error of 1 us already costs ~2.4e-4 of image relative
   L2 (10 us: ~2.4e-3) -- the surrogate's traveltime must be good to a few us;
 * the antialias width uses eikods2d's tds1 (the source-position derivative
-  its marching recursion computes).  The exact derivative of the same
-  traveltime tables across positions differs from tds1 by a few percent, and
-  using it moves the image by more than 1e-3 -- so a surrogate that supplies
-  its own source-position derivative (the derivative of its traveltime)
-  cannot meet 1e-3 however well it fits the traveltimes;
+  its marching recursion computes).  The central difference of the same
+  tables across neighbouring positions differs from tds1 by a few percent
+  (it carries the tables' grid-scale noise from position to position) and
+  moves the image by more than 1e-3 -- a surrogate's own derivative must
+  follow tds1, not that difference (a smooth network's derivative does: on
+  the GPU it gives the same image error as tds1 itself);
 * the scattering angle comes from the finite-difference gradient of the
   traveltime with triangle smoothing.  Taking it from the exact eikonal
   gradient (eikods2d's gradient volumes) instead moves the image by more than
