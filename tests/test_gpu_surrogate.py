@@ -278,54 +278,61 @@ def test_surrogate_leg_fields_match_eval(golden):
 
 
 def test_surrogate_training_gain_and_migration():
-    # train on the v(z) 201x401 tables (GPU eikonal, 401 positions), then
-    # migrate its gathers with the surrogate's leg fields.  What the network
-    # gains over the method without it (the straight-ray background T0 alone):
-    # traveltime error on the tables and image error against the table path.
+    # train on the v(z) 201x401 tables (GPU eikonal, 401 positions) and
+    # migrate its gathers with the surrogate's traveltimes, every image judged
+    # against the FP64 oracle of the table path.  What the network gains over
+    # the method without it (the linear-gradient background alone), and what
+    # the angle source costs: the network's own input gradient against the
+    # finite-difference gradient of its traveltime (the tables' way).
+    # Bounds from the measured sweep (40k steps: 0.98 us rms traveltime,
+    # image 2.8e-3; the background alone 0.87 ms and 0.21).
     import torch
+    import _cases
+    import oracle
     from kirch_datuming_b200 import synth
     vel, T1, D1, data1, g = synth.vz_small_workload(seed=4)
-    net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
-    losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, 6000, batch=16384, lr=3e-3, lr_final=3e-5, seed=3)
+    net = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1, vgrad=0.6,
+                       residual_ms=1.0)
+    losses = net.train(T1, 0.0, g.dp, 0.0, g.dz, 0.0, g.dx, 40000, batch=16384, lr=1e-3, lr_final=1e-5, seed=3)
     assert np.all(np.isfinite(losses)) and losses[-50:].mean() < 1e-3 * losses[:50].mean()
+    bg = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1, vgrad=0.6,
+                      residual_ms=1.0)
+    p = bg.get_params()
+    p[sgo.OFF_WO:] = 0.0  # T = the background alone
+    bg.set_params(p)
     rng = np.random.default_rng(1)
     n = 50000
     ip, iz, ix = rng.integers(0, g.npos, n), rng.integers(0, g.nz, n), rng.integers(0, g.nx, n)
     Tt = T1[torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), torch.from_numpy(iz).cuda()].cpu().numpy()
-    xs, z, x = (ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32), (ix * g.dx).astype(np.float32)
-    Tg = net.eval(xs, z, x)[0].cpu().numpy()
-    rms_net = 1000 * np.sqrt(np.mean((Tg - Tt) ** 2))
-    rms_bg = 1000 * np.sqrt(np.mean((np.hypot(x - xs, z) / 1.5 - Tt) ** 2))
-    print("traveltime rms: network %.3f ms, straight-ray background %.1f ms" % (rms_net, rms_bg))
-    assert rms_net < 0.6 and rms_net < 0.01 * rms_bg
+    pts = ((ip * g.dp).astype(np.float32), (iz * g.dz).astype(np.float32), (ix * g.dx).astype(np.float32))
+    rms = lambda s: 1e6 * np.sqrt(np.mean((s.eval(*pts)[0].cpu().numpy() - Tt) ** 2))  # noqa: E731
+    rms_net, rms_bg = rms(net), rms(bg)
+    print("traveltime rms: network %.3f us, background %.1f us" % (rms_net, rms_bg))
+    assert rms_net < 2.0 and rms_net < 0.01 * rms_bg
 
     f = lambda v: float(np.float32(v))  # noqa: E731
-    geom = kd.geometry(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds),
-                       nz=g.nz, nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0,
-                       sdy=f(g.dp), rny=g.npos, ry0=0.0, rdy=f(g.dp))
+    gd = dict(nt=g.nt, nh=g.nh, ns=g.ns, t0=0.0, dt=f(g.dt), h0=f(g.h0), dh=f(g.dh), s0=0.0, ds=f(g.ds), nz=g.nz,
+              nx=g.nx, z0=0.0, dz=f(g.dz), x0=0.0, dx=f(g.dx), sny=g.npos, sy0=0.0, sdy=f(g.dp), rny=g.npos,
+              ry0=0.0, rdy=f(g.dp))
+    geom = kd.geometry(**gd)
     kp = kd.params("cig=1", "mode=angle", "cmp=0", "angle_min=0", "angle_max=60", "angle_step=1", "angle_n=61",
                    "direct_mute=1", "direct_mute_slope=0.5", "direct_mute_intercept=0", "direct_mute_taper=0.05")
-    bg = kd.Surrogate((0.0, 0.0, 0.0), (4.0, 2.0, 4.0), fmax=3.0, vref=1.5, zsrc=0.0, seed=1)
-    p = bg.get_params()
-    p[sgo.OFF_WO:] = 0.0
-    bg.set_params(p)
-    imgs = []
-    for sur in (None, net, bg):
+    Th, Dh = T1.cpu().numpy(), D1.cpu().numpy()
+    o64 = oracle.migrate_adj(_cases.oracle_params(kp, gd, kd.output_axis(kp, geom)), data1.cpu().numpy(), Th, Dh,
+                             Th, Dh, fp64=True)
+
+    def image(sur, angle="fd", tx="network"):
         plan = kd.Plan(kp, geom)
         plan.set_tables(T1, D1, T1, D1)
-        if sur is not None:
-            plan.set_surrogate(sur, sur)
+        plan.set_surrogate(sur, sur, angle=angle, tx=tx)
         img = torch.zeros((plan.ng, g.nx, g.nz), device="cuda")
         plan.migrate(data1, img)
-        imgs.append(img.cpu().double().numpy())
         plan.close()
-    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)  # noqa: E731
-    r_net, r_bg = rel(imgs[1], imgs[0]), rel(imgs[2], imgs[0])
-    print("image relL2 vs table path: network %.3f, background %.3f" % (r_net, r_bg))
-    assert r_net < 0.35 and r_net < 0.5 * r_bg
-    # the reflectors stay where the table path puts them
-    prof = [np.abs(im).sum(axis=(0, 1)) for im in imgs[:2]]
-    for zr in (60, 120, 170):
-        assert abs(int(np.argmax(prof[1][zr - 8:zr + 9])) - int(np.argmax(prof[0][zr - 8:zr + 9]))) <= 1
+        return oracle.rel_l2(img.cpu().numpy(), o64)
+
+    r_net, r_tab, r_ang, r_bg = image(net), image(net, tx="table"), image(net, angle="network"), image(bg)
+    print("image relL2 vs FP64 oracle: network %.2e, with table derivative %.2e, network angle %.2e, "
+          "background %.2e" % (r_net, r_tab, r_ang, r_bg))
+    assert r_net < 5e-3 and r_tab < 5e-3 and r_net < 0.05 * r_bg and r_ang > 5 * r_net
     net.close()
     bg.close()
