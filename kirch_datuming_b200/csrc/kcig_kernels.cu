@@ -1,6 +1,6 @@
 // sm_100a kernels of the adjoint angle-domain Kirchhoff summation.
 //
-//   K1 k_prelude      per-trace direct mute + doubint (FP64 running sums) +
+//   K1 k_prelude_cta  per-trace direct mute + doubint (FP64 running sums) +
 //                     optional diff2, written as {D[i], D[i+1]-D[i]} pairs so
 //                     a linear-interpolated pick is one 16-byte load and one
 //                     fused multiply-add.
@@ -29,12 +29,13 @@ namespace kcig {
 
 
 // =============================================================== K1 prelude ==
-// One warp per trace.  The trace is staged in shared memory as double, muted
-// (kirchmig2d_cig.cpp:110-129), then integrated causally and anticausally
-// (kirmig.cpp:8-24) with every running sum in FP64: each lane scans a
-// contiguous chunk and a warp scan of the chunk totals links the chunks.
-// FP64 sums keep the later second differences (the pick) accurate, which an
-// FP32 running sum of a long trace does not.
+// doubint of one trace per warp (the building block kcig_doubint_device and
+// the forward modelling's final integration): the trace is staged in shared
+// memory as double and integrated causally and anticausally (kirmig.cpp:8-24)
+// with every running sum in FP64: each lane scans a contiguous chunk and a
+// warp scan of the chunk totals links the chunks.  FP64 sums keep the later
+// second differences (the pick) accurate, which an FP32 running sum of a long
+// trace does not.  The migration's prelude is k_prelude_cta further down.
 __device__ __forceinline__ double warp_excl_scan(double v, double *total)
 {
     const int lane = threadIdx.x & 31;
@@ -102,52 +103,6 @@ __device__ void diff2_warp(double *s, int nt, double dt)
         cur = nx;
     }
     __syncwarp();
-}
-
-__global__ void __launch_bounds__(64) k_prelude(PreludeArgs a)
-{
-    extern __shared__ double smem_d[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tr = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (tr >= a.ntr) return;
-    double *s = smem_d + (size_t)warp * a.nt;
-    const int k = tr / a.nhc, r = tr % a.nhc;
-    const float *x = a.data + ((size_t)(a.shot0 + k) * a.nh + (a.rcv0 + r)) * a.nt;
-    int nt = a.nt;
-    if (a.toff) {  // ragged shots: own samples, own length (k_sum reads no
-                   // padding trace and no sample past a trace's own end)
-        const long long off = a.toff[tr];
-        if (off < 0) return;
-        x = a.data + off;
-        nt = a.tnt[tr];
-    }
-    double boundary = 0.0;
-    const bool mute = a.mute_sx != nullptr;
-    if (mute) {
-        const double off = a.slope * fabs(a.mute_rx[tr] - a.mute_sx[tr]);
-        boundary = a.invert ? a.intercept - off : a.intercept + off;
-    }
-    for (int i = lane; i < nt; i += 32) {
-        double v = (double)x[i];
-        if (mute) {
-            const double t = a.t0 + (double)i * a.dt;
-            double w = 0.0;
-            if (t >= boundary + a.taper) w = 1.0;
-            else if (t > boundary) w = 0.5 * (1.0 - cospi((t - boundary) / a.taper));
-            v *= w;
-        }
-        s[i] = v;
-    }
-    __syncwarp();
-    doubint_warp(s, nt);
-    if (a.isdiff == 1) diff2_warp(s, nt, a.dt);
-    double2 *out = a.D + (size_t)tr * a.nt;
-    for (int i = lane; i < nt; i += 32) {
-        double2 e;
-        e.x = s[i];
-        e.y = (i + 1 < nt) ? s[i + 1] - s[i] : 0.0;
-        out[i] = e;
-    }
 }
 
 template <typename IN, typename OUT>
