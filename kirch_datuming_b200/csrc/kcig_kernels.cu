@@ -692,8 +692,7 @@ __global__ void __launch_bounds__(256, 3) k_leg_tile(FieldArgs a, LegFields out)
         return;
     }
 
-    // ---- interpolated traveltime (FP64) on the block and its halo; the
-    // block's own points also get T, Tx and the aperture weight written
+    // ---- interpolated traveltime (FP64) on the block and its halo
     double2 *TPo = out.TP + (size_t)blockIdx.y * nzx;
     const double hc0 = L.c[0], hc1 = L.c[1], hc2 = L.c[2], hc3 = L.c[3];
     for (int lx = xlo + (int)threadIdx.y; lx < xhi; lx += blockDim.y) {
@@ -701,30 +700,42 @@ __global__ void __launch_bounds__(256, 3) k_leg_tile(FieldArgs a, LegFields out)
         const float *c1 = stage + (size_t)(1 * W + lx) * SW + phs[1][lx] - zlo;
         const float *c2 = two ? stage + (size_t)(2 * W + lx) * SW + phs[2][lx] - zlo : c0;
         const float *c3 = two ? stage + (size_t)(3 * W + lx) * SW + phs[3][lx] - zlo : c1;
-        const bool xin = lx >= H && lx < H + kGradTile;
         for (int lz = zlo + (int)threadIdx.x; lz < zhi; lz += blockDim.x) {
-            double T, Tx = 0.0;
+            double T;
             if (!two) {
                 T = c0[lz];
-                Tx = c1[lz];
             } else {
                 const double p0 = c0[lz], p1 = c2[lz];
                 const double m0 = c1[lz], m1 = c3[lz];
                 T = hc0 * p0 + hc1 * m0 + hc2 * p1 + hc3 * m1;
             }
             P0[lx * W + lz] = T;
-            if (xin && lz >= H && lz < H + kGradTile) {
-                if (two) {
-                    const double p0 = c0[lz], p1 = c2[lz];
-                    const double m0 = c1[lz], m1 = c3[lz];
-                    Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
-                }
-                const int iz = gz0 + lz, ix = gx0 + lx;
-                const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin,
-                                                     a.rtaper);
-                TPo[(size_t)ix * nz + iz].x = T;
-                out.XW[(size_t)blockIdx.y * nzx + (size_t)ix * nz + iz] = make_float2((float)Tx * L.scale, (float)w);
+        }
+    }
+    // ---- the block's own points, lanes aligned with its kGradTile rows (one
+    // full warp pass per row): T, Tx and the aperture weight written
+    {
+        const int lz = H + (int)threadIdx.x;  // blockDim.x == kGradTile
+        const bool zin = lz >= zlo && lz < zhi;
+        for (int lx = max(H, xlo) + (int)threadIdx.y; lx < min(H + kGradTile, xhi); lx += blockDim.y) {
+            if (!zin) continue;
+            const double p0 = stage[(size_t)(0 * W + lx) * SW + phs[0][lx] + (lz - zlo)];
+            const double m0 = stage[(size_t)(1 * W + lx) * SW + phs[1][lx] + (lz - zlo)];
+            double T, Tx;
+            if (!two) {
+                T = p0;
+                Tx = m0;
+            } else {
+                const double p1 = stage[(size_t)(2 * W + lx) * SW + phs[2][lx] + (lz - zlo)];
+                const double m1 = stage[(size_t)(3 * W + lx) * SW + phs[3][lx] + (lz - zlo)];
+                T = hc0 * p0 + hc1 * m0 + hc2 * p1 + hc3 * m1;
+                Tx = L.e[0] * p0 + L.e[1] * m0 + L.e[2] * p1 + L.e[3] * m1;
             }
+            const int iz = gz0 + lz, ix = gx0 + lx;
+            const double w = leg_aperture_weight(L.pos, iz, ix, a.dz, a.x0, a.dx, a.aper, a.aper_taper, a.rmin,
+                                                 a.rtaper);
+            TPo[(size_t)ix * nz + iz].x = T;
+            out.XW[(size_t)blockIdx.y * nzx + (size_t)ix * nz + iz] = make_float2((float)Tx * L.scale, (float)w);
         }
     }
     __syncthreads();  // the staging buffer is free: it becomes P1..P3

@@ -74,6 +74,11 @@ struct kcig_plan {
     int use_graph = 0;                                     // replay kcig_migrate_prepared as a CUDA graph
     int tile = 0;                                          // summation tile variant (kcig_plan_autotune)
     cudaStream_t own_st = nullptr;                         // capture stream when the plan's is the legacy one
+    // host traces are copied on their own non-blocking stream while the leg
+    // fields compute (it does not synchronise with the legacy stream); the
+    // first trace prelude waits for copy_ev
+    cudaStream_t copy_st = nullptr;
+    cudaEvent_t copy_ev = nullptr, order_ev = nullptr;
 };
 
 // Ragged shots on the device, batched (kcig_shots_prepare); the launch
@@ -442,6 +447,9 @@ extern "C" int kcig_plan_destroy(kcig_plan *P)
     for (DevBuf *b : bufs) b->release();
     release_shots(P);
     if (P->own_st) cudaStreamDestroy(P->own_st);
+    if (P->copy_st) cudaStreamDestroy(P->copy_st);
+    if (P->copy_ev) cudaEventDestroy(P->copy_ev);
+    if (P->order_ev) cudaEventDestroy(P->order_ev);
     delete P;
     return KCIG_OK;
 }
@@ -597,8 +605,21 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     float *d_img = image;
     const int ns = P->shot_count > 0 ? P->shot_count : g.ns;  // shots of this call (kcig_plan_set_shot_range)
     const size_t data_bytes = (size_t)ns * g.nh * g.nt * sizeof(float);
+    bool data_pending = false;
     if (memory == KCIG_MEM_HOST) {
-        KCIG_TRY(upload(P->d_data, data, data_bytes, st));
+        if (!P->copy_st) {
+            KCIG_CUDA(cudaStreamCreateWithFlags(&P->copy_st, cudaStreamNonBlocking));
+            KCIG_CUDA(cudaEventCreateWithFlags(&P->copy_ev, cudaEventDisableTiming));
+            KCIG_CUDA(cudaEventCreateWithFlags(&P->order_ev, cudaEventDisableTiming));
+        }
+        KCIG_TRY(P->d_data.ensure(data_bytes));
+        // the copy starts after the plan's earlier work (which may still read
+        // the buffer) and overlaps the leg fields computed below
+        KCIG_CUDA(cudaEventRecord(P->order_ev, st));
+        KCIG_CUDA(cudaStreamWaitEvent(P->copy_st, P->order_ev, 0));
+        KCIG_CUDA(cudaMemcpyAsync(P->d_data.p, data, data_bytes, cudaMemcpyHostToDevice, P->copy_st));
+        KCIG_CUDA(cudaEventRecord(P->copy_ev, P->copy_st));
+        data_pending = true;
         d_data = P->d_data.as<float>();
         KCIG_TRY(P->d_image.ensure((size_t)P->ng * nzx * sizeof(float)));
         d_img = P->d_image.as<float>();
@@ -806,6 +827,14 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
             pa.slope = p.direct_mute_slope;
             pa.intercept = p.direct_mute_intercept;
             pa.taper = p.direct_mute_taper;
+            if (data_pending) {  // the traces have landed before their first use
+                cudaError_t e = cudaStreamWaitEvent(st, P->copy_ev, 0);
+                if (e != cudaSuccess) {
+                    rc = cuda_error(e, "cudaStreamWaitEvent(traces)");
+                    break;
+                }
+                data_pending = false;
+            }
             rc = launch_prelude(pa, st);
             if (rc) break;
             P->all_launches++;
@@ -885,6 +914,10 @@ extern "C" int kcig_migrate(kcig_plan *P, const float *data, float *image, int m
     }
     cudaError_t e = cudaStreamSynchronize(st);
     if (rc == KCIG_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(migrate)");
+    if (memory == KCIG_MEM_HOST && P->copy_st) {  // the caller's traces are no longer read after this
+        e = cudaStreamSynchronize(P->copy_st);
+        if (rc == KCIG_OK && e != cudaSuccess) rc = cuda_error(e, "cudaStreamSynchronize(trace copy)");
+    }
     for (size_t i = 0; i + 1 < evs.size(); i += 2) {
         float ms = 0.f;
         if (rc == KCIG_OK && cudaEventElapsedTime(&ms, evs[i], evs[i + 1]) == cudaSuccess) P->sum_ms += ms;
