@@ -928,8 +928,15 @@ __device__ __forceinline__ double floor_shift(double x) { return __dadd_rd(x, kF
 #define KCIG_SUM_MINB 7
 #endif
 
+// The unshared-receiver variant (its own receiver stream per shot) can trade
+// resident CTAs for streams in flight: its own count.
+#ifndef KCIG_SUM_MINB_UNSHARED
+#define KCIG_SUM_MINB_UNSHARED KCIG_SUM_MINB
+#endif
+
 template <int TZ, int TX, int KB, bool SHARED_R, int MODE>
-__global__ void __launch_bounds__(TZ *TX, KCIG_SUM_MINB * 128 / (TZ * TX)) k_sum(const __grid_constant__ SumArgs a)
+__global__ void __launch_bounds__(TZ *TX, (SHARED_R ? KCIG_SUM_MINB : KCIG_SUM_MINB_UNSHARED) * 128 / (TZ * TX))
+    k_sum(const __grid_constant__ SumArgs a)
 {
     constexpr int P = TZ * TX;
     constexpr double kPiD = 3.141592653589793238463, kTwoPi = 6.283185307179586476925;

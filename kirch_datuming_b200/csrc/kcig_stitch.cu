@@ -171,13 +171,16 @@ extern "C" int kcig_stitch_window(float *out, int n1, int n2, int n3, const floa
 }
 
 // ------------------------------------------------- all windows, one pass --
-// The windows of one stitch in a single kernel: every output sample is
-// formed from the windows that cover its depth row, taken in window order
-// with exactly the per-window rule above (write; keep the upper value; or
-// blend), so the result equals the window-by-window calls bit for bit.  Each
-// window sample is read once and each output sample written once (rows no
-// window covers are written as 0): no read of the output, one launch, one
-// upload of the weights and one read-back of the counters.
+// The windows of one stitch in a single kernel.  Each warp owns an output
+// column (i3, i2) and keeps it in shared memory: zeroed, then every window
+// applied in order with exactly the per-window rule above (write; keep the
+// upper value; or blend), its lanes along the window's rows (each row of a
+// window has one lane, so a window's updates never collide), then written
+// out once.  The result equals the window-by-window calls on a zeroed volume
+// bit for bit (rows no window covers stay 0).  Each window sample is read
+// once and each output sample written once; the window records are
+// warp-uniform loads, once per column; one launch, one upload of the weights
+// and one read-back of the counters.
 namespace kcig {
 
 struct StitchWin {
@@ -189,44 +192,50 @@ struct StitchWin {
 struct StitchAllArgs {
     float *out;
     const StitchWin *win;     // [nwin]
-    const int *row_ptr;       // [n1 + 1]: windows covering row r are row_win[row_ptr[r] .. row_ptr[r+1])
-    const int *row_win;
-    const float *weights;     // blend weights of every window (at win.woff), then the lateral taper [n2]
-    const float *lateral;
+    const float *weights;     // blend weights of every window (at win.woff)
+    const float *lateral;     // lateral taper [n2], or null
     unsigned long long *nonfinite;  // [nwin]
     int n1, n2, n3, nwin;
 };
 
 __global__ void __launch_bounds__(256) k_stitch_all(const StitchAllArgs a)
 {
-    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    extern __shared__ float colbuf[];  // [warps][n1]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    float *buf = colbuf + (size_t)warp * a.n1;
     const int ncol = a.n2 * a.n3;
-    for (int col = blockIdx.x * warps + (threadIdx.x >> 5); col < ncol; col += gridDim.x * warps) {
+    for (int col = blockIdx.x * warps + warp; col < ncol; col += gridDim.x * warps) {
         const int i2 = col % a.n2;
         const float sx = a.lateral ? a.lateral[i2] : 1.0f;
-        float *dst = a.out + (size_t)col * a.n1;
-        for (int r = lane; r < a.n1; r += 32) {
-            float val = 0.0f;
-            for (int q = a.row_ptr[r]; q < a.row_ptr[r + 1]; q++) {
-                const int k = a.row_win[q];
-                const StitchWin &w = a.win[k];
-                const int i1 = r - w.start;
-                const float scale = __fmul_rn(w.scale, w.lateral ? sx : 1.0f);
-                float v = __fmul_rn(w.layer[(size_t)col * w.n1w + i1], scale);
+        for (int r = lane; r < a.n1; r += 32) buf[r] = 0.0f;
+        __syncwarp();
+        for (int k = 0; k < a.nwin; k++) {
+            const StitchWin w = a.win[k];
+            const float scale = __fmul_rn(w.scale, w.lateral ? sx : 1.0f);
+            const float *src = w.layer + (size_t)col * w.n1w;
+            unsigned long long bad = 0;
+            for (int i1 = lane; i1 < w.n1w; i1 += 32) {
+                float v = __fmul_rn(src[i1], scale);
                 if (!isfinite(v)) {
-                    atomicAdd(a.nonfinite + k, 1ull);
+                    ++bad;
                     v = 0.0f;
                 }
+                const int r = w.start + i1;
                 if (w.overlap > 0 && r <= w.previous_end) {
                     if (i1 < w.keep_upper || w.blend_count == 0) continue;
                     const float bw = a.weights[w.woff + i1 - w.keep_upper];
-                    val = __fadd_rn(__fmul_rn(val, __fsub_rn(1.0f, bw)), __fmul_rn(v, bw));
+                    buf[r] = __fadd_rn(__fmul_rn(buf[r], __fsub_rn(1.0f, bw)), __fmul_rn(v, bw));
                 } else {
-                    val = v;
+                    buf[r] = v;
                 }
             }
-            dst[r] = val;
+            for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
+            if (lane == 0 && bad) atomicAdd(a.nonfinite + k, bad);
+            __syncwarp();
         }
+        float *dst = a.out + (size_t)col * a.n1;
+        for (int r = lane; r < a.n1; r += 32) dst[r] = buf[r];
+        __syncwarp();
     }
 }
 
@@ -285,24 +294,16 @@ extern "C" int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin,
             wts.push_back(v);
         }
     }
-    // the windows covering each depth row, in window order
-    std::vector<int> row_ptr(n1 + 1, 0), row_win;
-    for (int r = 0; r < n1; r++) {
-        row_ptr[r] = (int)row_win.size();
-        for (int k = 0; k < nwin; k++)
-            if (r >= win[k].start && r < win[k].start + win[k].n1w) row_win.push_back(k);
-    }
-    row_ptr[n1] = (int)row_win.size();
-    // one staging upload: counters, window records, row lists, weights
+    // a column of the output per warp in shared memory
+    const size_t col_bytes = (size_t)n1 * sizeof(float);
+    if (col_bytes > 200 * 1024) return set_error(KCIG_ERR_ARG, "kcig_stitch_windows: n1=%d rows exceed one column buffer", n1);
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(8, (96 * 1024) / col_bytes));
+    // one staging upload: counters, window records, weights
     const size_t o_bad = 0, o_win = o_bad + (((size_t)nwin * 8 + 15) & ~(size_t)15);
-    const size_t o_ptr = o_win + (((size_t)nwin * sizeof(StitchWin) + 15) & ~(size_t)15);
-    const size_t o_rw = o_ptr + (((size_t)(n1 + 1) * 4 + 15) & ~(size_t)15);
-    const size_t o_w = o_rw + (((size_t)std::max<size_t>(1, row_win.size()) * 4 + 15) & ~(size_t)15);
+    const size_t o_w = o_win + (((size_t)nwin * sizeof(StitchWin) + 15) & ~(size_t)15);
     const size_t bytes = o_w + std::max<size_t>(1, wts.size()) * 4;
     std::vector<unsigned char> host(bytes, 0);
     memcpy(host.data() + o_win, win.data(), nwin * sizeof(StitchWin));
-    memcpy(host.data() + o_ptr, row_ptr.data(), (n1 + 1) * 4);
-    if (!row_win.empty()) memcpy(host.data() + o_rw, row_win.data(), row_win.size() * 4);
     if (!wts.empty()) memcpy(host.data() + o_w, wts.data(), wts.size() * 4);
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
@@ -321,8 +322,6 @@ extern "C" int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin,
         StitchAllArgs a;
         a.out = out;
         a.win = (const StitchWin *)(d + o_win);
-        a.row_ptr = (const int *)(d + o_ptr);
-        a.row_win = (const int *)(d + o_rw);
         a.weights = (const float *)(d + o_w);
         a.lateral = use_lateral ? a.weights + lat_off : nullptr;
         a.nonfinite = (unsigned long long *)(d + o_bad);
@@ -332,9 +331,12 @@ extern "C" int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin,
         a.nwin = nwin;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const size_t want = ((size_t)n2 * n3 + 7) / 8;
-        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 16));
-        k_stitch_all<<<grid, 256, 0, st>>>(a);
+        const int smem = (int)(warps * col_bytes);
+        int rc = set_dyn_smem((const void *)k_stitch_all, smem);
+        if (rc) return rc;
+        const size_t want = ((size_t)n2 * n3 + warps - 1) / warps;
+        const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 32));
+        k_stitch_all<<<grid, 32 * warps, smem, st>>>(a);
         e = cudaGetLastError();
     }
     std::vector<unsigned long long> bad(nwin, 0);
