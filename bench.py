@@ -868,6 +868,8 @@ def main():
     ap.add_argument("--no-stream", action="store_true", help="skip the host-resident-tables measurement")
     ap.add_argument("--large-grid-sample", action="store_true",
                     help="only the 1201x4001 grid sample with host-resident tables (one JSON object)")
+    ap.add_argument("--only-surrogate", action="store_true",
+                    help="run only the traveltime-surrogate section and print its object (profiling)")
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the uneven five-window workload and print its object (profiling)")
     ap.add_argument("--surrogate-steps", type=int, default=160000,
@@ -922,6 +924,11 @@ def main():
     if args.only_stitch:
         threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
         print(json.dumps({"stitch": stitch_section(args.steps, args.warmup, threads)}), flush=True)
+        return 0
+    if args.only_surrogate:
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        print(json.dumps({"surrogate": surrogate_section(args.surrogate_steps, args.steps, args.warmup, threads)}),
+              flush=True)
         return 0
     if args.only_batched:
         print(json.dumps({"batched": batched_section(args.steps, args.warmup, small=args.size == "small")}),
