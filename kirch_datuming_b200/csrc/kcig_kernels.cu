@@ -1365,6 +1365,12 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
     return KCIG_OK;
 }
 
+// Waves of resident CTAs a split summation aims for (a partial last wave
+// costs less the more waves there are; each split adds a partial image).
+#ifndef KCIG_SPLIT_WAVES
+#define KCIG_SPLIT_WAVES 2
+#endif
+
 int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
 {
     static int sms = 0;
@@ -1374,7 +1380,7 @@ int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
             sms = 148;
     }
     const long long tiles = (long long)((nz + 15) / 16) * ((nx + 7) / 8);
-    const long long want = 2LL * sms * KCIG_SUM_MINB;  // two waves of resident CTAs
+    const long long want = (long long)KCIG_SPLIT_WAVES * sms * KCIG_SUM_MINB;  // waves of resident CTAs
     if (tiles >= want) return 1;
     const int blocks = shared_r ? (nsb + KCIG_KB - 1) / KCIG_KB : (nsb + KCIG_KB_UNSHARED - 1) / KCIG_KB_UNSHARED;
     long long ns = (want + tiles - 1) / tiles;
