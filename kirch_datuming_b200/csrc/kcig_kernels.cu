@@ -500,24 +500,44 @@ constexpr int kGradTile = 32;
 // One box average along z (AXIS 0) or x (AXIS 1) of the local cells
 // [z0,z1) x [x0,x1), already clipped to the grid; the window is clamped to
 // the grid's local range [glo, ghi) of that axis.  rcp[k] = 1 / (k + 1).
+// Every cell of [z0,z1) x [x0,x1), walked by all threads of the block as one
+// flat range: consecutive threads take consecutive depths (rows stay
+// coalesced in shared memory) and no lane idles at the end of a row, as it
+// would with a row per 32 lanes on a halo tile 44 wide.  The column of flat
+// index q is q / nzr, taken exactly as a float product with the reciprocal:
+// (q + 0.5) / nzr lies at least 0.5 / nzr from an integer, far above the
+// float error for the tile sizes here (q < 2^20, nzr <= 1024).
+template <class F>
+__device__ __forceinline__ void for_cells(int z0, int z1, int x0, int x1, F f)
+{
+    const int nzr = z1 - z0, nxr = x1 - x0;
+    if (nzr <= 0 || nxr <= 0) return;
+    const int n = nzr * nxr;
+    const float inv = 1.0f / (float)nzr;
+    const int nthr = blockDim.x * blockDim.y;
+    for (int q = threadIdx.y * blockDim.x + threadIdx.x; q < n; q += nthr) {
+        const int cx = (int)(((float)q + 0.5f) * inv);
+        f(z0 + (q - cx * nzr), x0 + cx);
+    }
+}
+
 template <int AXIS>
 __device__ __forceinline__ void box_tile(const double *in0, double *out0, const double *in1, double *out1, int W,
                                          int s, int z0, int z1, int x0, int x1, int glo, int ghi, const double *rcp)
 {
-    for (int lx = x0 + (int)threadIdx.y; lx < x1; lx += blockDim.y)
-        for (int lz = z0 + (int)threadIdx.x; lz < z1; lz += blockDim.x) {
-            const int c = AXIS == 0 ? lz : lx;
-            const int a0 = max(c - s, glo), b0 = min(c + s, ghi - 1);
-            const int step = AXIS == 0 ? 1 : W;
-            const int base = AXIS == 0 ? lx * W + a0 : a0 * W + lz;
-            double s0 = 0.0, s1 = 0.0;
-            for (int k = 0; k <= b0 - a0; k++) {
-                s0 += in0[base + k * step];
-                s1 += in1[base + k * step];
-            }
-            out0[lx * W + lz] = s0 * rcp[b0 - a0];
-            out1[lx * W + lz] = s1 * rcp[b0 - a0];
+    for_cells(z0, z1, x0, x1, [&](int lz, int lx) {
+        const int c = AXIS == 0 ? lz : lx;
+        const int a0 = max(c - s, glo), b0 = min(c + s, ghi - 1);
+        const int step = AXIS == 0 ? 1 : W;
+        const int base = AXIS == 0 ? lx * W + a0 : a0 * W + lz;
+        double s0 = 0.0, s1 = 0.0;
+        for (int k = 0; k <= b0 - a0; k++) {
+            s0 += in0[base + k * step];
+            s1 += in1[base + k * step];
         }
+        out0[lx * W + lz] = s0 * rcp[b0 - a0];
+        out1[lx * W + lz] = s1 * rcp[b0 - a0];
+    });
 }
 
 __global__ void __launch_bounds__(256) k_leg_grad_fused(FieldArgs a, LegFields out)
@@ -538,12 +558,11 @@ __global__ void __launch_bounds__(256) k_leg_grad_fused(FieldArgs a, LegFields o
     double2 *TPo = out.TP + (size_t)blockIdx.y * nzx;
 
     // the traveltimes of the tile and its halo, all loads in flight at once
-    for (int lx = xlo + (int)threadIdx.y; lx < xhi; lx += blockDim.y)
-        for (int lz = zlo + (int)threadIdx.x; lz < zhi; lz += blockDim.x) {
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(P0 + lx * W + lz);
-            const double2 *src = TP + (size_t)(gx0 + lx) * nz + (gz0 + lz);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
-        }
+    for_cells(zlo, zhi, xlo, xhi, [&](int lz, int lx) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(P0 + lx * W + lz);
+        const double2 *src = TP + (size_t)(gx0 + lx) * nz + (gz0 + lz);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+    });
     for (int k = tid; k <= 2 * s; k += nthr) rcpb[k] = 1.0 / (double)(k + 1);
     for (int k = tid; k <= 2 * r; k += nthr) {
         rcpx[k] = k ? 1.0 / ((double)k * a.dx) : 0.0;
@@ -554,20 +573,19 @@ __global__ void __launch_bounds__(256) k_leg_grad_fused(FieldArgs a, LegFields o
 
     // centred differences on [r, W-r)^2: gx -> P1, gz -> P2
     const bool dox = nx > 1 && a.dx != 0.0f, doz = nz > 1 && a.dz != 0.0f;
-    for (int lx = max(r, xlo) + (int)threadIdx.y; lx < min(W - r, xhi); lx += blockDim.y)
-        for (int lz = max(r, zlo) + (int)threadIdx.x; lz < min(W - r, zhi); lz += blockDim.x) {
-            double vx = 0.0, vz = 0.0;
-            if (dox) {
-                const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
-                if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
-            }
-            if (doz) {
-                const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
-                if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
-            }
-            P1[lx * W + lz] = vx;
-            P2[lx * W + lz] = vz;
+    for_cells(max(r, zlo), min(W - r, zhi), max(r, xlo), min(W - r, xhi), [&](int lz, int lx) {
+        double vx = 0.0, vz = 0.0;
+        if (dox) {
+            const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
+            if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
         }
+        if (doz) {
+            const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
+            if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
+        }
+        P1[lx * W + lz] = vx;
+        P2[lx * W + lz] = vz;
+    });
     __syncthreads();
 
     if (s > 0) {
@@ -695,23 +713,20 @@ __global__ void __launch_bounds__(256, 3) k_leg_tile(FieldArgs a, LegFields out)
     // ---- interpolated traveltime (FP64) on the block and its halo
     double2 *TPo = out.TP + (size_t)blockIdx.y * nzx;
     const double hc0 = L.c[0], hc1 = L.c[1], hc2 = L.c[2], hc3 = L.c[3];
-    for (int lx = xlo + (int)threadIdx.y; lx < xhi; lx += blockDim.y) {
-        const float *c0 = stage + (size_t)(0 * W + lx) * SW + phs[0][lx] - zlo;
-        const float *c1 = stage + (size_t)(1 * W + lx) * SW + phs[1][lx] - zlo;
-        const float *c2 = two ? stage + (size_t)(2 * W + lx) * SW + phs[2][lx] - zlo : c0;
-        const float *c3 = two ? stage + (size_t)(3 * W + lx) * SW + phs[3][lx] - zlo : c1;
-        for (int lz = zlo + (int)threadIdx.x; lz < zhi; lz += blockDim.x) {
-            double T;
-            if (!two) {
-                T = c0[lz];
-            } else {
-                const double p0 = c0[lz], p1 = c2[lz];
-                const double m0 = c1[lz], m1 = c3[lz];
-                T = hc0 * p0 + hc1 * m0 + hc2 * p1 + hc3 * m1;
-            }
-            P0[lx * W + lz] = T;
+    for_cells(zlo, zhi, xlo, xhi, [&](int lz, int lx) {
+        const int o = lz - zlo;
+        double T;
+        if (!two) {
+            T = stage[(size_t)(0 * W + lx) * SW + phs[0][lx] + o];
+        } else {
+            const double p0 = stage[(size_t)(0 * W + lx) * SW + phs[0][lx] + o];
+            const double m0 = stage[(size_t)(1 * W + lx) * SW + phs[1][lx] + o];
+            const double p1 = stage[(size_t)(2 * W + lx) * SW + phs[2][lx] + o];
+            const double m1 = stage[(size_t)(3 * W + lx) * SW + phs[3][lx] + o];
+            T = hc0 * p0 + hc1 * m0 + hc2 * p1 + hc3 * m1;
         }
-    }
+        P0[lx * W + lz] = T;
+    });
     // ---- the block's own points, lanes aligned with its kGradTile rows (one
     // full warp pass per row): T, Tx and the aperture weight written
     {
@@ -742,20 +757,19 @@ __global__ void __launch_bounds__(256, 3) k_leg_tile(FieldArgs a, LegFields out)
 
     // ---- centred differences on [r, W-r)^2: gx -> P1, gz -> P2
     const bool dox = nx > 1 && a.dx != 0.0f, doz = nz > 1 && a.dz != 0.0f;
-    for (int lx = max(r, xlo) + (int)threadIdx.y; lx < min(W - r, xhi); lx += blockDim.y)
-        for (int lz = max(r, zlo) + (int)threadIdx.x; lz < min(W - r, zhi); lz += blockDim.x) {
-            double vx = 0.0, vz = 0.0;
-            if (dox) {
-                const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
-                if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
-            }
-            if (doz) {
-                const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
-                if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
-            }
-            P1[lx * W + lz] = vx;
-            P2[lx * W + lz] = vz;
+    for_cells(max(r, zlo), min(W - r, zhi), max(r, xlo), min(W - r, xhi), [&](int lz, int lx) {
+        double vx = 0.0, vz = 0.0;
+        if (dox) {
+            const int il = max(xlo, lx - r), ir = min(xhi - 1, lx + r);
+            if (ir != il) vx = (P0[ir * W + lz] - P0[il * W + lz]) * rcpx[ir - il];
         }
+        if (doz) {
+            const int it = max(zlo, lz - r), ib = min(zhi - 1, lz + r);
+            if (ib != it) vz = (P0[lx * W + ib] - P0[lx * W + it]) * rcpz[ib - it];
+        }
+        P1[lx * W + lz] = vx;
+        P2[lx * W + lz] = vz;
+    });
     __syncthreads();
     // ---- the four box passes (z, x, z, x; both components per pass), P0 and
     // P3 as scratch (the block's traveltimes are already written)
