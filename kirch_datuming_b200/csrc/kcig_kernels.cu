@@ -1379,10 +1379,15 @@ int launch_sum(const SumArgs &a0, cudaStream_t st, int *launches)
     return KCIG_OK;
 }
 
-// Waves of resident CTAs a split summation aims for (a partial last wave
-// costs less the more waves there are; each split adds a partial image).
+// A summation is split over shots only when its tiles fill fewer than
+// KCIG_SPLIT_BELOW waves of resident CTAs; it then aims for KCIG_SPLIT_WAVES
+// waves (a partial last wave costs less the more waves there are; each split
+// adds a partial image).
+#ifndef KCIG_SPLIT_BELOW
+#define KCIG_SPLIT_BELOW 2
+#endif
 #ifndef KCIG_SPLIT_WAVES
-#define KCIG_SPLIT_WAVES 2
+#define KCIG_SPLIT_WAVES 8
 #endif
 
 int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
@@ -1394,8 +1399,9 @@ int sum_nsplit(int nz, int nx, int nsb, bool shared_r)
             sms = 148;
     }
     const long long tiles = (long long)((nz + 15) / 16) * ((nx + 7) / 8);
-    const long long want = (long long)KCIG_SPLIT_WAVES * sms * KCIG_SUM_MINB;  // waves of resident CTAs
-    if (tiles >= want) return 1;
+    const long long slots = (long long)sms * KCIG_SUM_MINB;  // resident CTAs of one wave
+    if (tiles >= (long long)KCIG_SPLIT_BELOW * slots) return 1;
+    const long long want = (long long)KCIG_SPLIT_WAVES * slots;
     const int blocks = shared_r ? (nsb + KCIG_KB - 1) / KCIG_KB : (nsb + KCIG_KB_UNSHARED - 1) / KCIG_KB_UNSHARED;
     long long ns = (want + tiles - 1) / tiles;
     ns = std::min<long long>(ns, std::min(blocks, 64));
