@@ -12,6 +12,7 @@ container); the tests only read the committed outputs.
     python tests/golden/make_golden.py --eikods   # only the table-generator fixtures
     python tests/golden/make_golden.py --kirchmig2d  # only the plain-tool fixtures
     python tests/golden/make_golden.py --stitch   # only the ADCIG stitching fixtures
+    python tests/golden/make_golden.py --datum    # only the datuming fixtures
 """
 from __future__ import annotations
 
@@ -340,8 +341,132 @@ def stitch():
     print("wrote", os.path.join(HERE, "golden_stitch.npz"))
 
 
+# Datuming between depth levels: greensol_auto and kirchdat2d_freq
+# (oracle/_ref/kirchdat2d_freq is the reference tool linked against
+# oracle/fftw_dft.c), on the small five-layer salt model with tables every 10 m.
+DAT_NZ, DAT_NX, DAT_DATUM = 41, 81, 10
+DAT_NT, DAT_DT = 128, 0.004
+DAT_DATA = {
+    "cmp0": dict(ns=12, s0=0.2, ds=0.02, nh=24, h0=0.1, dh=0.02),
+    "cmp1": dict(ns=12, s0=0.25, ds=0.02, nh=16, h0=-0.12, dh=0.02),
+    "cmp1_jump": dict(ns=16, s0=0.25, ds=0.01, nh=12, h0=-0.1, dh=0.02),
+}
+DAT_CASES = {
+    "cmp0": dict(data="cmp0", interm=True, args=["cmp=0", "aperture=10", "taper=3", "data_taper=2", "antialias=1",
+                                                  "length=0.05", "use_bf=0"]),
+    "cmp0_workflow_bf": dict(data="cmp0", args=["aperture=200", "data_taper=20", "taper=0", "length=0.05", "cmp=0",
+                                                "antialias=1", "use_bf=1"]),
+    "cmp1": dict(data="cmp1", interm=True, args=["cmp=1", "aperture=5", "taper=2", "use_bf=0"]),
+    "cmp1_jump": dict(data="cmp1_jump", args=["cmp=1", "aperture=6", "taper=0", "data_taper=1", "use_bf=0"]),
+    "manual_datum": dict(data="cmp0", args=["cmp=0", "auto_datum=0", "sdatum=0.08", "rdatum=0.12",
+                                            "antialias=0.5", "length=0.03", "aperture=8", "taper=0", "use_bf=0"]),
+    "defaults": dict(data="cmp1", args=[]),
+}
+# (setup, arguments) of failing runs: exit code and ERROR text must match
+DAT_ERRORS = {
+    "no_input": ["output_file=o.rsf"],
+    "cmp": ["cmp=2"],
+    "auto_datum": ["auto_datum=2"],
+    "no_sdatum": ["auto_datum=0", "rdatum=0.1"],
+    "bf_p": ["bf_p=16", "bf_n_leaf=16"],
+    "bf_zero": ["bf_p=0"],
+    "data_taper": ["data_taper=-1"],
+    "antialias": ["antialias=-0.5"],
+    "small_table": ["input_file=d_wide.rsf"],
+    "no_should_datum": ["model_file=vel_nodatum.rsf"],
+    "input_2d": ["input_file=d_2d.rsf"],
+}
+GREEN_ERRORS = {
+    "no_ttabel": ["tgreen_file=g.rsf", "model_file=vel.rsf"],
+    "no_should_datum": ["ttabel_file=time.rsf", "tgreen_file=g.rsf", "model_file=vel_nodatum.rsf"],
+    "datum_range": ["ttabel_file=time.rsf", "tgreen_file=g.rsf", "model_file=vel_deep.rsf"],
+    "table_2d": ["ttabel_file=vel.rsf", "tgreen_file=g.rsf", "model_file=vel.rsf"],
+}
+
+
+def datum():
+    """greensol_auto + kirchdat2d_freq fixtures (golden_datum.npz, cases.json "datum")."""
+    with open(os.path.join(HERE, "cases.json")) as f:
+        meta = json.load(f)
+    v, _ = synth.five_layer_salt(DAT_NZ, DAT_NX, DZ, DZ)
+    out = {}
+    info = dict(nz=DAT_NZ, nx=DAT_NX, d=DZ, should_datum=DAT_DATUM, nt=DAT_NT, dt=DAT_DT, data=DAT_DATA,
+                cases={}, errors={}, green_errors={})
+    rng = np.random.default_rng(77)
+    with tempfile.TemporaryDirectory() as wd:
+        rsf.write(f"{wd}/vel.rsf", v, [DAT_NZ, DAT_NX], [0, 0], [DZ, DZ], extra={"should_datum": str(DAT_DATUM)})
+        rsf.write(f"{wd}/vel_nodatum.rsf", v, [DAT_NZ, DAT_NX], [0, 0], [DZ, DZ])
+        rsf.write(f"{wd}/vel_deep.rsf", v, [DAT_NZ, DAT_NX], [0, 0], [DZ, DZ], extra={"should_datum": "60"})
+        run([f"{REF}/shotgen", "shotfile=sht.rsf", f"nshot={DAT_NX}", "oy=0", f"dy={DZ}"], wd)
+        run([f"{REF}/eikods2d", "in=vel.rsf", "out=time.rsf", "shotfile=sht.rsf", "tdl1=tdl.rsf", "tds1=tds.rsf",
+             "b1=2", "b2=2"], wd)
+        h, t = rsf.read(f"{wd}/time.rsf")
+        out["vel"], out["table"] = v, t.reshape(h.n[2], h.n[1], h.n[0])
+        info["table"] = dict(n=h.n[:3], o=h.o[:3], d=h.d[:3])
+        log = run([f"{REF}/greensol_auto", "ttabel_file=time.rsf", "tgreen_file=green.rsf", "model_file=vel.rsf"], wd)
+        hg, g = rsf.read(f"{wd}/green.rsf", count=h.n[2] * h.n[2])
+        out["green"] = g.reshape(h.n[2], h.n[2])
+        with open(f"{wd}/green.rsf") as f:
+            info["green_header"] = f.read()
+        info["green_info"] = [l.split("INFO:", 1)[1] for l in log.splitlines()
+                              if "INFO:" in l and "INFO:greensol_auto " not in l]
+        for name, d in DAT_DATA.items():
+            x = rng.standard_normal((d["ns"], d["nh"], DAT_NT)).astype(np.float32)
+            x[d["ns"] // 2, d["nh"] // 3, DAT_NT // 2] += 25.0
+            out["data_" + name] = x
+            rsf.write(f"{wd}/d_{name}.rsf", x, [DAT_NT, d["nh"], d["ns"]], [0, d["h0"], d["s0"]],
+                      [DAT_DT, d["dh"], d["ds"]], extra={"label1": "Time", "unit1": "s"})
+        common = ["sgreen_file=green.rsf", "rgreen_file=green.rsf", "model_file=vel.rsf"]
+        for name, c in DAT_CASES.items():
+            args = [f"input_file=d_{c['data']}.rsf", "output_file=out.rsf"] + common + c["args"]
+            if c.get("interm"):
+                args.append("interm=interm.rsf")
+            log = run([f"{REF}/kirchdat2d_freq"] + args, wd)
+            d = DAT_DATA[c["data"]]
+            ho, o = rsf.read(f"{wd}/out.rsf")
+            out["out_" + name] = o.reshape(d["ns"], d["nh"], DAT_NT)
+            with open(f"{wd}/out.rsf") as f:
+                header = f.read()
+            rec = dict(data=c["data"], args=c["args"], header=header, interm=bool(c.get("interm")),
+                       info=[l.split("INFO:", 1)[1] for l in log.splitlines() if "INFO:" in l
+                             and "INFO:Processing " not in l and "Elapsed" not in l
+                             and "INFO:kirchdat2d_freq " not in l])
+            if c.get("interm"):
+                _, im = rsf.read(f"{wd}/interm.rsf", count=d["ns"] * d["nh"] * DAT_NT)
+                out["interm_" + name] = im.reshape(d["ns"], d["nh"], DAT_NT)
+                with open(f"{wd}/interm.rsf") as f:
+                    rec["interm_header"] = f.read()
+            info["cases"][name] = rec
+        # failing runs
+        wide = DAT_DATA["cmp0"]
+        rsf.write(f"{wd}/d_wide.rsf", np.zeros((4, 8, DAT_NT), np.float32), [DAT_NT, 8, 4], [0, 0.7, 0.2],
+                  [DAT_DT, 0.02, 0.02])
+        rsf.write(f"{wd}/d_2d.rsf", np.zeros((8, DAT_NT), np.float32), [DAT_NT, 8], [0, 0.1], [DAT_DT, 0.02])
+        base = ["input_file=d_cmp0.rsf", "output_file=o.rsf"] + common
+        for name, extra in DAT_ERRORS.items():
+            args = (base if name != "no_input" else common) + extra
+            r = subprocess.run([f"{REF}/kirchdat2d_freq"] + args, cwd=wd, capture_output=True, text=True)
+            assert r.returncode != 0, name
+            info["errors"][name] = dict(args=args, returncode=r.returncode,
+                                        error=[l.split("ERROR:", 1)[1] for l in r.stderr.splitlines()
+                                               if "ERROR:" in l])
+        for name, args in GREEN_ERRORS.items():
+            r = subprocess.run([f"{REF}/greensol_auto"] + args, cwd=wd, capture_output=True, text=True)
+            assert r.returncode != 0, name
+            info["green_errors"][name] = dict(args=args, returncode=r.returncode,
+                                              error=[l.split("ERROR:", 1)[1] for l in r.stderr.splitlines()
+                                                     if "ERROR:" in l])
+    meta["datum"] = info
+    np.savez_compressed(os.path.join(HERE, "golden_datum.npz"), **out)
+    with open(os.path.join(HERE, "cases.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", os.path.join(HERE, "golden_datum.npz"))
+
+
 if __name__ == "__main__":
-    if "--stitch" in sys.argv:
+    if "--datum" in sys.argv:
+        datum()
+    elif "--stitch" in sys.argv:
         stitch()
     elif "--forward" in sys.argv:
         forward()
