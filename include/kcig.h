@@ -436,6 +436,77 @@ int kcig_stitch_windows(float *out, int n1, int n2, int n3, int nwin, const floa
  * (the message printed to stderr). */
 int kcig_run_layercom_cig_cli(int argc, char **argv);
 
+/* ---- datuming between depth levels (greensol_auto, kirchdat2d_freq) ----- */
+
+/* The datum-depth slice of a traveltime table (src/greensol_auto.cpp:71-93):
+ * tgreen[igx1][igx2] = table[igx1][ix2][idatum], ix2 = (int)((ogx + igx2 dgx
+ * - ox) / dx + 0.5), idatum = (int)((datum - oz) / dz + 0.5), every index in
+ * the reference's float arithmetic.  table: [ngx][nx][nz], tgreen:
+ * [ngx][ngx], both host (memory = KCIG_MEM_HOST) or both device
+ * (KCIG_MEM_DEVICE: a gather kernel on `stream`, synchronous).  Errors:
+ * "Datum out of range.", "Receiver table too small." (KCIG_ERR_ARG). */
+int kcig_green_slice(const float *table, int nz, int nx, int ngx, float oz, float ox, float dz, float dx, float ogx,
+                     float dgx, float datum, float *tgreen, int memory, void *stream);
+
+/* Parameters of kirchdat2d_freq (src/kirchdat2d_frequency_cs.cpp:37-52 and
+ * :1177-1290).  The input cube is [ns][nh][nt] (time fastest) with axes
+ * (0, dt), (h0, dh), (s0, ds): h is the absolute receiver position when
+ * cmp = 0 and the offset when cmp = 1.  Green's tables are square,
+ * [nsg][nsg] (origin sg0, step dsg) and [nrg][nrg], indexed [cc][c] as the
+ * reference reads them.  use_bf and the bf_* values are validated as the
+ * reference validates them; the device always applies the exact operator
+ * that the reference's butterfly (use_bf = 1) approximates. */
+typedef struct kcig_datum_params {
+    int nt, nh, ns;
+    float dt, h0, dh, s0, ds;
+    int nsg, nrg;
+    float sg0, dsg, rg0, drg;
+    float sdatum, rdatum;
+    int aperture, taper, data_taper, cmp;
+    float antialias, length;
+    int use_bf, bf_p, bf_n_leaf, bf_panel_levels;
+    float bf_amp_eps, bf_phase_tol;
+} kcig_datum_params;
+
+/* The reference's defaults (:1215-1263): aperture 50, taper 10,
+ * data_taper 0, cmp 1, antialias 1, length 0.025, use_bf 1, bf_p 12,
+ * bf_n_leaf 16, bf_panel_levels 1, bf_amp_eps 1e-20, bf_phase_tol 2; every
+ * size and table field 0. */
+int kcig_datum_params_init(kcig_datum_params *p);
+
+/* FFT length and filter length of a run (:82-96, :1343-1346): nsam =
+ * (int)(length / dt) + 2, nfft = the next power of two >= nt + ceil(max tau /
+ * dt) + nsam. tables: host arrays. */
+int kcig_datum_sizes(const kcig_datum_params *p, const float *stable, const float *rtable, int *nsam, int *nfft);
+
+/* Datuming of one shot-gather cube from the recording surface to the datum
+ * (src/kirchdat2d_frequency_cs.cpp:1327-1392): each trace reversed in time,
+ * edge-tapered (data_taper) and transformed to nfft/2+1 frequencies; per
+ * frequency the receiver-side Kirchhoff sum (:493-546) and then the
+ * source-side sum (:548-672, the common-receiver walk for cmp = 1), each term
+ * w(aperture taper, distance) x anti-alias weight x H(tau, w); back to time,
+ * / nfft, reversed.  out: [ns][nh][nt]; interm (may be NULL): the
+ * receiver-side result [ns][nh][nt], not reversed (the reference's interm=).
+ * stable, rtable, in, out, interm: all host (KCIG_MEM_HOST) or all device
+ * (KCIG_MEM_DEVICE) memory.  Synchronous on `stream`.  Errors with the
+ * reference's texts ("cmp must be 0 or 1.", "Receiver table too small.",
+ * "Source table too small.", ...: KCIG_ERR_ARG), KCIG_ERR_NOMEM when the
+ * spectra do not fit the device. */
+int kcig_datum_freq(const kcig_datum_params *p, const float *stable, const float *rtable, const float *in, float *out,
+                    float *interm, int memory, void *stream);
+
+/* Device time of the stages of the last kcig_datum_freq call on this thread
+ * (ms): forward transforms, operator tables, receiver side, source side,
+ * inverse transforms; and the number of kernel launches of the call. */
+int kcig_datum_last_timing(float *ms5, int *launches);
+
+/* The drop-in greensol_auto (src/greensol_auto.cpp:23-101) and
+ * kirchdat2d_freq (src/kirchdat2d_frequency_cs.cpp:1177-1413): the same keys,
+ * defaults, checks, INFO lines, "ERROR:" texts and output headers.  Return 0
+ * or the KCIG_ERR_* code (the message printed to stderr). */
+int kcig_run_greensol_auto_cli(int argc, char **argv);
+int kcig_run_kirchdat2d_freq_cli(int argc, char **argv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,8 +153,30 @@ def lib():
         L.kcig_plan_last_timing.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]
         L.kcig_plan_last_prelude_ms.argtypes = [vp]
         L.kcig_plan_last_prelude_ms.restype = ctypes.c_float
+        DP = ctypes.POINTER(DatumParams)
+        L.kcig_datum_params_init.argtypes = [DP]
+        L.kcig_datum_sizes.argtypes = [DP, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.kcig_datum_freq.argtypes = [DP, vp, vp, vp, vp, vp, ctypes.c_int, vp]
+        L.kcig_datum_last_timing.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
+        L.kcig_green_slice.argtypes = ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 7
+                                       + [vp, ctypes.c_int, vp])
+        L.kcig_run_greensol_auto_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+        L.kcig_run_kirchdat2d_freq_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
         _lib = L
     return _lib
+
+
+class DatumParams(ctypes.Structure):
+    """kcig_datum_params (include/kcig.h): the settings of kirchdat2d_freq."""
+    _fields_ = [("nt", ctypes.c_int), ("nh", ctypes.c_int), ("ns", ctypes.c_int), ("dt", ctypes.c_float),
+                ("h0", ctypes.c_float), ("dh", ctypes.c_float), ("s0", ctypes.c_float), ("ds", ctypes.c_float),
+                ("nsg", ctypes.c_int), ("nrg", ctypes.c_int), ("sg0", ctypes.c_float), ("dsg", ctypes.c_float),
+                ("rg0", ctypes.c_float), ("drg", ctypes.c_float), ("sdatum", ctypes.c_float),
+                ("rdatum", ctypes.c_float), ("aperture", ctypes.c_int), ("taper", ctypes.c_int),
+                ("data_taper", ctypes.c_int), ("cmp", ctypes.c_int), ("antialias", ctypes.c_float),
+                ("length", ctypes.c_float), ("use_bf", ctypes.c_int), ("bf_p", ctypes.c_int),
+                ("bf_n_leaf", ctypes.c_int), ("bf_panel_levels", ctypes.c_int), ("bf_amp_eps", ctypes.c_float),
+                ("bf_phase_tol", ctypes.c_float)]
 
 
 def _check(rc: int):
@@ -655,3 +677,74 @@ class Graph:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------ datuming between depth levels
+
+def datum_params(**kw) -> DatumParams:
+    """kcig_datum_params with the reference's defaults, then the given fields."""
+    p = DatumParams()
+    _check(lib().kcig_datum_params_init(ctypes.byref(p)))
+    for k, v in kw.items():
+        if not any(f[0] == k for f in DatumParams._fields_):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def datum_sizes(p: DatumParams, stable, rtable):
+    """(nsam, nfft) of a run (kcig_datum_sizes); host float32 tables."""
+    st = np.ascontiguousarray(stable, np.float32)
+    rt = np.ascontiguousarray(rtable, np.float32)
+    nsam, nfft = ctypes.c_int(), ctypes.c_int()
+    _check(lib().kcig_datum_sizes(ctypes.byref(p), st.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                  rt.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(nsam),
+                                  ctypes.byref(nfft)))
+    return nsam.value, nfft.value
+
+
+def datum_freq(p: DatumParams, stable, rtable, data, out, interm=None, stream=None):
+    """kcig_datum_freq: data [ns][nh][nt] -> out (and interm) of the same shape.
+    All arrays host (contiguous float32 numpy) or all CUDA float32 tensors."""
+    ptrs = [_ptr(a) for a in (stable, rtable, data, out)]
+    kinds = {k for _, k in ptrs}
+    if interm is not None:
+        kinds.add(_ptr(interm)[1])
+    if len(kinds) != 1:
+        raise ValueError("datum_freq: all arrays host or all device")
+    for a in (stable, rtable, data, out) + ((interm,) if interm is not None else ()):
+        if isinstance(a, np.ndarray) and (a.dtype != np.float32 or not a.flags.c_contiguous):
+            raise ValueError("datum_freq: contiguous float32 arrays")
+    st = stream
+    if st is None and kinds == {MEM_DEVICE}:
+        import torch
+        st = torch.cuda.current_stream().cuda_stream
+    _check(lib().kcig_datum_freq(ctypes.byref(p), ptrs[0][0], ptrs[1][0], ptrs[2][0], ptrs[3][0],
+                                 _ptr(interm)[0] if interm is not None else None, kinds.pop(),
+                                 ctypes.c_void_p(st) if st else None))
+    return out
+
+
+def datum_last_timing():
+    """(forward, operators, receiver side, source side, inverse) ms and the
+    kernel launches of the last datum_freq call on this thread."""
+    ms = (ctypes.c_float * 5)()
+    n = ctypes.c_int()
+    _check(lib().kcig_datum_last_timing(ms, ctypes.byref(n)))
+    return list(ms), n.value
+
+
+def green_slice(table, nz: int, nx: int, ngx: int, oz: float, ox: float, dz: float, dx: float, ogx: float,
+                dgx: float, datum: float, out, stream=None):
+    """kcig_green_slice: tgreen [ngx][ngx] from a table [ngx][nx][nz] (both
+    host numpy or both CUDA tensors)."""
+    (tp, tk), (op, ok) = _ptr(table), _ptr(out)
+    if tk != ok:
+        raise ValueError("green_slice: table and output in the same memory")
+    st = stream
+    if st is None and tk == MEM_DEVICE:
+        import torch
+        st = torch.cuda.current_stream().cuda_stream
+    _check(lib().kcig_green_slice(tp, nz, nx, ngx, oz, ox, dz, dx, ogx, dgx, datum, op, tk,
+                                  ctypes.c_void_p(st) if st else None))
+    return out

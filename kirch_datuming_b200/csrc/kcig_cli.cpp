@@ -288,6 +288,14 @@ static int run_tool(int argc, char **argv, int tool)
     return KCIG_OK;
 }
 
-extern "C" int kcig_run_cli(int argc, char **argv) { return run_tool(argc, argv, 0); }
+extern "C" int kcig_run_cli(int argc, char **argv)
+{
+    rsf_set_program("kirchmig2d_cig");
+    return run_tool(argc, argv, 0);
+}
 
-extern "C" int kcig_run_kirchmig2d_cli(int argc, char **argv) { return run_tool(argc, argv, 1); }
+extern "C" int kcig_run_kirchmig2d_cli(int argc, char **argv)
+{
+    rsf_set_program("kirchmig2d");
+    return run_tool(argc, argv, 1);
+}

@@ -1,0 +1,1086 @@
+// Datuming between depth levels on the device: the frequency-domain
+// Kirchhoff extrapolation of the reference's kirchdat2d_freq
+// (src/kirchdat2d_frequency_cs.cpp) and the datum-depth slice of greensol_auto
+// (src/greensol_auto.cpp).
+//
+// Layout in HBM.  After the forward transforms the spectra are kept
+// frequency-major, U[iw][is][ih] (complex FP32): one ns x nh matrix per
+// frequency.  For cmp = 0 the receiver operator is the same for every shot
+// and the source operator the same for every receiver, so each side is one
+// complex matrix product per frequency:
+//     receiver side  Utmp[iw] = U[iw] . Kr[iw],   Kr[ic][ih]  (nh x nh)
+//     source side    Uout[iw] = Ks[iw] . Utmp[iw], Ks[is][ic]  (ns x ns)
+// (k_cgemm, batched over a chunk of frequencies, skipping the K tiles outside
+// the aperture band).  The operators of a chunk are built on the device
+// (k_dat_op): per term the weight of :508-523 (aperture taper, distance,
+// tau) precomputed on the host in the reference's arithmetic, times the
+// anti-aliasing weight (:197-226) and the filter H(tau, w) (:98-182), which is
+// evaluated in FP64 with exact phase reduction (the reference's FP32 phase
+// omega * m loses ~1e-3 rad at high frequencies).  For cmp = 1 the receiver
+// operator moves with the shot and the source side walks common-receiver
+// gathers (:556-619), so the sums run term by term (k_dat_rcv_cmp1,
+// k_dat_src_cmp1) over per-chunk tables of aH for the table pairs they use.
+// Transforms: cuFFT R2C / C2R of length nfft on batches of traces
+// (k_dat_prep reverses, tapers and pads; k_dat_finish scales, reverses and
+// trims), with tiled transposes between trace-major and frequency-major.
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <math.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "kcig_common.h"
+
+namespace kcig {
+namespace {
+
+constexpr int kFilterMax = 64;  // filter samples kept in registers / local memory
+
+struct DatEntry {
+    float w;     // term weight before the anti-alias weight (0: no term)
+    float tau;   // table traveltime of the term
+    float dtau;  // |slope| x coordinate step, the anti-alias phase increment
+};
+
+struct DatOpArgs {
+    const DatEntry *ent;
+    int ne;
+    float2 *out;  // [nf][ne]
+    int f0, nf, nfft, K;
+    float dt, antialias;
+};
+
+// antialias_weight_iw (:197-226), in the reference's float arithmetic
+__device__ __forceinline__ float dat_aa(float antialias, int iw, float dtau, int nfft, float dt)
+{
+    if (antialias <= 0.0f || iw <= 0) return 1.0f;
+    dtau = __fmul_rn(fabsf(dtau), antialias);
+    if (dtau <= 1e-12f || !isfinite(dtau)) return 1.0f;
+    const float freq = __fdiv_rn((float)iw, __fmul_rn((float)nfft, dt));
+    const float fnyq = __fdiv_rn(0.5f, dt);
+    const float fmax = __fdiv_rn(0.5f, dtau);
+    if (fmax >= fnyq) return 1.0f;
+    if (fmax <= 0.0f) return 0.0f;
+    const float fpass = __fmul_rn(0.8f, fmax);
+    if (freq <= fpass) return 1.0f;
+    if (freq >= fmax) return 0.0f;
+    const float x = __fdiv_rn(__fsub_rn(freq, fpass), __fsub_rn(fmax, fpass));
+    return __fmul_rn(0.5f, __fadd_rn(1.0f, cospif(x)));
+}
+
+// sqrt(t^2 - 1) for t = 1 + u, written without the cancellation of t^2 - 1
+__device__ __forceinline__ double dat_root(int j, double dt_over_tau)
+{
+    if (j < 0) return 0.0;
+    const double u = (double)(j + 1) * dt_over_tau;
+    return sqrt(u * (2.0 + u));
+}
+
+// One thread per operator term, looping over the chunk's frequencies:
+// out[c][e] = w aa(iw) H(tau, iw), H = lin . sum_k F[k]/dt exp(-i w k) with
+// F the second differences of sqrt(t^2 - 1) (build_filter_F, :98-116), lin =
+// (1-delta) exp(-i w m) + delta exp(-i w (m-1)), m = ceil(tau/dt) (:128-181).
+__global__ void __launch_bounds__(128) k_dat_op(const DatOpArgs a)
+{
+    extern __shared__ double zs[];  // [nf][2]: cos w, sin w of the chunk's frequencies
+    for (int c = threadIdx.x; c < a.nf; c += blockDim.x) {
+        double s, co;
+        sincospi(2.0 * (double)(a.f0 + c) / (double)a.nfft, &s, &co);
+        zs[2 * c] = co;
+        zs[2 * c + 1] = s;
+    }
+    __syncthreads();
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.ne) return;
+    const DatEntry d = a.ent[e];
+    float2 *o = a.out + e;
+    if (d.w == 0.0f || !(d.tau > 0.0f) || !isfinite(d.tau) || a.K <= 0) {
+        for (int c = 0; c < a.nf; c++) o[(size_t)c * a.ne] = make_float2(0.0f, 0.0f);
+        return;
+    }
+    const double r = (double)a.dt / (double)d.tau, inv_dt = 1.0 / (double)a.dt;
+    const int K = a.K;
+    double F[kFilterMax];
+    const bool cached = K <= kFilterMax;
+    if (cached) {
+        double p2 = 0.0, p1 = 0.0;
+        for (int k = 0; k < K; k++) {
+            const double ck = dat_root(k, r);
+            F[k] = (ck - 2.0 * p1 + p2) * inv_dt;
+            p2 = p1;
+            p1 = ck;
+        }
+    }
+    const double q = (double)d.tau * inv_dt, mceil = ceil(q), delta = mceil - q;
+    const long long m = (long long)mceil;
+    for (int c = 0; c < a.nf; c++) {
+        const int iw = a.f0 + c;
+        const float wa = __fmul_rn(d.w, dat_aa(a.antialias, iw, d.dtau, a.nfft, a.dt));
+        if (fabsf(wa) < 1e-20f) {  // the reference skips these terms (:525)
+            o[(size_t)c * a.ne] = make_float2(0.0f, 0.0f);
+            continue;
+        }
+        const double zr = zs[2 * c], zi = zs[2 * c + 1];  // exp(-i w) = zr - i zi
+        // Horner from the last filter sample down: S = ((F[K-1] z + F[K-2]) z + ...) z + F[0]
+        double sr, si = 0.0;
+        if (cached) {
+            sr = F[K - 1];
+            for (int k = K - 2; k >= 0; k--) {
+                const double tr = sr * zr + si * zi, ti = si * zr - sr * zi;
+                sr = tr + F[k];
+                si = ti;
+            }
+        } else {  // long filters: the samples from three running roots
+            double c0 = dat_root(K - 1, r), c1 = dat_root(K - 2, r), c2 = dat_root(K - 3, r);
+            sr = (c0 - 2.0 * c1 + c2) * inv_dt;
+            for (int k = K - 2; k >= 0; k--) {
+                c0 = c1;
+                c1 = c2;
+                c2 = dat_root(k - 2, r);
+                const double tr = sr * zr + si * zi, ti = si * zr - sr * zi;
+                sr = tr + (c0 - 2.0 * c1 + c2) * inv_dt;
+                si = ti;
+            }
+        }
+        // exp(-i w m) with the phase reduced exactly: (iw m) mod nfft
+        const long long red = ((long long)iw * m) % (long long)a.nfft;
+        float es, ec;
+        sincospif(__fdiv_rn(2.0f * (float)red, (float)a.nfft), &es, &ec);
+        const double lr = (1.0 - delta) + delta * zr, li = delta * zi;  // (1-delta) + delta exp(+i w)
+        const double mr = (double)ec * lr + (double)es * li, mi = (double)ec * li - (double)es * lr;
+        const double hr = mr * sr - mi * si, hi = mr * si + mi * sr;
+        o[(size_t)c * a.ne] = make_float2((float)(wa * hr), (float)(wa * hi));
+    }
+}
+
+// Batched complex GEMM, FP32: C[z] = A[z] . B[z] (row-major, complex
+// interleaved), 64x64 tiles of C per CTA, 4x4 per thread, K in steps of 8.
+// band >= 0: the nonzero terms satisfy |k - m| <= band (band_rows) or
+// |k - n| <= band, so a tile reads only the K range that can touch it.
+struct CGemmArgs {
+    const float2 *A;
+    const float2 *B;
+    float2 *C;
+    long long sA, sB, sC;  // batch strides (elements)
+    int lda, ldb, ldc;
+    int M, N, K;
+    int band, band_rows;
+};
+
+__global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
+{
+    constexpr int BM = 64, BN = 64, BK = 8;
+    __shared__ __align__(16) float2 As[BK][BM + 2];
+    __shared__ __align__(16) float2 Bs[BK][BN + 2];
+    const int z = blockIdx.z;
+    const float2 *A = a.A + (size_t)z * a.sA;
+    const float2 *B = a.B + (size_t)z * a.sB;
+    float2 *C = a.C + (size_t)z * a.sC;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    int k_lo = 0, k_hi = a.K;
+    if (a.band >= 0) {
+        const int c0 = a.band_rows ? m0 : n0, c1 = (a.band_rows ? min(a.M, m0 + BM) : min(a.N, n0 + BN)) - 1;
+        k_lo = max(0, c0 - a.band);
+        k_hi = min(a.K, c1 + a.band + 1);
+    }
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    float ar[4][4], ai[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) ar[i][j] = ai[i][j] = 0.0f;
+    for (int k0 = k_lo; k0 < k_hi; k0 += BK) {
+#pragma unroll
+        for (int rr = 0; rr < 2; rr++) {
+            const int e = tid + 256 * rr;
+            const int mm = e >> 3, kk = e & 7, gm = m0 + mm, gk = k0 + kk;
+            As[kk][mm] = (gm < a.M && gk < k_hi) ? A[(size_t)gm * a.lda + gk] : make_float2(0.0f, 0.0f);
+            const int kb = e >> 6, nn = e & 63, gkb = k0 + kb, gn = n0 + nn;
+            Bs[kb][nn] = (gkb < k_hi && gn < a.N) ? B[(size_t)gkb * a.ldb + gn] : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk++) {
+            const float4 a01 = *reinterpret_cast<const float4 *>(&As[kk][ty * 4]);
+            const float4 a23 = *reinterpret_cast<const float4 *>(&As[kk][ty * 4 + 2]);
+            const float4 b01 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4]);
+            const float4 b23 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4 + 2]);
+            const float xr[4] = {a01.x, a01.z, a23.x, a23.z}, xi[4] = {a01.y, a01.w, a23.y, a23.w};
+            const float yr[4] = {b01.x, b01.z, b23.x, b23.z}, yi[4] = {b01.y, b01.w, b23.y, b23.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    ar[i][j] = fmaf(xr[i], yr[j], ar[i][j]);
+                    ar[i][j] = fmaf(-xi[i], yi[j], ar[i][j]);
+                    ai[i][j] = fmaf(xr[i], yi[j], ai[i][j]);
+                    ai[i][j] = fmaf(xi[i], yr[j], ai[i][j]);
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int gm = m0 + ty * 4 + i;
+        if (gm >= a.M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int gn = n0 + tx * 4 + j;
+            if (gn < a.N) C[(size_t)gm * a.ldc + gn] = make_float2(ar[i][j], ai[i][j]);
+        }
+    }
+}
+
+// cmp = 1 receiver side (:493-546 with s_abs = s0 + is ds): one thread per
+// (frequency, shot, trace), the sum over the aperture of
+// geom[ih][ic] tau (aH)[pair], pair = (table row cc = cabs[is][ic], column
+// c = cabs[is][ih]) looked up in the chunk's band table P[c][row][j],
+// j = c - cc + band.
+struct RcvCmp1Args {
+    const float2 *U;   // [nf][ns][nh] (the chunk's input spectra)
+    float2 *Utmp;      // [nf][ns][nh]
+    const float2 *P;   // [nf][nrow * (2 band + 1)]
+    const float *Ptau; // [nrow * (2 band + 1)]
+    const int *cabs;   // [ns][nh]
+    const float *geom; // [nh][nh]
+    int ns, nh, aper, band, row0, nrow;
+    long long sU;      // U batch stride
+};
+
+__global__ void __launch_bounds__(128) k_dat_rcv_cmp1(const RcvCmp1Args a)
+{
+    const int tr = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    const int ntr = a.ns * a.nh;
+    if (tr >= ntr) return;
+    const int is = tr / a.nh, ih = tr - is * a.nh;
+    const float2 *U = a.U + (size_t)c * a.sU + (size_t)is * a.nh;
+    const int wid = 2 * a.band + 1;
+    const float2 *P = a.P + (size_t)c * a.nrow * wid;
+    const int cih = a.cabs[tr];
+    float sr = 0.0f, si = 0.0f;
+    const int left = max(0, ih - a.aper), right = min(a.nh - 1, ih + a.aper);
+    for (int ic = left; ic <= right; ic++) {
+        const float g = a.geom[(size_t)ih * a.nh + ic];
+        if (g == 0.0f) continue;
+        const int cc = a.cabs[(size_t)is * a.nh + ic];
+        const size_t pi = (size_t)(cc - a.row0) * wid + (cih - cc + a.band);
+        const float w = __fmul_rn(g, a.Ptau[pi]);
+        const float2 h = P[pi], u = U[ic];
+        sr = fmaf(w, u.x * h.x - u.y * h.y, sr);
+        si = fmaf(w, u.x * h.y + u.y * h.x, si);
+    }
+    a.Utmp[(size_t)c * ntr + tr] = make_float2(sr, si);
+}
+
+// cmp = 1 source side (:556-619): one thread per (frequency, shot); it walks
+// the common-receiver gathers r that hold the shot (ir in [ir_lo, ir_hi]),
+// and adds the sum over the gather's neighbouring shots to its own trace
+// ih(r) of the output, so every output row has one writer and a fixed order.
+struct SrcCmp1Args {
+    const float2 *Utmp;  // [nf][ns][nh]
+    float2 *Uout;        // [nf][ns][nh] (zeroed)
+    const float2 *P;     // [nf][ns][ns]: aH of pair (c_s[ic], c_s[is]) at [is][ic]
+    const float *Ptau;   // [ns][ns]
+    const int *sleft, *sright;  // [nr] the gather's shot range
+    const int *ihmap;    // [nr][ns]: trace of shot is in gather r, -1 outside
+    const int *ir_lo, *ir_hi;   // [ns]
+    int ns, nh, nr, aper, jump, tap;
+    float ds, sdatum;
+    long long sUout;
+};
+
+__device__ __forceinline__ float dat_taper(int left, int center, int right, int tap, int stride)
+{
+    if (center < left || center > right) return 0.0f;
+    if (tap <= 0) return 1.0f;
+    if (stride < 1) stride = 1;
+    const float width = __fmul_rn((float)tap, (float)stride);
+    const float ul = fminf(1.0f, fmaxf(0.0f, __fdiv_rn((float)(center - left), width)));
+    const float ur = fminf(1.0f, fmaxf(0.0f, __fdiv_rn((float)(right - center), width)));
+    return __fmul_rn(__fmul_rn(__fmul_rn(0.5f, __fsub_rn(1.0f, cospif(ul))), 0.5f), __fsub_rn(1.0f, cospif(ur)));
+}
+
+__global__ void __launch_bounds__(128) k_dat_src_cmp1(const SrcCmp1Args a)
+{
+    const int is = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    if (is >= a.ns) return;
+    const int ntr = a.ns * a.nh;
+    const float2 *Ut = a.Utmp + (size_t)c * ntr;
+    float2 *Uo = a.Uout + (size_t)c * a.sUout + (size_t)is * a.nh;
+    const float2 *P = a.P + (size_t)c * a.ns * a.ns + (size_t)is * a.ns;
+    const float *Pt = a.Ptau + (size_t)is * a.ns;
+    const double kw = (double)a.ds * (double)a.sdatum / 3.14159265358979323846;
+    for (int ir = a.ir_lo[is]; ir <= a.ir_hi[is]; ir++) {
+        const int sl = a.sleft[ir], sr = a.sright[ir];
+        if (is < sl || is > sr || (is - sl) % a.jump) continue;
+        const int ih = a.ihmap[(size_t)ir * a.ns + is];
+        if (ih < 0) continue;
+        const int il = max(sl, is - a.jump * a.aper), iu = min(sr, is + a.jump * a.aper);
+        float accr = 0.0f, acci = 0.0f;
+        for (int ic = il; ic <= iu; ic += a.jump) {
+            const int hh = a.ihmap[(size_t)ir * a.ns + ic];
+            if (hh < 0) continue;
+            const float coef = dat_taper(il, ic, iu, a.tap, a.jump);
+            const float dist = __fadd_rn(__fmul_rn(a.sdatum, a.sdatum),
+                                         __fmul_rn(__fmul_rn((float)((ic - is) * (ic - is)), a.ds), a.ds));
+            const float w = (float)((double)coef * kw * (double)Pt[ic] / (double)dist);
+            const float2 h = P[ic], u = Ut[(size_t)ic * a.nh + hh];
+            accr = fmaf(w, u.x * h.x - u.y * h.y, accr);
+            acci = fmaf(w, u.x * h.y + u.y * h.x, acci);
+        }
+        float2 o = Uo[ih];
+        o.x += accr;
+        o.y += acci;
+        Uo[ih] = o;
+    }
+}
+
+// reverse in time, edge taper and zero-pad one batch of traces (:287-306)
+__global__ void k_dat_prep(const float *in, const float *wtr, float *pad, int tr0, int nb, int nt, int nfft)
+{
+    const size_t n = (size_t)nb * nfft;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(i / nfft), t = (int)(i - (size_t)b * nfft);
+        float v = 0.0f;
+        if (t < nt) {
+            const float w = wtr[tr0 + b];
+            const float x = in[(size_t)(tr0 + b) * nt + (nt - 1 - t)];
+            v = w == 1.0f ? x : __fmul_rn(w, x);
+        }
+        pad[i] = v;
+    }
+}
+
+// scale by 1/nfft, optionally reverse, trim to nt (:476-487)
+__global__ void k_dat_finish(const float *pad, float *out, int tr0, int nb, int nt, int nfft, float scale, int reverse)
+{
+    const size_t n = (size_t)nb * nt;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(i / nt), t = (int)(i - (size_t)b * nt);
+        out[(size_t)(tr0 + b) * nt + t] = __fmul_rn(pad[(size_t)b * nfft + (reverse ? nt - 1 - t : t)], scale);
+    }
+}
+
+// tiled transposes between spec[b][nw] (a batch of traces) and U[iw][ntr]
+__global__ void k_dat_to_fmajor(const float2 *spec, float2 *U, int tr0, int nb, int nw, int ntr)
+{
+    __shared__ float2 tile[32][33];
+    const int w0 = blockIdx.x * 32, b0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int b = b0 + r, w = w0 + threadIdx.x;
+        if (b < nb && w < nw) tile[r][threadIdx.x] = spec[(size_t)b * nw + w];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int w = w0 + r, b = b0 + threadIdx.x;
+        if (b < nb && w < nw) U[(size_t)w * ntr + tr0 + b] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void k_dat_to_tmajor(const float2 *U, float2 *spec, int tr0, int nb, int nw, int ntr)
+{
+    __shared__ float2 tile[32][33];
+    const int w0 = blockIdx.y * 32, b0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int w = w0 + r, b = b0 + threadIdx.x;
+        if (b < nb && w < nw) tile[r][threadIdx.x] = U[(size_t)w * ntr + tr0 + b];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int b = b0 + r, w = w0 + threadIdx.x;
+        if (b < nb && w < nw) spec[(size_t)b * nw + w] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void k_green_gather(const float *table, const int *ix, float *out, int ngx, int nx, int nz, int idatum)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ngx * ngx) return;
+    const int i1 = i / ngx, i2 = i - i1 * ngx;
+    out[i] = table[((size_t)i1 * nx + ix[i2]) * nz + idatum];
+}
+
+// ------------------------------------------------------------ host side --
+
+// the reference's float arithmetic for indices and weights (x86-64 SSE, no
+// contraction): every operation below rounds to float as it does there
+inline int f2i(float x) { return (int)x; }
+
+float taper_host(int left, int center, int right, int tap, int stride)  // taper_weight (:229-240)
+{
+    if (center < left || center > right) return 0.0f;
+    if (tap <= 0) return 1.0f;
+    if (stride < 1) stride = 1;
+    const float width = (float)tap * (float)stride;
+    const float ul = fminf(1.0f, fmaxf(0.0f, (float)(center - left) / width));
+    const float ur = fminf(1.0f, fmaxf(0.0f, (float)(right - center) / width));
+    return 0.5f * (1.0f - cosf((float)M_PI * ul)) * 0.5f * (1.0f - cosf((float)M_PI * ur));
+}
+
+float edge_host(int i, int n, int tap)  // data_edge_taper_weight (:255-279)
+{
+    if (tap <= 0 || n <= 1) return 1.0f;
+    int ntap = tap;
+    const int max_tap = (n - 1) / 2;
+    if (ntap > max_tap) ntap = max_tap;
+    if (ntap <= 0) return 1.0f;
+    if (i < ntap) return 0.5f * (1.0f - cosf((float)M_PI * ((float)i / (float)ntap)));
+    if (i > n - 1 - ntap) return 0.5f * (1.0f - cosf((float)M_PI * ((float)(n - 1 - i) / (float)ntap)));
+    return 1.0f;
+}
+
+float slope_host(const float *t, int n, int row, int col, float dcoord)  // :184-194, t[row][col] row-major n x n
+{
+    if (n <= 1 || dcoord == 0.0f) return 0.0f;
+    if (row <= 0) return (t[(size_t)1 * n + col] - t[col]) / dcoord;
+    if (row >= n - 1) return (t[(size_t)(n - 1) * n + col] - t[(size_t)(n - 2) * n + col]) / dcoord;
+    return 0.5f * (t[(size_t)(row + 1) * n + col] - t[(size_t)(row - 1) * n + col]) / dcoord;
+}
+
+int rcv_index(const kcig_datum_params &p, int is, int ih)  // :502, :507
+{
+    const float s = p.cmp ? p.s0 + (float)is * p.ds : 0.0f;
+    return f2i((s + p.h0 + (float)ih * p.dh - p.rg0) / p.drg + 0.5f);
+}
+
+int src_index(const kcig_datum_params &p, int is)  // :583, :638
+{
+    return f2i((p.s0 + (float)is * p.ds - p.sg0) / p.dsg + 0.5f);
+}
+
+// w = coef / M_PI * d * datum * tau / dist, in double as written, then float
+float term_weight(float coef, float d, float datum, float tau, float dist)
+{
+    return (float)(coef / M_PI * d * datum * tau / dist);
+}
+
+struct Stage {
+    cudaEvent_t ev[6] = {};
+};
+
+thread_local float g_last_ms[5] = {0, 0, 0, 0, 0};
+thread_local int g_last_launches = 0;
+
+struct DBuf {
+    void *p = nullptr;
+    ~DBuf()
+    {
+        if (p) cudaFree(p);
+    }
+    template <class T>
+    T *as() const
+    {
+        return (T *)p;
+    }
+};
+
+int dalloc(DBuf &b, size_t bytes, const char *what)
+{
+    if (bytes == 0) bytes = 16;
+    const cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return set_error(KCIG_ERR_NOMEM, "kcig_datum_freq: cannot allocate %.3f GB for %s on the device",
+                         bytes / 1e9, what);
+    }
+    return KCIG_OK;
+}
+
+template <class T>
+int upload(DBuf &b, const std::vector<T> &v, cudaStream_t st, const char *what)
+{
+    KCIG_TRY(dalloc(b, v.size() * sizeof(T), what));
+    if (!v.empty()) KCIG_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return KCIG_OK;
+}
+
+struct CufftPlan {
+    cufftHandle h = 0;
+    bool ok = false;
+    ~CufftPlan()
+    {
+        if (ok) cufftDestroy(h);
+    }
+};
+
+int cufft_error(cufftResult r, const char *what)
+{
+    return set_error(KCIG_ERR_CUDA, "%s failed: cufftResult %d", what, (int)r);
+}
+
+int validate(const kcig_datum_params &p)
+{
+    if (p.cmp != 0 && p.cmp != 1) return set_error(KCIG_ERR_ARG, "cmp must be 0 or 1.");
+    if (p.bf_p <= 0 || p.bf_n_leaf <= 1) return set_error(KCIG_ERR_ARG, "Need bf_p > 0 and bf_n_leaf > 1.");
+    if (p.bf_p >= p.bf_n_leaf)
+        return set_error(KCIG_ERR_ARG,
+                         "Need bf_p < bf_n_leaf for meaningful butterfly interpolation / exact leaf-stage settings.");
+    if (p.data_taper < 0) return set_error(KCIG_ERR_ARG, "data_taper must be >= 0.");
+    if (!(p.antialias >= 0.0f)) return set_error(KCIG_ERR_ARG, "antialias must be >= 0.");
+    if (p.nt <= 0 || p.nh <= 0 || p.ns <= 0 || p.nsg <= 0 || p.nrg <= 0)
+        return set_error(KCIG_ERR_ARG, "kcig_datum_freq: sizes must be positive");
+    if (!(p.dt > 0.0f)) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: dt must be positive");
+    if ((long long)p.ns * p.nh > 0x7fffffffLL) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: too many traces");
+    return KCIG_OK;
+}
+
+int sizes(const kcig_datum_params &p, const float *st, const float *rt, int *nsam_out, int *nfft_out)
+{
+    const float ratio = p.length / p.dt;
+    if (!(fabsf(ratio) < 1e8f)) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: length / dt out of range");
+    const int nsam = f2i(ratio) + 2;
+    float max_tau = 0.0f;  // choose_nfft (:82-96)
+    for (size_t i = 0; i < (size_t)p.nrg * p.nrg; i++)
+        if (rt[i] > max_tau) max_tau = rt[i];
+    for (size_t i = 0; i < (size_t)p.nsg * p.nsg; i++)
+        if (st[i] > max_tau) max_tau = st[i];
+    const float steps = ceilf(max_tau / p.dt);
+    if (!(steps < 5e8f)) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: table traveltimes too long for an FFT");
+    const long long need = (long long)p.nt + (long long)steps + (nsam - 2) + 2;
+    long long n = 1;
+    while (n < need) n <<= 1;
+    if (n > (1LL << 30)) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: nfft %lld too large", n);
+    *nsam_out = nsam;
+    *nfft_out = (int)n;
+    return KCIG_OK;
+}
+
+// Operator terms of one side in the reference's arithmetic.  Dense matrices
+// of DatEntry: receiver (cmp 0) at [ic][ih] (the K x N operand), source
+// (cmp 0) at [is][ic]; for cmp = 1, the band table of receiver pairs and the
+// source pair matrix, whose entries carry w = 1 (the geometric factor is
+// applied by the sums).
+struct Host {
+    std::vector<DatEntry> rcv, src;
+    // cmp = 1 receiver side
+    std::vector<int> cabs;        // [ns][nh]
+    std::vector<float> geom, rtau;  // [nh][nh], [nrow][2 band + 1]
+    int band = 0, row0 = 0, nrow = 0;
+    // cmp = 1 source side
+    std::vector<float> stau;  // [ns][ns]
+    std::vector<int> sleft, sright, ihmap, ir_lo, ir_hi;
+    int nr = 0, jump = 1;
+};
+
+int build_receiver(const kcig_datum_params &p, const float *rt, Host &h)
+{
+    const int nh = p.nh, ns = p.ns, aper = p.aperture, nrg = p.nrg;
+    if (p.cmp == 0) {
+        h.rcv.assign((size_t)nh * nh, DatEntry{0.0f, 0.0f, 0.0f});
+        for (int ih = 0; ih < nh; ih++) {
+            const int c = rcv_index(p, 0, ih);
+            const int left = std::max(0, ih - aper), right = std::min(nh - 1, ih + aper);
+            for (int ic = left; ic <= right; ic++) {
+                const int cc = rcv_index(p, 0, ic);
+                if (c < 0 || c >= nrg || cc < 0 || cc >= nrg) return set_error(KCIG_ERR_ARG, "Receiver table too small.");
+                const float coef = taper_host(left, ic, right, p.taper, 1);
+                const float tau = rt[(size_t)cc * nrg + c];
+                const float dist = p.rdatum * p.rdatum + (float)((ic - ih) * (ic - ih)) * p.dh * p.dh;
+                DatEntry &e = h.rcv[(size_t)ic * nh + ih];
+                e.w = term_weight(coef, p.dh, p.rdatum, tau, dist);
+                e.tau = tau;
+                e.dtau = slope_host(rt, nrg, cc, c, p.drg) * fabsf(p.dh);
+            }
+        }
+        return KCIG_OK;
+    }
+    h.cabs.resize((size_t)ns * nh);
+    int lo = 0x7fffffff, hi = -0x7fffffff - 1;
+    for (int is = 0; is < ns; is++)
+        for (int ih = 0; ih < nh; ih++) {
+            const int c = rcv_index(p, is, ih);
+            h.cabs[(size_t)is * nh + ih] = c;
+            if (aper >= 0 && (c < 0 || c >= nrg)) return set_error(KCIG_ERR_ARG, "Receiver table too small.");
+            lo = std::min(lo, c);
+            hi = std::max(hi, c);
+        }
+    h.geom.assign((size_t)nh * nh, 0.0f);
+    int band = 0;
+    for (int ih = 0; ih < nh; ih++) {
+        const int left = std::max(0, ih - aper), right = std::min(nh - 1, ih + aper);
+        for (int ic = left; ic <= right; ic++) {
+            const float coef = taper_host(left, ic, right, p.taper, 1);
+            const float dist = p.rdatum * p.rdatum + (float)((ic - ih) * (ic - ih)) * p.dh * p.dh;
+            h.geom[(size_t)ih * nh + ic] = (float)(coef / M_PI * p.dh * p.rdatum / dist);
+        }
+        for (int is = 0; is < ns && left <= right; is++) {
+            const int c = h.cabs[(size_t)is * nh + ih];
+            band = std::max(band, std::abs(c - h.cabs[(size_t)is * nh + left]));
+            band = std::max(band, std::abs(c - h.cabs[(size_t)is * nh + right]));
+        }
+    }
+    if (aper < 0 || lo > hi) {
+        lo = hi = 0;
+    }
+    h.band = band;
+    h.row0 = lo;
+    h.nrow = hi - lo + 1;
+    const int wid = 2 * band + 1;
+    h.rcv.assign((size_t)h.nrow * wid, DatEntry{0.0f, 0.0f, 0.0f});
+    h.rtau.assign((size_t)h.nrow * wid, 0.0f);
+    for (int r = 0; r < h.nrow; r++)
+        for (int j = 0; j < wid; j++) {
+            const int cc = h.row0 + r, c = cc + j - band;
+            if (cc < 0 || cc >= nrg || c < 0 || c >= nrg) continue;
+            DatEntry &e = h.rcv[(size_t)r * wid + j];
+            e.w = 1.0f;
+            e.tau = rt[(size_t)cc * nrg + c];
+            e.dtau = slope_host(rt, nrg, cc, c, p.drg) * fabsf(p.dh);
+            h.rtau[(size_t)r * wid + j] = e.tau;
+        }
+    return KCIG_OK;
+}
+
+int build_source(const kcig_datum_params &p, const float *st, Host &h)
+{
+    const int ns = p.ns, nh = p.nh, aper = p.aperture, nsg = p.nsg;
+    std::vector<int> cs(ns);
+    for (int is = 0; is < ns; is++) cs[is] = src_index(p, is);
+    if (p.cmp == 0) {
+        h.src.assign((size_t)ns * ns, DatEntry{0.0f, 0.0f, 0.0f});
+        for (int is = 0; is < ns; is++) {
+            const int c = cs[is];
+            if (c < 0 || c >= nsg) return set_error(KCIG_ERR_ARG, "Source table too small.");
+            const int left = std::max(0, is - aper), right = std::min(ns - 1, is + aper);
+            for (int ic = left; ic <= right; ic++) {
+                const int cc = cs[ic];
+                if (cc < 0 || cc >= nsg) return set_error(KCIG_ERR_ARG, "Source table too small.");
+                const float coef = taper_host(left, ic, right, p.taper, 1);
+                const float tau = st[(size_t)cc * nsg + c];
+                const float dist = p.sdatum * p.sdatum + (float)((ic - is) * (ic - is)) * p.ds * p.ds;
+                DatEntry &e = h.src[(size_t)is * ns + ic];
+                e.w = term_weight(coef, p.ds, p.sdatum, tau, dist);
+                e.tau = tau;
+                e.dtau = slope_host(st, nsg, cc, c, p.dsg) * fabsf(p.ds);
+            }
+        }
+        return KCIG_OK;
+    }
+    // the common-receiver walk (:556-579), in float as the reference
+    const float ds = p.ds, dh = p.dh;
+    const float s = fabsf((float)(ns - 1) * ds), hl = fabsf((float)(nh - 1) * dh);
+    const bool wide = fabsf(ds) >= fabsf(dh);
+    const int jump = wide ? 1 : f2i(dh / ds + 0.5f);
+    const float dr = wide ? fabsf(dh) : fabsf(ds);
+    const int nr = f2i((s + hl) / dr + 1.5f);
+    if (jump < 1) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: cmp=1 needs dh / ds >= 1 when |ds| < |dh|");
+    if (nr < 0 || (long long)nr * ns > 0x7fffffffLL) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: cmp=1 gather count");
+    h.nr = nr;
+    h.jump = jump;
+    h.sleft.resize(nr);
+    h.sright.resize(nr);
+    h.ihmap.assign((size_t)nr * ns, -1);
+    h.ir_lo.assign(ns, 0);
+    h.ir_hi.assign(ns, -1);
+    const float as = ds <= 0.f ? -1.f : 0.f, ah = dh <= 0.f ? -1.f : 0.f, bl = ds <= 0.f ? 0.f : -1.f;
+    for (int ir = 0; ir < nr; ir++) {
+        const float r = (float)ir * dr + as * s + ah * hl;
+        int sl = f2i(((float)ir * dr + as * s + bl * hl) / ds + 0.5f);
+        int sr = f2i(((float)ir * dr + as * s + as * hl) / ds + 0.5f);
+        if (sl < 0) sl = 0;
+        if (sr > ns - 1) sr = ns - 1;
+        const int left = f2i((r - (float)sl * ds) / dh + 0.5f);
+        if (left < 0 || left > nh - 1) sl++;
+        const int right = f2i((r - (float)sr * ds) / dh + 0.5f);
+        if (right < 0 || right > nh - 1) sr--;
+        h.sleft[ir] = sl;
+        h.sright[ir] = sr;
+        for (int is = sl; is <= sr; is += jump) {
+            if (is < 0 || is >= ns) continue;
+            const int c = cs[is];
+            if (c < 0 || c >= nsg) return set_error(KCIG_ERR_ARG, "Source table too small.");
+            const int ih = f2i((r - (float)is * ds) / dh + 0.5f);
+            h.ihmap[(size_t)ir * ns + is] = (ih >= 0 && ih < nh) ? ih : -1;
+            if (h.ir_hi[is] < h.ir_lo[is]) h.ir_lo[is] = ir;
+            h.ir_hi[is] = ir;
+        }
+    }
+    h.src.assign((size_t)ns * ns, DatEntry{0.0f, 0.0f, 0.0f});
+    h.stau.assign((size_t)ns * ns, 0.0f);
+    const float jds = fabsf((float)jump * ds);
+    for (int is = 0; is < ns; is++)
+        for (int ic = std::max(0, is - jump * aper); ic <= std::min(ns - 1, is + jump * aper); ic++) {
+            const int c = cs[is], cc = cs[ic];
+            if (c < 0 || c >= nsg || cc < 0 || cc >= nsg) continue;
+            DatEntry &e = h.src[(size_t)is * ns + ic];
+            e.w = 1.0f;
+            e.tau = st[(size_t)cc * nsg + c];
+            e.dtau = slope_host(st, nsg, cc, c, p.dsg) * jds;
+            h.stau[(size_t)is * ns + ic] = e.tau;
+        }
+    return KCIG_OK;
+}
+
+int launch_op(const DBuf &ent, int ne, float2 *out, int f0, int nf, int nfft, int K, const kcig_datum_params &p,
+              cudaStream_t st, int &launches)
+{
+    if (ne <= 0) return KCIG_OK;
+    DatOpArgs a;
+    a.ent = ent.as<DatEntry>();
+    a.ne = ne;
+    a.out = out;
+    a.f0 = f0;
+    a.nf = nf;
+    a.nfft = nfft;
+    a.K = K;
+    a.dt = p.dt;
+    a.antialias = p.antialias;
+    k_dat_op<<<(ne + 127) / 128, 128, (size_t)nf * 2 * sizeof(double), st>>>(a);
+    launches++;
+    KCIG_CUDA(cudaGetLastError());
+    return KCIG_OK;
+}
+
+int launch_gemm(const float2 *A, long long sA, int lda, const float2 *B, long long sB, int ldb, float2 *C,
+                long long sC, int ldc, int M, int N, int K, int band, int band_rows, int batch, cudaStream_t st,
+                int &launches)
+{
+    CGemmArgs g;
+    g.A = A;
+    g.B = B;
+    g.C = C;
+    g.sA = sA;
+    g.sB = sB;
+    g.sC = sC;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.ldc = ldc;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.band = band;
+    g.band_rows = band_rows;
+    for (int z0 = 0; z0 < batch; z0 += 65535) {
+        const int nz = std::min(65535, batch - z0);
+        CGemmArgs gz = g;
+        gz.A += (size_t)z0 * sA;
+        gz.B += (size_t)z0 * sB;
+        gz.C += (size_t)z0 * sC;
+        k_cgemm<<<dim3((N + 63) / 64, (M + 63) / 64, nz), 256, 0, st>>>(gz);
+        launches++;
+        KCIG_CUDA(cudaGetLastError());
+    }
+    return KCIG_OK;
+}
+
+}  // namespace
+}  // namespace kcig
+
+using namespace kcig;
+
+extern "C" int kcig_datum_params_init(kcig_datum_params *p)
+{
+    if (!p) return set_error(KCIG_ERR_ARG, "kcig_datum_params_init: null");
+    *p = kcig_datum_params{};
+    p->aperture = 50;
+    p->taper = 10;
+    p->data_taper = 0;
+    p->cmp = 1;
+    p->antialias = 1.0f;
+    p->length = 0.025f;
+    p->use_bf = 1;
+    p->bf_p = 12;
+    p->bf_n_leaf = 16;
+    p->bf_panel_levels = 1;
+    p->bf_amp_eps = 1e-20f;
+    p->bf_phase_tol = 2.0f;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_datum_sizes(const kcig_datum_params *p, const float *stable, const float *rtable, int *nsam,
+                                int *nfft)
+{
+    if (!p || !stable || !rtable || !nsam || !nfft) return set_error(KCIG_ERR_ARG, "kcig_datum_sizes: null argument");
+    KCIG_TRY(validate(*p));
+    return sizes(*p, stable, rtable, nsam, nfft);
+}
+
+extern "C" int kcig_datum_last_timing(float *ms5, int *launches)
+{
+    if (ms5)
+        for (int i = 0; i < 5; i++) ms5[i] = g_last_ms[i];
+    if (launches) *launches = g_last_launches;
+    return KCIG_OK;
+}
+
+extern "C" int kcig_green_slice(const float *table, int nz, int nx, int ngx, float oz, float ox, float dz, float dx,
+                                float ogx, float dgx, float datum, float *tgreen, int memory, void *stream)
+{
+    if (!table || !tgreen || nz <= 0 || nx <= 0 || ngx <= 0) return set_error(KCIG_ERR_ARG, "kcig_green_slice: bad arguments");
+    if (memory != KCIG_MEM_HOST && memory != KCIG_MEM_DEVICE) return set_error(KCIG_ERR_ARG, "kcig_green_slice: bad memory kind");
+    // src/greensol_auto.cpp:68-69 and :75-82: float operands, double 0.5
+    const int idatum = (int)((datum - oz) / dz + 0.5);
+    if (idatum < 0 || idatum >= nz) return set_error(KCIG_ERR_ARG, "Datum out of range.");
+    std::vector<int> ix(ngx);
+    for (int i = 0; i < ngx; i++) {
+        const float gx = ogx + (float)i * dgx;
+        ix[i] = (int)((gx - ox) / dx + 0.5);
+        if (ix[i] < 0 || ix[i] >= nx) return set_error(KCIG_ERR_ARG, "Receiver table too small.");
+    }
+    if (memory == KCIG_MEM_HOST) {
+        for (int i1 = 0; i1 < ngx; i1++)
+            for (int i2 = 0; i2 < ngx; i2++)
+                tgreen[(size_t)i1 * ngx + i2] = table[((size_t)i1 * nx + ix[i2]) * nz + idatum];
+        return KCIG_OK;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    DBuf dix;
+    KCIG_TRY(upload(dix, ix, st, "table indices"));
+    const int n = ngx * ngx;
+    k_green_gather<<<(n + 255) / 256, 256, 0, st>>>(table, dix.as<int>(), tgreen, ngx, nx, nz, idatum);
+    KCIG_CUDA(cudaGetLastError());
+    KCIG_CUDA(cudaStreamSynchronize(st));
+    return KCIG_OK;
+}
+
+extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable, const float *rtable, const float *in,
+                               float *out, float *interm, int memory, void *stream)
+{
+    if (!pp || !stable || !rtable || !in || !out) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: null argument");
+    if (memory != KCIG_MEM_HOST && memory != KCIG_MEM_DEVICE) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: bad memory kind");
+    const kcig_datum_params p = *pp;
+    KCIG_TRY(validate(p));
+    cudaStream_t st = (cudaStream_t)stream;
+    // host copies of the tables (indices, weights and nfft are decided there)
+    std::vector<float> sth, rth;
+    const float *stp = stable, *rtp = rtable;
+    if (memory == KCIG_MEM_DEVICE) {
+        sth.resize((size_t)p.nsg * p.nsg);
+        rth.resize((size_t)p.nrg * p.nrg);
+        KCIG_CUDA(cudaMemcpyAsync(sth.data(), stable, sth.size() * 4, cudaMemcpyDeviceToHost, st));
+        KCIG_CUDA(cudaMemcpyAsync(rth.data(), rtable, rth.size() * 4, cudaMemcpyDeviceToHost, st));
+        KCIG_CUDA(cudaStreamSynchronize(st));
+        stp = sth.data();
+        rtp = rth.data();
+    }
+    int nsam = 0, nfft = 0;
+    KCIG_TRY(sizes(p, stp, rtp, &nsam, &nfft));
+    const int nw = nfft / 2 + 1, K = nsam - 1;
+    const int ns = p.ns, nh = p.nh, nt = p.nt;
+    const long long ntr = (long long)ns * nh;
+    Host h;
+    KCIG_TRY(build_receiver(p, rtp, h));  // the receiver side's checks come first, as in the reference
+    KCIG_TRY(build_source(p, stp, h));
+    std::vector<float> wtr((size_t)ntr);
+    for (int is = 0; is < ns; is++) {
+        const float ws = edge_host(is, ns, p.data_taper);
+        for (int ih = 0; ih < nh; ih++) wtr[(size_t)is * nh + ih] = ws * edge_host(ih, nh, p.data_taper);
+    }
+
+    // ---- device buffers
+    int launches = 0;
+    const size_t spec_bytes = (size_t)nw * ntr * sizeof(float2);
+    DBuf din, dout, dim, U, Ufull, dwtr, drcv, dsrc, dextra[8];
+    const float *d_in = in;
+    float *d_out = out, *d_interm = interm;
+    if (memory == KCIG_MEM_HOST) {
+        KCIG_TRY(dalloc(din, (size_t)ntr * nt * 4, "the input traces"));
+        KCIG_CUDA(cudaMemcpyAsync(din.p, in, (size_t)ntr * nt * 4, cudaMemcpyHostToDevice, st));
+        KCIG_TRY(dalloc(dout, (size_t)ntr * nt * 4, "the output traces"));
+        d_in = din.as<float>();
+        d_out = dout.as<float>();
+        if (interm) {
+            KCIG_TRY(dalloc(dim, (size_t)ntr * nt * 4, "the intermediate traces"));
+            d_interm = dim.as<float>();
+        }
+    }
+    KCIG_TRY(dalloc(U, spec_bytes, "the spectra"));
+    if (interm) KCIG_TRY(dalloc(Ufull, spec_bytes, "the receiver-side spectra"));
+    KCIG_TRY(upload(dwtr, wtr, st, "trace weights"));
+    KCIG_TRY(upload(drcv, h.rcv, st, "receiver terms"));
+    KCIG_TRY(upload(dsrc, h.src, st, "source terms"));
+    // per-frequency bytes of a chunk: Utmp + both operators
+    const size_t op_r = h.rcv.size(), op_s = h.src.size();
+    const size_t per_f = (interm ? 0 : (size_t)ntr * sizeof(float2)) + (op_r + op_s) * sizeof(float2);
+    int chunk = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1536 << 20) / std::max<size_t>(per_f, 1)));
+    chunk = std::min(chunk, nw);
+    DBuf Ut, Kr, Ks;
+    if (!interm) KCIG_TRY(dalloc(Ut, (size_t)chunk * ntr * sizeof(float2), "the receiver-side chunk"));
+    KCIG_TRY(dalloc(Kr, (size_t)chunk * std::max<size_t>(op_r, 1) * sizeof(float2), "the receiver operator"));
+    KCIG_TRY(dalloc(Ks, (size_t)chunk * std::max<size_t>(op_s, 1) * sizeof(float2), "the source operator"));
+    DBuf dcabs, dgeom, drtau, dstau, dsl, dsr, dihm, dirl, dirh;
+    if (p.cmp == 1) {
+        KCIG_TRY(upload(dcabs, h.cabs, st, "receiver indices"));
+        KCIG_TRY(upload(dgeom, h.geom, st, "receiver weights"));
+        KCIG_TRY(upload(drtau, h.rtau, st, "receiver pair times"));
+        KCIG_TRY(upload(dstau, h.stau, st, "source pair times"));
+        KCIG_TRY(upload(dsl, h.sleft, st, "gather ranges"));
+        KCIG_TRY(upload(dsr, h.sright, st, "gather ranges"));
+        KCIG_TRY(upload(dihm, h.ihmap, st, "gather traces"));
+        KCIG_TRY(upload(dirl, h.ir_lo, st, "gather ranges"));
+        KCIG_TRY(upload(dirh, h.ir_hi, st, "gather ranges"));
+    }
+    // transform batches
+    const long long bmax = std::max<long long>(1, std::min<long long>(ntr, ((long long)1 << 28) / nfft));
+    const int B = (int)bmax;
+    DBuf pad, spec;
+    KCIG_TRY(dalloc(pad, (size_t)B * nfft * 4, "the transform buffer"));
+    KCIG_TRY(dalloc(spec, (size_t)B * nw * sizeof(float2), "the transform buffer"));
+    CufftPlan pf, pb, pf_tail, pb_tail;
+    int n_fft = nfft;
+    cufftResult cr;
+    if ((cr = cufftPlanMany(&pf.h, 1, &n_fft, nullptr, 1, nfft, nullptr, 1, nw, CUFFT_R2C, B)) != CUFFT_SUCCESS)
+        return cufft_error(cr, "cufftPlanMany (R2C)");
+    pf.ok = true;
+    if ((cr = cufftPlanMany(&pb.h, 1, &n_fft, nullptr, 1, nw, nullptr, 1, nfft, CUFFT_C2R, B)) != CUFFT_SUCCESS)
+        return cufft_error(cr, "cufftPlanMany (C2R)");
+    pb.ok = true;
+    const int tail = (int)(ntr % B);
+    if (tail) {
+        if ((cr = cufftPlanMany(&pf_tail.h, 1, &n_fft, nullptr, 1, nfft, nullptr, 1, nw, CUFFT_R2C, tail)) != CUFFT_SUCCESS)
+            return cufft_error(cr, "cufftPlanMany (R2C)");
+        pf_tail.ok = true;
+        if ((cr = cufftPlanMany(&pb_tail.h, 1, &n_fft, nullptr, 1, nw, nullptr, 1, nfft, CUFFT_C2R, tail)) != CUFFT_SUCCESS)
+            return cufft_error(cr, "cufftPlanMany (C2R)");
+        pb_tail.ok = true;
+    }
+    for (CufftPlan *q : {&pf, &pb, &pf_tail, &pb_tail})
+        if (q->ok && (cr = cufftSetStream(q->h, st)) != CUFFT_SUCCESS) return cufft_error(cr, "cufftSetStream");
+
+    cudaEvent_t ev[6];
+    for (auto &e : ev) KCIG_CUDA(cudaEventCreate(&e));
+    struct EvGuard {
+        cudaEvent_t *e;
+        ~EvGuard()
+        {
+            for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]);
+        }
+    } evg{ev};
+    const int tgrid = 148 * 8;
+    KCIG_CUDA(cudaEventRecord(ev[0], st));
+    // ---- forward: reverse, taper, pad, R2C, to frequency-major
+    for (long long t0 = 0; t0 < ntr; t0 += B) {
+        const int nb = (int)std::min<long long>(B, ntr - t0);
+        k_dat_prep<<<tgrid, 256, 0, st>>>(d_in, dwtr.as<float>(), pad.as<float>(), (int)t0, nb, nt, nfft);
+        launches++;
+        KCIG_CUDA(cudaGetLastError());
+        if ((cr = cufftExecR2C(nb == B ? pf.h : pf_tail.h, pad.as<cufftReal>(), spec.as<cufftComplex>())) != CUFFT_SUCCESS)
+            return cufft_error(cr, "cufftExecR2C");
+        launches++;
+        k_dat_to_fmajor<<<dim3((nw + 31) / 32, (nb + 31) / 32), dim3(32, 8), 0, st>>>(spec.as<float2>(), U.as<float2>(),
+                                                                                     (int)t0, nb, nw, (int)ntr);
+        launches++;
+        KCIG_CUDA(cudaGetLastError());
+    }
+    KCIG_CUDA(cudaEventRecord(ev[1], st));
+    // ---- per chunk of frequencies: operators, receiver side, source side
+    float ms_op = 0.0f, ms_r = 0.0f, ms_s = 0.0f;
+    cudaEvent_t ce[4];
+    for (auto &e : ce) KCIG_CUDA(cudaEventCreate(&e));
+    struct EvGuard4 {
+        cudaEvent_t *e;
+        ~EvGuard4()
+        {
+            for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]);
+        }
+    } evg4{ce};
+    for (int f0 = 0; f0 < nw; f0 += chunk) {
+        const int nf = std::min(chunk, nw - f0);
+        float2 *Uc = U.as<float2>() + (size_t)f0 * ntr;
+        float2 *Utc = interm ? Ufull.as<float2>() + (size_t)f0 * ntr : Ut.as<float2>();
+        KCIG_CUDA(cudaEventRecord(ce[0], st));
+        KCIG_TRY(launch_op(drcv, (int)op_r, Kr.as<float2>(), f0, nf, nfft, K, p, st, launches));
+        KCIG_TRY(launch_op(dsrc, (int)op_s, Ks.as<float2>(), f0, nf, nfft, K, p, st, launches));
+        KCIG_CUDA(cudaEventRecord(ce[1], st));
+        if (p.cmp == 0) {
+            KCIG_TRY(launch_gemm(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
+                                 p.aperture >= 0 ? p.aperture : 0, 0, nf, st, launches));
+        } else {
+            RcvCmp1Args a;
+            a.U = Uc;
+            a.Utmp = Utc;
+            a.P = Kr.as<float2>();
+            a.Ptau = drtau.as<float>();
+            a.cabs = dcabs.as<int>();
+            a.geom = dgeom.as<float>();
+            a.ns = ns;
+            a.nh = nh;
+            a.aper = p.aperture;
+            a.band = h.band;
+            a.row0 = h.row0;
+            a.nrow = h.nrow;
+            a.sU = ntr;
+            k_dat_rcv_cmp1<<<dim3((unsigned)((ntr + 127) / 128), nf), 128, 0, st>>>(a);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+        }
+        KCIG_CUDA(cudaEventRecord(ce[2], st));
+        if (p.cmp == 0) {
+            KCIG_TRY(launch_gemm(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                 p.aperture >= 0 ? p.aperture : 0, 1, nf, st, launches));
+        } else {
+            KCIG_CUDA(cudaMemsetAsync(Uc, 0, (size_t)nf * ntr * sizeof(float2), st));
+            SrcCmp1Args a;
+            a.Utmp = Utc;
+            a.Uout = Uc;
+            a.P = Ks.as<float2>();
+            a.Ptau = dstau.as<float>();
+            a.sleft = dsl.as<int>();
+            a.sright = dsr.as<int>();
+            a.ihmap = dihm.as<int>();
+            a.ir_lo = dirl.as<int>();
+            a.ir_hi = dirh.as<int>();
+            a.ns = ns;
+            a.nh = nh;
+            a.nr = h.nr;
+            a.aper = p.aperture;
+            a.jump = h.jump;
+            a.tap = p.taper;
+            a.ds = p.ds;
+            a.sdatum = p.sdatum;
+            a.sUout = ntr;
+            k_dat_src_cmp1<<<dim3((ns + 127) / 128, nf), 128, 0, st>>>(a);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+        }
+        KCIG_CUDA(cudaEventRecord(ce[3], st));
+        KCIG_CUDA(cudaEventSynchronize(ce[3]));
+        float t;
+        cudaEventElapsedTime(&t, ce[0], ce[1]);
+        ms_op += t;
+        cudaEventElapsedTime(&t, ce[1], ce[2]);
+        ms_r += t;
+        cudaEventElapsedTime(&t, ce[2], ce[3]);
+        ms_s += t;
+    }
+    KCIG_CUDA(cudaEventRecord(ev[2], st));
+    // ---- inverse: to trace-major, C2R, scale, reverse, trim
+    auto inverse = [&](const float2 *Usrc, float *dst, int reverse) -> int {
+        for (long long t0 = 0; t0 < ntr; t0 += B) {
+            const int nb = (int)std::min<long long>(B, ntr - t0);
+            k_dat_to_tmajor<<<dim3((nb + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(Usrc, spec.as<float2>(), (int)t0,
+                                                                                         nb, nw, (int)ntr);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+            if ((cr = cufftExecC2R(nb == B ? pb.h : pb_tail.h, spec.as<cufftComplex>(), pad.as<cufftReal>())) != CUFFT_SUCCESS)
+                return cufft_error(cr, "cufftExecC2R");
+            launches++;
+            k_dat_finish<<<tgrid, 256, 0, st>>>(pad.as<float>(), dst, (int)t0, nb, nt, nfft, 1.0f / (float)nfft, reverse);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+        }
+        return KCIG_OK;
+    };
+    if (interm) KCIG_TRY(inverse(Ufull.as<float2>(), d_interm, 0));
+    KCIG_TRY(inverse(U.as<float2>(), d_out, 1));
+    KCIG_CUDA(cudaEventRecord(ev[3], st));
+    if (memory == KCIG_MEM_HOST) {
+        KCIG_CUDA(cudaMemcpyAsync(out, d_out, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
+        if (interm) KCIG_CUDA(cudaMemcpyAsync(interm, d_interm, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
+    }
+    KCIG_CUDA(cudaStreamSynchronize(st));
+    float t;
+    cudaEventElapsedTime(&t, ev[0], ev[1]);
+    g_last_ms[0] = t;
+    g_last_ms[1] = ms_op;
+    g_last_ms[2] = ms_r;
+    g_last_ms[3] = ms_s;
+    cudaEventElapsedTime(&t, ev[2], ev[3]);
+    g_last_ms[4] = t;
+    g_last_launches = launches;
+    return KCIG_OK;
+}

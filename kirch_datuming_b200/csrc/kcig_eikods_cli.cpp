@@ -43,6 +43,7 @@ struct DevPtr {
 
 extern "C" int kcig_run_eikods_cli(int argc, char **argv)
 {
+    rsf_set_program("eikods2d");
     if (argc < 2) {
         printf("eikods2d in=vel.rsf out=time.rsf tdl1=... tds1=... [shotfile= gradz= gradx= order=2 b1= b2= "
                "vel=1 l=1 zshot= yshot=]\n");

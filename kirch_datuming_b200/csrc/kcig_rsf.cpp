@@ -212,6 +212,11 @@ static std::string fmt_double(double v)
     return s;
 }
 
+// the program named in the history line of the headers this process writes
+static std::string g_program = "kirchmig2d_cig";
+
+void rsf_set_program(const std::string &name) { g_program = name; }
+
 int rsf_write(const std::string &path, int ndim, const int *n, const double *o, const double *d,
               const std::vector<std::pair<std::string, std::string>> &keys, const float *data, long long count)
 {
@@ -237,7 +242,7 @@ int rsf_write(const std::string &path, int ndim, const int *n, const double *o, 
     time_t t = time(nullptr);
     char tb[64];
     ctime_r(&t, tb);
-    fprintf(fh, "\nkirchmig2d_cig\t\"%s\"\t%s@%s\t%s", cwd, user, host, tb);
+    fprintf(fh, "\n%s\t\"%s\"\t%s@%s\t%s", g_program.c_str(), cwd, user, host, tb);
     fprintf(fh, "\tin=\"%s\"\n", base_of(bin).c_str());
     fprintf(fh, "\tdata_format=\"native_float\"\n");
     for (int i = 0; i < ndim; i++) fprintf(fh, "\tn%d=%d\n", i + 1, n[i]);

@@ -25,6 +25,9 @@ struct RsfFile {
 int rsf_open(const std::string &path, RsfFile *f);
 // Read `count` floats starting at element `offset`.
 int rsf_read(const RsfFile &f, long long offset, long long count, float *dst);
+// The program name written in the history line of new headers (default
+// kirchmig2d_cig); each drop-in tool sets its own.
+void rsf_set_program(const std::string &name);
 // Write a new native_float header + "<path>@" binary (se_fs_sep.cpp:704-977).
 // keys are written after esize, in the given order.
 int rsf_write(const std::string &path, int ndim, const int *n, const double *o, const double *d,

@@ -214,19 +214,33 @@ __global__ void __launch_bounds__(256) k_stitch_all(const StitchAllArgs a)
             const float scale = __fmul_rn(w.scale, w.lateral ? sx : 1.0f);
             const float *src = w.layer + (size_t)col * w.n1w;
             unsigned long long bad = 0;
-            for (int i1 = lane; i1 < w.n1w; i1 += 32) {
-                float v = __fmul_rn(src[i1], scale);
-                if (!isfinite(v)) {
-                    ++bad;
-                    v = 0.0f;
+            // eight loads per lane in flight before the first is used: a
+            // window column is 256 samples or fewer in the common case, one
+            // round of independent loads instead of a dependent chain
+            for (int base = 0; base < w.n1w; base += 256) {
+                float ld[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int i1 = base + lane + 32 * u;
+                    ld[u] = i1 < w.n1w ? __ldcs(src + i1) : 0.0f;
                 }
-                const int r = w.start + i1;
-                if (w.overlap > 0 && r <= w.previous_end) {
-                    if (i1 < w.keep_upper || w.blend_count == 0) continue;
-                    const float bw = a.weights[w.woff + i1 - w.keep_upper];
-                    buf[r] = __fadd_rn(__fmul_rn(buf[r], __fsub_rn(1.0f, bw)), __fmul_rn(v, bw));
-                } else {
-                    buf[r] = v;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int i1 = base + lane + 32 * u;
+                    if (i1 >= w.n1w) continue;
+                    float v = __fmul_rn(ld[u], scale);
+                    if (!isfinite(v)) {
+                        ++bad;
+                        v = 0.0f;
+                    }
+                    const int r = w.start + i1;
+                    if (w.overlap > 0 && r <= w.previous_end) {
+                        if (i1 < w.keep_upper || w.blend_count == 0) continue;
+                        const float bw = a.weights[w.woff + i1 - w.keep_upper];
+                        buf[r] = __fadd_rn(__fmul_rn(buf[r], __fsub_rn(1.0f, bw)), __fmul_rn(v, bw));
+                    } else {
+                        buf[r] = v;
+                    }
                 }
             }
             for (int off = 16; off > 0; off >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, off);
