@@ -126,13 +126,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def measured_peaks():
+def measured_peaks(kind: str = "hbm"):
+    """(peak, source) of the HBM copy bandwidth (GB/s) or, kind="tensor", the
+    dense BF16 tensor throughput of a burst (TFLOP/s)."""
+    key, fallback = ("hbm_gbs", 6650.0) if kind == "hbm" else ("bf16_tflops", 1590.0)
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             m = json.load(f)
-        return float(m["hbm_gbs"]), "of measured"
+        return float(m[key]), "of measured"
     except Exception:
-        return 6650.0, "of fallback"
+        return fallback, "of fallback"
 
 
 def profiled_traffic():
@@ -632,6 +635,160 @@ def stitch_section(steps: int, warmup: int, threads: int):
     return res
 
 
+DAT_ROW = 120         # datum depth row (1.2 km) of the migration workload's tables
+DAT_ARGS = dict(aperture=200, taper=0, data_taper=20, length=0.05, antialias=1.0, cmp=0)  # the workflow's settings
+DAT_WORKLOAD = ("kirchdat2d_freq on the migration workload: five-layer salt 601x1601@10m, Green's tables sliced "
+                "at row 120 (1.2 km) from the 400-position eikods2d tables, 400 shots x 400 receivers (cmp=0, 40 m), "
+                "nt=3001 dt=1ms; aperture=200 taper=0 data_taper=20 length=0.05 antialias=1")
+DAT_SAMPLE = 100      # the CPU reference's bounded sample: the first 100 shots x 100 receivers
+
+
+def datum_terms(nh: int, ns: int, aper: int) -> int:
+    """Terms of the exact operator per frequency, both sides, cmp=0: every
+    (output trace, input trace) pair inside the aperture."""
+    r = sum(min(nh - 1, i + aper) - max(0, i - aper) + 1 for i in range(nh)) * ns
+    s = sum(min(ns - 1, i + aper) - max(0, i - aper) + 1 for i in range(ns)) * nh
+    return r + s
+
+
+def datum_section(steps: int, warmup: int, threads: int, T=None, data=None):
+    """Frequency-domain datuming (the recursive workflow's step between depth
+    windows) on the migration workload: device time with the cube in HBM,
+    end to end through the C ABI with host arrays, the stage split, the
+    reference tool on a bounded sample and the FP64 oracle on a smaller one."""
+    import torch
+    import kirch_datuming_b200 as kd
+    from kirch_datuming_b200 import rsf, synth
+    f = lambda x: float(np.float32(x))  # noqa: E731
+    if T is None or data is None:
+        v, refl = synth.five_layer_salt(NZ, NX, DZ, DZ, seed=7)
+        T, _ = kd.eikonal_tables(torch.from_numpy(v).cuda(), DZ, DZ, NPOS, 0.0, DP, deriv=False)
+        g = synth.Geometry(nz=NZ, nx=NX, dz=DZ, dx=DZ, z0=0, x0=0, ns=NPOS, s0=0.0, ds=DP, nh=NPOS, h0=0.0, dh=DP,
+                           cmp=0, nt=NT, dt=DT, t0=0.0, npos=NPOS, p0=0.0, dp=DP)
+        data = synth.shot_gathers(T, g, [(rows, a) for rows, a in zip(refl.values(), synth.reflectivities(len(refl), 3))],
+                                  FREQ, seed=3)
+    datum = f(DAT_ROW * DZ)
+    green = torch.empty((NPOS, NPOS), dtype=torch.float32, device="cuda")
+    kd.green_slice(T, NZ, NX, NPOS, 0.0, 0.0, DZ, DZ, 0.0, DP, datum, green)
+    gh = green.cpu().numpy()
+
+    def params(ns, nh, ng):
+        return kd.datum_params(nt=NT, nh=nh, ns=ns, dt=f(DT), h0=0.0, dh=f(DP), s0=0.0, ds=f(DP), nsg=ng, nrg=ng,
+                               sg0=0.0, dsg=f(DP), rg0=0.0, drg=f(DP), sdatum=datum, rdatum=datum, **DAT_ARGS)
+
+    p = params(NPOS, NPOS, NPOS)
+    nsam, nfft = kd.datum_sizes(p, gh, gh)
+    nw = nfft // 2 + 1
+    out = torch.empty_like(data)
+    st = torch.cuda.current_stream()
+    for _ in range(max(1, warmup)):
+        kd.datum_freq(p, green, green, data, out)
+    ms, stages = [], []
+    for _ in range(max(1, steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        kd.datum_freq(p, green, green, data, out)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        stages.append(kd.datum_last_timing())
+    t = statistics.median(ms)
+    st_ms, launches = stages[len(stages) // 2]
+    terms = datum_terms(NPOS, NPOS, DAT_ARGS["aperture"]) * nw
+    # end to end: host arrays through kcig_datum_freq (the cube in and out over PCIe)
+    hdata = data.cpu().numpy()
+    hout = np.empty_like(hdata)
+    e2e = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        kd.datum_freq(p, gh, gh, hdata, hout)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = min(e2e)
+    same = bool(np.array_equal(hout, out.cpu().numpy()))
+    gemm_ms = st_ms[2] + st_ms[3]
+    # executed tensor work of k_cgemm_tc: per side and frequency ceil(400/128)^2 tiles of a 128 x 256 real
+    # accumulator over 2 x 400 real k, three TF32 products each
+    tiles = math.ceil(NPOS / 128) ** 2
+    tensor_flops = 2 * nw * tiles * (128 * 256 * 2 * NPOS) * 2.0 * 3
+    peak_bf16, peak_src = measured_peaks(kind="tensor")
+    tf32_peak = peak_bf16 / 2
+    res = {"workload": DAT_WORKLOAD, "nfft": nfft, "frequencies": nw, "nsam": nsam,
+           "value": terms / (t / 1e3) / 1e9, "unit": "Gterms/s", "ms": t,
+           "stages_ms": {"forward_fft": st_ms[0], "operators": st_ms[1], "receiver_side": st_ms[2],
+                         "source_side": st_ms[3], "inverse_fft": st_ms[4]},
+           "gpu_launches": launches,
+           "e2e": {"value": terms / (e2e_ms / 1e3) / 1e9, "unit": "Gterms/s", "ms": e2e_ms,
+                   "h2d_bytes": hdata.nbytes + 2 * gh.nbytes, "d2h_bytes": hout.nbytes,
+                   "equals_device_run": same},
+           "roofline": {"bound": "tensor", "kernel": "k_cgemm_tc (both sides)",
+                        "achieved": tensor_flops / (gemm_ms / 1e3) / 1e12, "peak": tf32_peak, "unit": "TFLOP/s",
+                        "frac": tensor_flops / (gemm_ms / 1e3) / 1e12 / tf32_peak,
+                        "peak_source": "dense TF32 = half the BF16 figure " + peak_src,
+                        "useful_frac": datum_terms(NPOS, NPOS, DAT_ARGS["aperture"]) * 8.0 * 3 * nw
+                                       / tensor_flops,
+                        "note": "executed TF32 tensor flops (3 products per FP32 product, padded 128-row / "
+                                "128-column tiles); useful_frac = the exact operator's terms over the executed "
+                                "products"},
+           "unit_note": "a term is one (output trace, input trace, frequency) product of the exact operator, "
+                        "receiver and source sides; the reference's butterfly approximates these sums"}
+    # the reference tool (use_bf=1, its default) on the bounded sample, and the GPU on the same sample
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "kirchdat2d_freq")
+    n = DAT_SAMPLE
+    sub = np.ascontiguousarray(hdata[:n, :n, :])
+    gsub = np.ascontiguousarray(gh[:n, :n])
+    ps = params(n, n, n)
+    gpu_sub = np.empty_like(sub)
+    kd.datum_freq(ps, gsub, gsub, sub, gpu_sub)
+    nfft_s = kd.datum_sizes(ps, gsub, gsub)[1]
+    terms_s = datum_terms(n, n, DAT_ARGS["aperture"]) * (nfft_s // 2 + 1)
+    if os.path.exists(ref_bin):
+        with tempfile.TemporaryDirectory() as wd:
+            rsf.write(f"{wd}/vel.rsf", np.zeros((4, 4), np.float32), [4, 4], [0, 0], [DZ, DZ],
+                      extra={"should_datum": str(DAT_ROW)})
+            rsf.write(f"{wd}/green.rsf", gsub, [n, n], [0.0, 0.0], [f(DP), f(DP)])
+            rsf.write(f"{wd}/d.rsf", sub, [NT, n, n], [0, 0, 0], [f(DT), f(DP), f(DP)])
+            args = ["input_file=d.rsf", "output_file=o.rsf", "sgreen_file=green.rsf", "rgreen_file=green.rsf",
+                    "model_file=vel.rsf", "aperture=200", "taper=0", "data_taper=20", "length=0.05", "cmp=0",
+                    "antialias=1", "use_bf=1"]
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            t0 = time.perf_counter()
+            r = subprocess.run([ref_bin] + args, cwd=wd, env=env, capture_output=True, text=True, timeout=900)
+            sec = time.perf_counter() - t0
+            if r.returncode == 0:
+                _, ro = rsf.read(f"{wd}/o.rsf")
+                ro = ro.astype(np.float64).reshape(gpu_sub.shape)
+                res["cpu_baseline"] = {"value": terms_s / sec / 1e9, "unit": "Gterms/s", "cores": threads,
+                                       "kind": "reference", "seconds": sec,
+                                       "sample": "oracle/_ref/kirchdat2d_freq (use_bf=1, the default) on the first "
+                                                 "%d shots x %d receivers, nt=%d, %d frequencies, wall time incl. "
+                                                 "file I/O" % (n, n, NT, nfft_s // 2 + 1)}
+                res["parity"] = {"relL2_gpu_vs_reference_bf": float(np.linalg.norm(gpu_sub - ro) / np.linalg.norm(ro)),
+                                 "note": "the reference's default applies the butterfly approximation of the "
+                                         "operator; the GPU applies the exact operator"}
+            else:
+                res["cpu_baseline"] = {"value": None, "error": r.stderr[-300:]}
+    # the FP64 oracle on a smaller sample (12 shots x 24 receivers, full nt)
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import datum as D
+        ns_o, nh_o = 12, 24
+        so = np.ascontiguousarray(hdata[:ns_o, :nh_o, :])
+        ng = max(ns_o, nh_o)
+        go = np.ascontiguousarray(gh[:ng, :ng])
+        po = params(ns_o, nh_o, ng)
+        gpu_o = np.empty_like(so)
+        kd.datum_freq(po, go, go, so, gpu_o)
+        o = D.Datum(NT, nh_o, ns_o, f(DT), 0.0, f(DP), 0.0, f(DP), go, 0.0, f(DP), go, 0.0, f(DP), np.float32(datum),
+                    np.float32(datum), **DAT_ARGS).run(so)
+        res.setdefault("parity", {})["relL2_gpu_vs_fp64_oracle"] = float(np.linalg.norm(gpu_o - o) / np.linalg.norm(o))
+        res["parity"]["oracle_sample"] = "first %d shots x %d receivers, nt=%d" % (ns_o, nh_o, NT)
+    except Exception as e:  # noqa: BLE001
+        res.setdefault("parity", {})["oracle_error"] = str(e)[-300:]
+    return res
+
+
 def surrogate_section(train_steps: int, steps: int, warmup: int, threads: int):
     """Table path vs learned-surrogate path on the same v(z) 201x401 gathers,
     every image judged against the FP64 oracle of the table path (run on the
@@ -864,6 +1021,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the uneven five-window workload")
     ap.add_argument("--no-stitch", action="store_true", help="skip the ADCIG stitching section")
     ap.add_argument("--only-stitch", action="store_true", help="only the ADCIG stitching section (one JSON object)")
+    ap.add_argument("--no-datum", action="store_true", help="skip the datuming section")
+    ap.add_argument("--only-datum", action="store_true", help="only the datuming section (one JSON object)")
     ap.add_argument("--no-tables", action="store_true", help="skip the table-generator section")
     ap.add_argument("--no-stream", action="store_true", help="skip the host-resident-tables measurement")
     ap.add_argument("--large-grid-sample", action="store_true",
@@ -924,6 +1083,10 @@ def main():
     if args.only_stitch:
         threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
         print(json.dumps({"stitch": stitch_section(args.steps, args.warmup, threads)}), flush=True)
+        return 0
+    if args.only_datum:
+        threads = len(os.sched_getaffinity(0))
+        print(json.dumps({"datum": datum_section(args.steps, args.warmup, threads)}), flush=True)
         return 0
     if args.only_surrogate:
         threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
@@ -1083,6 +1246,12 @@ def main():
             line["surrogate"] = surrogate_section(args.surrogate_steps, args.steps, args.warmup, threads)
         except Exception as e:  # noqa: BLE001
             line["surrogate"] = {"workload": SG_WORKLOAD, "error": str(e)[-400:]}
+    if dist is None and not args.no_datum and args.size == "full":
+        try:  # an extra object: its failure is recorded, the line still prints
+            line["datum"] = datum_section(args.steps, args.warmup, threads, T=T, data=data)
+        except Exception as e:  # noqa: BLE001
+            line["datum"] = {"workload": DAT_WORKLOAD, "error": str(e)[-400:]}
+        torch.cuda.empty_cache()
     if dist is None and not args.no_batched:
         plan.close()
         del T, D, data, image

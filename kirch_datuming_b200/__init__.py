@@ -25,6 +25,8 @@ cli_path = os.path.join(_HERE, "bin", "kirchmig2d_cig")
 kirchmig2d_cli_path = os.path.join(_HERE, "bin", "kirchmig2d")
 eikods_cli_path = os.path.join(_HERE, "bin", "eikods2d")
 layercom_cig_cli_path = os.path.join(_HERE, "bin", "layercom_cig")
+greensol_auto_cli_path = os.path.join(_HERE, "bin", "greensol_auto")
+kirchdat2d_freq_cli_path = os.path.join(_HERE, "bin", "kirchdat2d_freq")
 
 MEM_HOST = 0
 MEM_DEVICE = 1

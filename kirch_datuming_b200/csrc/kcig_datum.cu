@@ -27,12 +27,16 @@
 #include <cufft.h>
 #include <math.h>
 
+#include <stdlib.h>
+#include <string.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <vector>
 
 #include "kcig_common.h"
+#include "kcig_tc.h"
 
 namespace kcig {
 namespace {
@@ -232,6 +236,233 @@ __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
             if (gn < a.N) C[(size_t)gm * a.ldc + gn] = make_float2(ar[i][j], ai[i][j]);
         }
     }
+}
+
+// The same batched complex GEMM on the tensor cores (tcgen05, kind::tf32,
+// accumulator in TMEM) with FP32 accuracy from three TF32 products:
+// x = hi + lo (hi = TF32(x), lo = TF32(x - hi), both rounded to nearest),
+// a.b ~ ah.bh + ah.bl + al.bh,
+// the dropped al.bl and the TF32 rounding of lo being ~2^-22 relative.
+// The complex product is one real GEMM: A viewed as floats is the real
+// M x 2K matrix [.. Ar Ai ..], each complex entry of B becomes the 2x2 real
+// block [[Br, Bi], [-Bi, Br]] (rows k re/im, columns n re/im), and the real
+// M x 2N result is C in its interleaved layout.
+// CTA tile: 128 rows x 128 complex columns (a 128 x 256 FP32 accumulator,
+// 256 TMEM columns); K in chunks of 8 complex (16 real) through 2 pipeline
+// stages of 48 KB (hi and lo of A and of the expanded B, canonical K-major
+// layout); warps 0-7 load, split, expand and store the operands and then
+// read the accumulator out, warp 8 allocates TMEM and one of its lanes
+// issues the MMAs.  Every mbarrier wait is bounded; a wait that gives up
+// sets *status, and the CTA stops issuing work, waits (bounded) for its own
+// MMAs and frees its TMEM.
+namespace tcg {
+constexpr int TM = 128, TNC = 128, TN = 256, KC = 8, KR = 16, S = 2;
+constexpr int A_BYTES = TM * KR * 4;               // one of hi / lo
+constexpr int B_BYTES = TN * KR * 4;
+constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;   // 48 KB
+constexpr int SMEM = S * STAGE + 128;              // + barriers and slots
+constexpr int THREADS = 288;
+}  // namespace tcg
+
+// a bounded mbarrier wait: at most 2^22 polls, each suspending the thread for
+// up to 1 us (a few seconds in all; a tile's whole main loop takes ~20 us)
+__device__ __forceinline__ bool dat_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t addr = tc::smem_u32(bar);
+    for (uint32_t i = 0; i < (1u << 22); i++) {
+        uint32_t ready;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ready)
+            : "r"(addr), "r"(parity), "r"(1000u)
+            : "memory");
+        if (ready) return true;
+    }
+    return false;
+}
+
+// x rounded to 10 mantissa bits (half an ulp added to the magnitude's bits,
+// the low 13 bits cleared): the TF32 value nearest x, on the integer pipes
+__device__ __forceinline__ float tf32_round(float x)
+{
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+__device__ __forceinline__ void tc_store_split(uint8_t *hi, uint8_t *lo, uint32_t off, float4 v)
+{
+    float4 h, l;
+    h.x = tf32_round(v.x);
+    h.y = tf32_round(v.y);
+    h.z = tf32_round(v.z);
+    h.w = tf32_round(v.w);
+    l.x = tf32_round(v.x - h.x);
+    l.y = tf32_round(v.y - h.y);
+    l.z = tf32_round(v.z - h.z);
+    l.w = tf32_round(v.w - h.w);
+    *reinterpret_cast<float4 *>(hi + off) = h;
+    *reinterpret_cast<float4 *>(lo + off) = l;
+}
+
+__global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a, int *status)
+{
+    using namespace tcg;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + S * STAGE);
+    uint64_t *empty = full + S;
+    uint64_t *done = empty + S;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tslot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int z = blockIdx.z;
+    const float2 *A = a.A + (size_t)z * a.sA;
+    const float2 *B = a.B + (size_t)z * a.sB;
+    float2 *C = a.C + (size_t)z * a.sC;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TNC;
+    int k_lo = 0, k_hi = a.K;
+    if (a.band >= 0) {
+        const int c0 = a.band_rows ? m0 : n0, c1 = (a.band_rows ? min(a.M, m0 + TM) : min(a.N, n0 + TNC)) - 1;
+        k_lo = max(0, c0 - a.band);
+        k_hi = min(a.K, c1 + a.band + 1);
+    }
+    const int nchunks = k_hi > k_lo ? (k_hi - k_lo + KC - 1) / KC : 0;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            tc::mbar_init(&full[s], 8);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(done, 1);
+        *abort_flag = 0;
+    }
+    if (warp == 8) tc::tmem_alloc(tslot, 256);
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp < 8) {
+        // ---- producers: chunk i of 8 complex k into stage i % S.  The
+        // global loads of chunk i+1 are issued before chunk i is split and
+        // stored, so their latency overlaps the stores and the stage wait.
+        const int t = threadIdx.x;  // 0..255
+        float2 xa[2][2], yb[4][2];
+        auto load = [&](int i) {
+            const int k0 = k_lo + i * KC;
+#pragma unroll
+            for (int rr = 0; rr < 2; rr++) {
+                const int e = t + 256 * rr, row = e >> 2, j = e & 3, gm = m0 + row, gk = k0 + 2 * j;
+                xa[rr][0] = xa[rr][1] = make_float2(0.0f, 0.0f);
+                if (gm < a.M) {
+                    const float2 *src = A + (size_t)gm * a.lda;
+                    if (gk < k_hi) xa[rr][0] = src[gk];
+                    if (gk + 1 < k_hi) xa[rr][1] = src[gk + 1];
+                }
+            }
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) {
+                const int e = t + 256 * rr, j = e >> 8, nc = (e & 255) >> 1, gn = n0 + nc, gk = k0 + 2 * j;
+                yb[rr][0] = yb[rr][1] = make_float2(0.0f, 0.0f);
+                if (gn < a.N) {
+                    if (gk < k_hi) yb[rr][0] = B[(size_t)gk * a.ldb + gn];
+                    if (gk + 1 < k_hi) yb[rr][1] = B[(size_t)(gk + 1) * a.ldb + gn];
+                }
+            }
+        };
+        if (nchunks > 0) load(0);
+        for (int i = 0; i < nchunks; i++) {
+            const int slot = i % S;
+            float2 ca[2][2], cb[4][2];
+#pragma unroll
+            for (int rr = 0; rr < 2; rr++) ca[rr][0] = xa[rr][0], ca[rr][1] = xa[rr][1];
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) cb[rr][0] = yb[rr][0], cb[rr][1] = yb[rr][1];
+            if (i + 1 < nchunks) load(i + 1);
+            if (i >= S && !dat_wait(&empty[slot], ((i / S) - 1) & 1)) {
+                atomicExch(status, 1);
+                *abort_flag = 1;
+            }
+            if (*abort_flag) break;
+            uint8_t *st = smem + slot * STAGE;
+            uint8_t *a_hi = st, *a_lo = st + A_BYTES, *b_hi = st + 2 * A_BYTES, *b_lo = b_hi + B_BYTES;
+            // A: 128 rows x 4 pairs of complex k -> one 16-byte row segment of a k-group
+#pragma unroll
+            for (int rr = 0; rr < 2; rr++) {
+                const int e = t + 256 * rr, row = e >> 2, j = e & 3;
+                const uint32_t off = (uint32_t)(j * (TM * 16) + (row >> 3) * 128 + (row & 7) * 16);
+                tc_store_split(a_hi, a_lo, off, make_float4(ca[rr][0].x, ca[rr][0].y, ca[rr][1].x, ca[rr][1].y));
+            }
+            // B: 4 pairs of complex k x 128 complex n, each expanded to the two
+            // real rows 2n (C real) and 2n+1 (C imaginary)
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) {
+                const int e = t + 256 * rr, j = e >> 8, rw = e & 255, h = rw & 1;
+                const float2 y0 = cb[rr][0], y1 = cb[rr][1];
+                const float4 v = h ? make_float4(y0.y, y0.x, y1.y, y1.x) : make_float4(y0.x, -y0.y, y1.x, -y1.y);
+                const uint32_t off = (uint32_t)(j * (TN * 16) + (rw >> 3) * 128 + (rw & 7) * 16);
+                tc_store_split(b_hi, b_lo, off, v);
+            }
+            tc::fence_async_smem();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&full[slot]);
+        }
+    } else if (lane == 0) {
+        // ---- MMA issuer
+        const uint32_t idesc = tc::idesc_tf32(TM, TN);
+        for (int i = 0; i < nchunks; i++) {
+            const int slot = i % S;
+            if (!dat_wait(&full[slot], (i / S) & 1)) {
+                atomicExch(status, 2);
+                *abort_flag = 1;
+            }
+            if (*abort_flag) break;
+            tc::fence_after();
+            const uint32_t st = tc::smem_u32(smem + slot * STAGE);
+            const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
+#pragma unroll
+            for (int s = 0; s < KR / 8; s++) {
+                const uint32_t ao = s * 2 * (TM * 16), bo = s * 2 * (TN * 16);
+                const uint64_t dah = tc::sdesc(ah + ao, TM * 16, 128), dal = tc::sdesc(al + ao, TM * 16, 128);
+                const uint64_t dbh = tc::sdesc(bh + bo, TN * 16, 128), dbl = tc::sdesc(bl + bo, TN * 16, 128);
+                tc::mma_tf32(tmem, dah, dbh, idesc, (i > 0 || s > 0) ? 1u : 0u);
+                tc::mma_tf32(tmem, dah, dbl, idesc, 1u);
+                tc::mma_tf32(tmem, dal, dbh, idesc, 1u);
+            }
+            tc::commit(&empty[slot]);
+        }
+        tc::commit(done);  // tracks every MMA issued, also after an abort
+    }
+    __syncwarp();
+    // ---- epilogue: warps 0-7 read the accumulator; warp w owns TMEM lanes
+    // 32 (w % 4) .. +31 and real columns 128 (w / 4) .. +127
+    bool ok = true;
+    if (warp < 8 || lane == 0) ok = dat_wait(done, 0);
+    if (!ok) atomicExch(status, 3);
+    if (warp < 8) {
+        tc::fence_after();
+        const int q = warp & 3, half = warp >> 2;
+        const int gm = m0 + 32 * q + lane;
+        const bool live = __all_sync(0xffffffffu, ok && !*abort_flag);  // warp-uniform: TMEM loads are collective
+        for (int cb = 0; cb < 4; cb++) {
+            float v[32];
+            const int c0 = 128 * half + 32 * cb;  // real column of the tile
+            if (nchunks > 0 && live) {
+                tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; c++) v[c] = 0.0f;
+            }
+            if (gm < a.M && live) {
+                float2 *dst = C + (size_t)gm * a.ldc + n0 + c0 / 2;
+#pragma unroll
+                for (int c = 0; c < 16; c++)
+                    if (n0 + c0 / 2 + c < a.N) dst[c] = make_float2(v[2 * c], v[2 * c + 1]);
+            }
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 8) tc::tmem_free(tmem, 256);
 }
 
 // cmp = 1 receiver side (:493-546 with s_abs = s0 + is ds): one thread per
@@ -767,6 +998,48 @@ int launch_gemm(const float2 *A, long long sA, int lda, const float2 *B, long lo
     return KCIG_OK;
 }
 
+int launch_gemm_tc(const float2 *A, long long sA, int lda, const float2 *B, long long sB, int ldb, float2 *C,
+                   long long sC, int ldc, int M, int N, int K, int band, int band_rows, int batch, int *status,
+                   cudaStream_t st, int &launches)
+{
+    CGemmArgs g;
+    g.A = A;
+    g.B = B;
+    g.C = C;
+    g.sA = sA;
+    g.sB = sB;
+    g.sC = sC;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.ldc = ldc;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.band = band;
+    g.band_rows = band_rows;
+    KCIG_TRY(set_dyn_smem((const void *)k_cgemm_tc, tcg::SMEM));
+    for (int z0 = 0; z0 < batch; z0 += 65535) {
+        const int nz = std::min(65535, batch - z0);
+        CGemmArgs gz = g;
+        gz.A += (size_t)z0 * sA;
+        gz.B += (size_t)z0 * sB;
+        gz.C += (size_t)z0 * sC;
+        k_cgemm_tc<<<dim3((N + tcg::TNC - 1) / tcg::TNC, (M + tcg::TM - 1) / tcg::TM, nz), tcg::THREADS, tcg::SMEM, st>>>(
+            gz, status);
+        launches++;
+        KCIG_CUDA(cudaGetLastError());
+    }
+    return KCIG_OK;
+}
+
+// the GEMMs of cmp = 0 run on the tensor cores; KCIG_DATUM_GEMM=simt selects
+// the FP32 CUDA-core kernel instead (a diagnostic comparison)
+bool gemm_on_tensor_cores()
+{
+    const char *e = getenv("KCIG_DATUM_GEMM");
+    return !(e && strcmp(e, "simt") == 0);
+}
+
 }  // namespace
 }  // namespace kcig
 
@@ -889,6 +1162,10 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         }
     }
     KCIG_TRY(dalloc(U, spec_bytes, "the spectra"));
+    DBuf dstatus;
+    KCIG_TRY(dalloc(dstatus, sizeof(int), "a status word"));
+    KCIG_CUDA(cudaMemsetAsync(dstatus.p, 0, sizeof(int), st));
+    const bool tcore = gemm_on_tensor_cores();
     if (interm) KCIG_TRY(dalloc(Ufull, spec_bytes, "the receiver-side spectra"));
     KCIG_TRY(upload(dwtr, wtr, st, "trace weights"));
     KCIG_TRY(upload(drcv, h.rcv, st, "receiver terms"));
@@ -987,8 +1264,12 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         KCIG_TRY(launch_op(dsrc, (int)op_s, Ks.as<float2>(), f0, nf, nfft, K, p, st, launches));
         KCIG_CUDA(cudaEventRecord(ce[1], st));
         if (p.cmp == 0) {
-            KCIG_TRY(launch_gemm(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
-                                 p.aperture >= 0 ? p.aperture : 0, 0, nf, st, launches));
+            if (tcore)
+                KCIG_TRY(launch_gemm_tc(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
+                                        p.aperture >= 0 ? p.aperture : 0, 0, nf, dstatus.as<int>(), st, launches));
+            else
+                KCIG_TRY(launch_gemm(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
+                                     p.aperture >= 0 ? p.aperture : 0, 0, nf, st, launches));
         } else {
             RcvCmp1Args a;
             a.U = Uc;
@@ -1010,8 +1291,12 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         }
         KCIG_CUDA(cudaEventRecord(ce[2], st));
         if (p.cmp == 0) {
-            KCIG_TRY(launch_gemm(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
-                                 p.aperture >= 0 ? p.aperture : 0, 1, nf, st, launches));
+            if (tcore)
+                KCIG_TRY(launch_gemm_tc(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus.as<int>(), st, launches));
+            else
+                KCIG_TRY(launch_gemm(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                     p.aperture >= 0 ? p.aperture : 0, 1, nf, st, launches));
         } else {
             KCIG_CUDA(cudaMemsetAsync(Uc, 0, (size_t)nf * ntr * sizeof(float2), st));
             SrcCmp1Args a;
@@ -1072,7 +1357,11 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         KCIG_CUDA(cudaMemcpyAsync(out, d_out, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
         if (interm) KCIG_CUDA(cudaMemcpyAsync(interm, d_interm, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
     }
+    int dev_status = 0;
+    KCIG_CUDA(cudaMemcpyAsync(&dev_status, dstatus.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     KCIG_CUDA(cudaStreamSynchronize(st));
+    if (dev_status)
+        return set_error(KCIG_ERR_DEVICE, "kcig_datum_freq: a tensor-core GEMM gave up waiting (stage %d)", dev_status);
     float t;
     cudaEventElapsedTime(&t, ev[0], ev[1]);
     g_last_ms[0] = t;

@@ -68,6 +68,38 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         : "memory");
 }
 
+// instruction descriptor of kind::tf32: TF32 x TF32 -> FP32, M x N, both
+// operands K-major.  In the canonical layout a TF32 core matrix is 8 rows x
+// 4 elements (16 bytes), so one MMA (K = 8) spans two core matrices along K,
+// as a kind::f16 MMA (K = 16) does.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N)
+{
+    return (1u << 4)                      // D format F32
+           | (2u << 7)                    // A format TF32
+           | (2u << 10)                   // B format TF32
+           | ((uint32_t)(N >> 3) << 17)   // N / 8
+           | ((uint32_t)(M >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// round to the nearest TF32 value (10 mantissa bits; the low 13 bits become 0)
+__device__ __forceinline__ float to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
 // all tcgen05 operations issued so far by this thread arrive on `bar` when done
 __device__ __forceinline__ void commit(uint64_t *bar)
 {

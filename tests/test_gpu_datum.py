@@ -105,9 +105,9 @@ def test_datum_linearity_and_zero():
 
 
 def test_datum_larger_survey_vs_oracle():
-    """64 shots x 96 fixed receivers (cmp=0, full aperture, the workflow's
-    settings) on the salt fixture's tables: several K tiles of the GEMMs,
-    partial tiles at both ends."""
+    """40 shots x 70 fixed receivers (cmp=0, the aperture covering the whole
+    spread, the workflow's settings) on the salt fixture's tables, shots off
+    the table grid."""
     t = META["table"]
     G = np.ascontiguousarray(GOLD["green"])
     ns, nh, nt, dt = 40, 70, 128, 0.004
@@ -171,3 +171,43 @@ def test_kirchdat2d_freq_cli(case):
             assert rel(im, GOLD["interm_" + case]) < 3e-5
             with open(f"{wd}/interm.rsf") as f:
                 assert body(f.read()) == body(c["interm_header"])
+
+
+def _survey(ns, nh, aperture, seed, cmp=0):
+    t = META["table"]
+    G = np.ascontiguousarray(GOLD["green"])
+    nt, dt = 128, 0.004
+    x = np.random.default_rng(seed).standard_normal((ns, nh, nt)).astype(np.float32)
+    geo = dict(h0=0.05, dh=0.005, s0=0.02, ds=0.005)
+    p = kd.datum_params(nt=nt, nh=nh, ns=ns, dt=dt, nsg=G.shape[0], nrg=G.shape[0], sg0=t["o"][2], dsg=t["d"][2],
+                        rg0=t["o"][2], drg=t["d"][2], sdatum=0.1, rdatum=0.1, aperture=aperture, taper=3,
+                        data_taper=5, cmp=cmp, antialias=1.0, length=0.05, **geo)
+    o = D.Datum(nt, nh, ns, dt, geo["h0"], geo["dh"], geo["s0"], geo["ds"], G, t["o"][2], t["d"][2], G, t["o"][2],
+                t["d"][2], np.float32(0.1), np.float32(0.1), aperture=aperture, taper=3, data_taper=5, cmp=cmp,
+                antialias=1.0, length=0.05)
+    return p, G, x, o
+
+
+def test_datum_tiles_and_band_vs_oracle():
+    """150 shots x 140 receivers, aperture 20: two 128-row and two
+    128-column tiles per side, K ranges clipped by the aperture band at
+    offsets that are not multiples of the K chunk."""
+    p, G, x, o = _survey(150, 140, 20, 11)
+    out = np.empty_like(x)
+    kd.datum_freq(p, G, G, x, out)
+    assert rel(out, o.run(x)) < 1e-5
+
+
+def test_datum_tensor_cores_match_cuda_cores():
+    """the tcgen05 GEMM (three TF32 products) against the FP32 CUDA-core
+    kernel on the same inputs"""
+    p, G, x, _ = _survey(150, 140, 20, 12)
+    a = np.empty_like(x)
+    kd.datum_freq(p, G, G, x, a)
+    os.environ["KCIG_DATUM_GEMM"] = "simt"
+    try:
+        b = np.empty_like(x)
+        kd.datum_freq(p, G, G, x, b)
+    finally:
+        del os.environ["KCIG_DATUM_GEMM"]
+    assert rel(a, b) < 2e-6
