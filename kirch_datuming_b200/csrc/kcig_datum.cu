@@ -172,6 +172,7 @@ struct CGemmArgs {
     int lda, ldb, ldc;
     int M, N, K;
     int band, band_rows;
+    int a_trans;           // tensor-core kernel only: A(m, k) at A[k * lda + m]
 };
 
 __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
@@ -248,20 +249,27 @@ __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
 // block [[Br, Bi], [-Bi, Br]] (rows k re/im, columns n re/im), and the real
 // M x 2N result is C in its interleaved layout.
 // CTA tile: 128 rows x 128 complex columns (a 128 x 256 FP32 accumulator,
-// 256 TMEM columns); K in chunks of 8 complex (16 real) through 2 pipeline
+// 256 TMEM columns); K in chunks of 8 complex (16 real) through 4 pipeline
 // stages of 48 KB (hi and lo of A and of the expanded B, canonical K-major
-// layout); warps 0-7 load, split, expand and store the operands and then
-// read the accumulator out, warp 8 allocates TMEM and one of its lanes
-// issues the MMAs.  Every mbarrier wait is bounded; a wait that gives up
-// sets *status, and the CTA stops issuing work, waits (bounded) for its own
-// MMAs and frees its TMEM.
+// layout; A's four 16-byte k-groups are 2080 bytes apart instead of 2048, so
+// that the eight lanes of a quarter-warp store to distinct banks).  Two
+// groups of 8 producer warps take alternate chunks: each loads its next
+// chunk while it splits and stores the current one, so two chunks' loads are
+// in flight; after the main loop all 16 warps read the accumulator out.
+// Warp 16 allocates TMEM and one of its lanes issues the MMAs.  One CTA per
+// SM.  Every mbarrier wait is bounded; a wait that gives up sets *status,
+// and the CTA stops issuing work, waits (bounded) for its own MMAs and frees
+// its TMEM.
 namespace tcg {
-constexpr int TM = 128, TNC = 128, TN = 256, KC = 8, KR = 16, S = 2;
-constexpr int A_BYTES = TM * KR * 4;               // one of hi / lo
-constexpr int B_BYTES = TN * KR * 4;
-constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;   // 48 KB
+constexpr int TM = 128, TNC = 128, TN = 256, KC = 8, KR = 16, S = 4;
+constexpr int AK = TM * 16 + 32;                   // byte stride of A's k-groups (padded)
+constexpr int BK = TN * 16;                        // byte stride of B's k-groups
+constexpr int A_BYTES = 4 * AK;                    // one of hi / lo: 4 k-groups
+constexpr int B_BYTES = 4 * BK;
+constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;   // 48.25 KB
 constexpr int SMEM = S * STAGE + 128;              // + barriers and slots
-constexpr int THREADS = 288;
+constexpr int PRODUCERS = 16;                      // warps
+constexpr int THREADS = 32 * (PRODUCERS + 1);
 }  // namespace tcg
 
 // a bounded mbarrier wait: at most 2^22 polls, each suspending the thread for
@@ -335,28 +343,36 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
         tc::mbar_init(done, 1);
         *abort_flag = 0;
     }
-    if (warp == 8) tc::tmem_alloc(tslot, 256);
+    if (warp == PRODUCERS) tc::tmem_alloc(tslot, 256);
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
     const uint32_t tmem = *tslot;
 
-    if (warp < 8) {
-        // ---- producers: chunk i of 8 complex k into stage i % S.  The
-        // global loads of chunk i+1 are issued before chunk i is split and
-        // stored, so their latency overlaps the stores and the stage wait.
-        const int t = threadIdx.x;  // 0..255
+    if (warp < PRODUCERS) {
+        // ---- producers: group g (warps 8g .. 8g+7) stores chunks g, g+2, ...
+        // into stage i % S; the global loads of its next chunk are issued
+        // before the current one is split and stored.
+        const int g = warp >> 3, t = threadIdx.x & 255;
         float2 xa[2][2], yb[4][2];
         auto load = [&](int i) {
             const int k0 = k_lo + i * KC;
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) {
-                const int e = t + 256 * rr, row = e >> 2, j = e & 3, gm = m0 + row, gk = k0 + 2 * j;
+                // row-major A: 4 lanes per row, along k; transposed A: lanes along the rows
+                const int e = t + 256 * rr;
+                const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
+                const int gm = m0 + row, gk = k0 + 2 * j;
                 xa[rr][0] = xa[rr][1] = make_float2(0.0f, 0.0f);
                 if (gm < a.M) {
-                    const float2 *src = A + (size_t)gm * a.lda;
-                    if (gk < k_hi) xa[rr][0] = src[gk];
-                    if (gk + 1 < k_hi) xa[rr][1] = src[gk + 1];
+                    if (a.a_trans) {
+                        if (gk < k_hi) xa[rr][0] = A[(size_t)gk * a.lda + gm];
+                        if (gk + 1 < k_hi) xa[rr][1] = A[(size_t)(gk + 1) * a.lda + gm];
+                    } else {
+                        const float2 *src = A + (size_t)gm * a.lda;
+                        if (gk < k_hi) xa[rr][0] = src[gk];
+                        if (gk + 1 < k_hi) xa[rr][1] = src[gk + 1];
+                    }
                 }
             }
 #pragma unroll
@@ -369,15 +385,15 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 }
             }
         };
-        if (nchunks > 0) load(0);
-        for (int i = 0; i < nchunks; i++) {
+        if (g < nchunks) load(g);
+        for (int i = g; i < nchunks; i += 2) {
             const int slot = i % S;
             float2 ca[2][2], cb[4][2];
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) ca[rr][0] = xa[rr][0], ca[rr][1] = xa[rr][1];
 #pragma unroll
             for (int rr = 0; rr < 4; rr++) cb[rr][0] = yb[rr][0], cb[rr][1] = yb[rr][1];
-            if (i + 1 < nchunks) load(i + 1);
+            if (i + 2 < nchunks) load(i + 2);
             if (i >= S && !dat_wait(&empty[slot], ((i / S) - 1) & 1)) {
                 atomicExch(status, 1);
                 *abort_flag = 1;
@@ -388,8 +404,9 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
             // A: 128 rows x 4 pairs of complex k -> one 16-byte row segment of a k-group
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) {
-                const int e = t + 256 * rr, row = e >> 2, j = e & 3;
-                const uint32_t off = (uint32_t)(j * (TM * 16) + (row >> 3) * 128 + (row & 7) * 16);
+                const int e = t + 256 * rr;
+                const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
+                const uint32_t off = (uint32_t)(j * AK + (row >> 3) * 128 + (row & 7) * 16);
                 tc_store_split(a_hi, a_lo, off, make_float4(ca[rr][0].x, ca[rr][0].y, ca[rr][1].x, ca[rr][1].y));
             }
             // B: 4 pairs of complex k x 128 complex n, each expanded to the two
@@ -399,7 +416,7 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 const int e = t + 256 * rr, j = e >> 8, rw = e & 255, h = rw & 1;
                 const float2 y0 = cb[rr][0], y1 = cb[rr][1];
                 const float4 v = h ? make_float4(y0.y, y0.x, y1.y, y1.x) : make_float4(y0.x, -y0.y, y1.x, -y1.y);
-                const uint32_t off = (uint32_t)(j * (TN * 16) + (rw >> 3) * 128 + (rw & 7) * 16);
+                const uint32_t off = (uint32_t)(j * BK + (rw >> 3) * 128 + (rw & 7) * 16);
                 tc_store_split(b_hi, b_lo, off, v);
             }
             tc::fence_async_smem();
@@ -421,9 +438,9 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
             const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
 #pragma unroll
             for (int s = 0; s < KR / 8; s++) {
-                const uint32_t ao = s * 2 * (TM * 16), bo = s * 2 * (TN * 16);
-                const uint64_t dah = tc::sdesc(ah + ao, TM * 16, 128), dal = tc::sdesc(al + ao, TM * 16, 128);
-                const uint64_t dbh = tc::sdesc(bh + bo, TN * 16, 128), dbl = tc::sdesc(bl + bo, TN * 16, 128);
+                const uint32_t ao = s * 2 * AK, bo = s * 2 * BK;
+                const uint64_t dah = tc::sdesc(ah + ao, AK, 128), dal = tc::sdesc(al + ao, AK, 128);
+                const uint64_t dbh = tc::sdesc(bh + bo, BK, 128), dbl = tc::sdesc(bl + bo, BK, 128);
                 tc::mma_tf32(tmem, dah, dbh, idesc, (i > 0 || s > 0) ? 1u : 0u);
                 tc::mma_tf32(tmem, dah, dbl, idesc, 1u);
                 tc::mma_tf32(tmem, dal, dbh, idesc, 1u);
@@ -433,19 +450,19 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
         tc::commit(done);  // tracks every MMA issued, also after an abort
     }
     __syncwarp();
-    // ---- epilogue: warps 0-7 read the accumulator; warp w owns TMEM lanes
-    // 32 (w % 4) .. +31 and real columns 128 (w / 4) .. +127
+    // ---- epilogue: warps 0-15 read the accumulator; warp w owns TMEM lanes
+    // 32 (w % 4) .. +31 and real columns 64 (w / 4) .. +63
     bool ok = true;
-    if (warp < 8 || lane == 0) ok = dat_wait(done, 0);
+    if (warp < PRODUCERS || lane == 0) ok = dat_wait(done, 0);
     if (!ok) atomicExch(status, 3);
-    if (warp < 8) {
+    if (warp < PRODUCERS) {
         tc::fence_after();
-        const int q = warp & 3, half = warp >> 2;
+        const int q = warp & 3, quarter = warp >> 2;
         const int gm = m0 + 32 * q + lane;
         const bool live = __all_sync(0xffffffffu, ok && !*abort_flag);  // warp-uniform: TMEM loads are collective
-        for (int cb = 0; cb < 4; cb++) {
+        for (int cb = 0; cb < 2; cb++) {
             float v[32];
-            const int c0 = 128 * half + 32 * cb;  // real column of the tile
+            const int c0 = 64 * quarter + 32 * cb;  // real column of the tile
             if (nchunks > 0 && live) {
                 tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
             } else {
@@ -462,7 +479,7 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == 8) tc::tmem_free(tmem, 256);
+    if (warp == PRODUCERS) tc::tmem_free(tmem, 256);
 }
 
 // cmp = 1 receiver side (:493-546 with s_abs = s0 + is ds): one thread per
@@ -971,6 +988,7 @@ int launch_gemm(const float2 *A, long long sA, int lda, const float2 *B, long lo
                 int &launches)
 {
     CGemmArgs g;
+    g.a_trans = 0;
     g.A = A;
     g.B = B;
     g.C = C;
@@ -1000,9 +1018,10 @@ int launch_gemm(const float2 *A, long long sA, int lda, const float2 *B, long lo
 
 int launch_gemm_tc(const float2 *A, long long sA, int lda, const float2 *B, long long sB, int ldb, float2 *C,
                    long long sC, int ldc, int M, int N, int K, int band, int band_rows, int batch, int *status,
-                   cudaStream_t st, int &launches)
+                   cudaStream_t st, int &launches, int a_trans = 0)
 {
     CGemmArgs g;
+    g.a_trans = a_trans;
     g.A = A;
     g.B = B;
     g.C = C;
@@ -1138,6 +1157,18 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
     Host h;
     KCIG_TRY(build_receiver(p, rtp, h));  // the receiver side's checks come first, as in the reference
     KCIG_TRY(build_source(p, stp, h));
+    // cmp = 0 with shots and receivers on the same positions, tables and
+    // datums: Ks[a][b] == Kr[b][a] term for term, so one operator serves both
+    // sides (the source side reads it transposed) and is built once
+    bool shared_op = p.cmp == 0 && ns == nh && gemm_on_tensor_cores();
+    for (size_t a0 = 0; shared_op && a0 < (size_t)ns; a0++)
+        for (size_t b0 = 0; b0 < (size_t)ns; b0++) {
+            const DatEntry &x = h.src[a0 * ns + b0], &y = h.rcv[b0 * nh + a0];
+            if (memcmp(&x, &y, sizeof(DatEntry)) != 0) {
+                shared_op = false;
+                break;
+            }
+        }
     std::vector<float> wtr((size_t)ntr);
     for (int is = 0; is < ns; is++) {
         const float ws = edge_host(is, ns, p.data_taper);
@@ -1171,7 +1202,7 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
     KCIG_TRY(upload(drcv, h.rcv, st, "receiver terms"));
     KCIG_TRY(upload(dsrc, h.src, st, "source terms"));
     // per-frequency bytes of a chunk: Utmp + both operators
-    const size_t op_r = h.rcv.size(), op_s = h.src.size();
+    const size_t op_r = h.rcv.size(), op_s = shared_op ? 0 : h.src.size();
     const size_t per_f = (interm ? 0 : (size_t)ntr * sizeof(float2)) + (op_r + op_s) * sizeof(float2);
     int chunk = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1536 << 20) / std::max<size_t>(per_f, 1)));
     chunk = std::min(chunk, nw);
@@ -1261,7 +1292,7 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         float2 *Utc = interm ? Ufull.as<float2>() + (size_t)f0 * ntr : Ut.as<float2>();
         KCIG_CUDA(cudaEventRecord(ce[0], st));
         KCIG_TRY(launch_op(drcv, (int)op_r, Kr.as<float2>(), f0, nf, nfft, K, p, st, launches));
-        KCIG_TRY(launch_op(dsrc, (int)op_s, Ks.as<float2>(), f0, nf, nfft, K, p, st, launches));
+        if (op_s) KCIG_TRY(launch_op(dsrc, (int)op_s, Ks.as<float2>(), f0, nf, nfft, K, p, st, launches));
         KCIG_CUDA(cudaEventRecord(ce[1], st));
         if (p.cmp == 0) {
             if (tcore)
@@ -1291,7 +1322,10 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         }
         KCIG_CUDA(cudaEventRecord(ce[2], st));
         if (p.cmp == 0) {
-            if (tcore)
+            if (tcore && shared_op)
+                KCIG_TRY(launch_gemm_tc(Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus.as<int>(), st, launches, 1));
+            else if (tcore)
                 KCIG_TRY(launch_gemm_tc(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
                                         p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus.as<int>(), st, launches));
             else

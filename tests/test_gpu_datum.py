@@ -211,3 +211,32 @@ def test_datum_tensor_cores_match_cuda_cores():
     finally:
         del os.environ["KCIG_DATUM_GEMM"]
     assert rel(a, b) < 2e-6
+
+
+def test_datum_shared_operator_vs_oracle():
+    """shots and receivers on the same positions, one table, one datum: the
+    source operator is the receiver operator transposed term for term, built
+    once and read transposed by the source-side GEMM"""
+    t = META["table"]
+    G = np.ascontiguousarray(GOLD["green"])
+    n, nt, dt = 140, 128, 0.004
+    x = np.random.default_rng(13).standard_normal((n, n, nt)).astype(np.float32)
+    p = kd.datum_params(nt=nt, nh=n, ns=n, dt=dt, h0=0.05, dh=0.005, s0=0.05, ds=0.005, nsg=G.shape[0],
+                        nrg=G.shape[0], sg0=t["o"][2], dsg=t["d"][2], rg0=t["o"][2], drg=t["d"][2], sdatum=0.1,
+                        rdatum=0.1, aperture=30, taper=4, data_taper=3, cmp=0, antialias=1.0, length=0.05)
+    out = np.empty_like(x)
+    kd.datum_freq(p, G, G, x, out)
+    o = D.Datum(nt, n, n, dt, 0.05, 0.005, 0.05, 0.005, G, t["o"][2], t["d"][2], G, t["o"][2], t["d"][2],
+                np.float32(0.1), np.float32(0.1), aperture=30, taper=4, data_taper=3, cmp=0, antialias=1.0,
+                length=0.05)
+    assert rel(out, o.run(x)) < 1e-5
+    ms, _ = kd.datum_last_timing()
+    os.environ["KCIG_DATUM_GEMM"] = "simt"
+    try:
+        b = np.empty_like(x)
+        kd.datum_freq(p, G, G, x, b)
+        ms_simt, _ = kd.datum_last_timing()
+    finally:
+        del os.environ["KCIG_DATUM_GEMM"]
+    assert rel(out, b) < 2e-6
+    assert ms[1] < ms_simt[1]   # one operator built instead of two
