@@ -173,6 +173,7 @@ struct CGemmArgs {
     int M, N, K;
     int band, band_rows;
     int a_trans;           // tensor-core kernel only: A(m, k) at A[k * lda + m]
+    int a_vec;             // tensor-core kernel only: row-major A rows start on 16 bytes (lda, sA even)
 };
 
 __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
@@ -331,7 +332,9 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
     int k_lo = 0, k_hi = a.K;
     if (a.band >= 0) {
         const int c0 = a.band_rows ? m0 : n0, c1 = (a.band_rows ? min(a.M, m0 + TM) : min(a.N, n0 + TNC)) - 1;
-        k_lo = max(0, c0 - a.band);
+        // even start (a 16-byte load covers k, k+1); the term added below the
+        // band has a zero operator entry
+        k_lo = max(0, c0 - a.band) & ~1;
         k_hi = min(a.K, c1 + a.band + 1);
     }
     const int nchunks = k_hi > k_lo ? (k_hi - k_lo + KC - 1) / KC : 0;
@@ -351,11 +354,13 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
 
     if (warp < PRODUCERS) {
         // ---- producers: group g (warps 8g .. 8g+7) stores chunks g, g+2, ...
-        // into stage i % S; the global loads of its next chunk are issued
-        // before the current one is split and stored.
+        // into stage i % S.
         const int g = warp >> 3, t = threadIdx.x & 255;
-        float2 xa[2][2], yb[4][2];
-        auto load = [&](int i) {
+        // the operands of one chunk as this thread loads them: A[2][2], B[4]
+        struct Chunk {
+            float2 a[2][2], b[4];
+        };
+        auto load = [&](int i, Chunk &c) {
             const int k0 = k_lo + i * KC;
 #pragma unroll
             for (int rr = 0; rr < 2; rr++) {
@@ -363,42 +368,49 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 const int e = t + 256 * rr;
                 const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
                 const int gm = m0 + row, gk = k0 + 2 * j;
-                xa[rr][0] = xa[rr][1] = make_float2(0.0f, 0.0f);
+                c.a[rr][0] = c.a[rr][1] = make_float2(0.0f, 0.0f);
                 if (gm < a.M) {
                     if (a.a_trans) {
-                        if (gk < k_hi) xa[rr][0] = A[(size_t)gk * a.lda + gm];
-                        if (gk + 1 < k_hi) xa[rr][1] = A[(size_t)(gk + 1) * a.lda + gm];
+                        if (gk < k_hi) c.a[rr][0] = A[(size_t)gk * a.lda + gm];
+                        if (gk + 1 < k_hi) c.a[rr][1] = A[(size_t)(gk + 1) * a.lda + gm];
                     } else {
                         const float2 *src = A + (size_t)gm * a.lda;
-                        if (gk < k_hi) xa[rr][0] = src[gk];
-                        if (gk + 1 < k_hi) xa[rr][1] = src[gk + 1];
+                        if (a.a_vec && gk + 1 < k_hi) {  // gk is even: one 16-byte load
+                            const float4 q = *reinterpret_cast<const float4 *>(src + gk);
+                            c.a[rr][0] = make_float2(q.x, q.y);
+                            c.a[rr][1] = make_float2(q.z, q.w);
+                        } else {
+                            if (gk < k_hi) c.a[rr][0] = src[gk];
+                            if (gk + 1 < k_hi) c.a[rr][1] = src[gk + 1];
+                        }
                     }
                 }
             }
+            // B: the two lanes of a pair (rows 2n and 2n+1 of the same column)
+            // each load one of the chunk's two k rows; they swap them when the
+            // chunk is stored, so nothing waits on the load here
 #pragma unroll
             for (int rr = 0; rr < 4; rr++) {
-                const int e = t + 256 * rr, j = e >> 8, nc = (e & 255) >> 1, gn = n0 + nc, gk = k0 + 2 * j;
-                yb[rr][0] = yb[rr][1] = make_float2(0.0f, 0.0f);
-                if (gn < a.N) {
-                    if (gk < k_hi) yb[rr][0] = B[(size_t)gk * a.ldb + gn];
-                    if (gk + 1 < k_hi) yb[rr][1] = B[(size_t)(gk + 1) * a.ldb + gn];
-                }
+                const int e = t + 256 * rr, j = e >> 8, nc = (e & 255) >> 1, h = e & 1, gn = n0 + nc;
+                const int gk = k0 + 2 * j + h;
+                c.b[rr] = make_float2(0.0f, 0.0f);
+                if (gn < a.N && gk < k_hi) c.b[rr] = B[(size_t)gk * a.ldb + gn];
             }
         };
-        if (g < nchunks) load(g);
+        // group g takes chunks g, g+2, g+4, ...: the loads of its next chunk
+        // are issued before the current one is split and stored (holding two
+        // chunks ahead in registers measured slower)
+        Chunk nxt;
+        if (g < nchunks) load(g, nxt);
         for (int i = g; i < nchunks; i += 2) {
             const int slot = i % S;
-            float2 ca[2][2], cb[4][2];
-#pragma unroll
-            for (int rr = 0; rr < 2; rr++) ca[rr][0] = xa[rr][0], ca[rr][1] = xa[rr][1];
-#pragma unroll
-            for (int rr = 0; rr < 4; rr++) cb[rr][0] = yb[rr][0], cb[rr][1] = yb[rr][1];
-            if (i + 2 < nchunks) load(i + 2);
+            const Chunk c = nxt;
+            if (i + 2 < nchunks) load(i + 2, nxt);
             if (i >= S && !dat_wait(&empty[slot], ((i / S) - 1) & 1)) {
                 atomicExch(status, 1);
                 *abort_flag = 1;
             }
-            if (*abort_flag) break;
+            if (__any_sync(0xffffffffu, *abort_flag)) break;  // warp-uniform: the stores below shuffle
             uint8_t *st = smem + slot * STAGE;
             uint8_t *a_hi = st, *a_lo = st + A_BYTES, *b_hi = st + 2 * A_BYTES, *b_lo = b_hi + B_BYTES;
             // A: 128 rows x 4 pairs of complex k -> one 16-byte row segment of a k-group
@@ -407,14 +419,17 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 const int e = t + 256 * rr;
                 const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
                 const uint32_t off = (uint32_t)(j * AK + (row >> 3) * 128 + (row & 7) * 16);
-                tc_store_split(a_hi, a_lo, off, make_float4(ca[rr][0].x, ca[rr][0].y, ca[rr][1].x, ca[rr][1].y));
+                tc_store_split(a_hi, a_lo, off, make_float4(c.a[rr][0].x, c.a[rr][0].y, c.a[rr][1].x, c.a[rr][1].y));
             }
             // B: 4 pairs of complex k x 128 complex n, each expanded to the two
             // real rows 2n (C real) and 2n+1 (C imaginary)
 #pragma unroll
             for (int rr = 0; rr < 4; rr++) {
                 const int e = t + 256 * rr, j = e >> 8, rw = e & 255, h = rw & 1;
-                const float2 y0 = cb[rr][0], y1 = cb[rr][1];
+                float2 other;
+                other.x = __shfl_xor_sync(0xffffffffu, c.b[rr].x, 1);
+                other.y = __shfl_xor_sync(0xffffffffu, c.b[rr].y, 1);
+                const float2 y0 = h ? other : c.b[rr], y1 = h ? c.b[rr] : other;
                 const float4 v = h ? make_float4(y0.y, y0.x, y1.y, y1.x) : make_float4(y0.x, -y0.y, y1.x, -y1.y);
                 const uint32_t off = (uint32_t)(j * BK + (rw >> 3) * 128 + (rw & 7) * 16);
                 tc_store_split(b_hi, b_lo, off, v);
@@ -989,6 +1004,7 @@ int launch_gemm(const float2 *A, long long sA, int lda, const float2 *B, long lo
 {
     CGemmArgs g;
     g.a_trans = 0;
+    g.a_vec = 0;
     g.A = A;
     g.B = B;
     g.C = C;
@@ -1022,6 +1038,7 @@ int launch_gemm_tc(const float2 *A, long long sA, int lda, const float2 *B, long
 {
     CGemmArgs g;
     g.a_trans = a_trans;
+    g.a_vec = !a_trans && lda % 2 == 0 && sA % 2 == 0 && ((uintptr_t)A & 15) == 0;
     g.A = A;
     g.B = B;
     g.C = C;
