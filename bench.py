@@ -708,10 +708,10 @@ def datum_section(steps: int, warmup: int, threads: int, T=None, data=None):
     e2e_ms = min(e2e)
     same = bool(np.array_equal(hout, out.cpu().numpy()))
     gemm_ms = st_ms[2] + st_ms[3]
-    # executed tensor work of k_cgemm_tc: per side and frequency ceil(400/128)^2 tiles of a 128 x 256 real
-    # accumulator over 2 x 400 real k, three TF32 products each
-    tiles = math.ceil(NPOS / 128) ** 2
-    tensor_flops = 2 * nw * tiles * (128 * 256 * 2 * NPOS) * 2.0 * 3
+    # executed tensor work of k_cgemm_tc: per side and frequency ceil(400/128) x ceil(400/104) tiles of a
+    # 128 x 208 real accumulator over 2 x 400 real k, three TF32 products each
+    tiles = math.ceil(NPOS / 128) * math.ceil(NPOS / 104)
+    tensor_flops = 2 * nw * tiles * (128 * 208 * 2 * NPOS) * 2.0 * 3
     peak_bf16, peak_src = measured_peaks(kind="tensor")
     tf32_peak = peak_bf16 / 2
     res = {"workload": DAT_WORKLOAD, "nfft": nfft, "frequencies": nw, "nsam": nsam,

@@ -249,8 +249,9 @@ __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
 // M x 2K matrix [.. Ar Ai ..], each complex entry of B becomes the 2x2 real
 // block [[Br, Bi], [-Bi, Br]] (rows k re/im, columns n re/im), and the real
 // M x 2N result is C in its interleaved layout.
-// CTA tile: 128 rows x 128 complex columns (a 128 x 256 FP32 accumulator,
-// 256 TMEM columns); K in chunks of 8 complex (16 real) through 4 pipeline
+// CTA tile: 128 rows x 104 complex columns (a 128 x 208 FP32 accumulator in
+// 256 allocated TMEM columns; 104 covers 400 columns in four tiles with 4%
+// padding, against 28% for 128); K in chunks of 8 complex (16 real) through 4 pipeline
 // stages of 48 KB (hi and lo of A and of the expanded B, canonical K-major
 // layout; A's four 16-byte k-groups are 2080 bytes apart instead of 2048, so
 // that the eight lanes of a quarter-warp store to distinct banks).  Two
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
 // and the CTA stops issuing work, waits (bounded) for its own MMAs and frees
 // its TMEM.
 namespace tcg {
-constexpr int TM = 128, TNC = 128, TN = 256, KC = 8, KR = 16, S = 4;
+constexpr int TM = 128, TNC = 104, TN = 2 * TNC, KC = 8, KR = 16, S = 4;  // TN: a multiple of 16, <= 256
 constexpr int AK = TM * 16 + 32;                   // byte stride of A's k-groups (padded)
 constexpr int BK = TN * 16;                        // byte stride of B's k-groups
 constexpr int A_BYTES = 4 * AK;                    // one of hi / lo: 4 k-groups
@@ -391,10 +392,10 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
             // chunk is stored, so nothing waits on the load here
 #pragma unroll
             for (int rr = 0; rr < 4; rr++) {
-                const int e = t + 256 * rr, j = e >> 8, nc = (e & 255) >> 1, h = e & 1, gn = n0 + nc;
+                const int e = t + 256 * rr, j = e / TN, nc = (e - j * TN) >> 1, h = e & 1, gn = n0 + nc;
                 const int gk = k0 + 2 * j + h;
                 c.b[rr] = make_float2(0.0f, 0.0f);
-                if (gn < a.N && gk < k_hi) c.b[rr] = B[(size_t)gk * a.ldb + gn];
+                if (e < 4 * TN && gn < a.N && gk < k_hi) c.b[rr] = B[(size_t)gk * a.ldb + gn];
             }
         };
         // group g takes chunks g, g+2, g+4, ...: the loads of its next chunk
@@ -421,11 +422,12 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 const uint32_t off = (uint32_t)(j * AK + (row >> 3) * 128 + (row & 7) * 16);
                 tc_store_split(a_hi, a_lo, off, make_float4(c.a[rr][0].x, c.a[rr][0].y, c.a[rr][1].x, c.a[rr][1].y));
             }
-            // B: 4 pairs of complex k x 128 complex n, each expanded to the two
+            // B: 4 pairs of complex k x 104 complex n, each expanded to the two
             // real rows 2n (C real) and 2n+1 (C imaginary)
 #pragma unroll
             for (int rr = 0; rr < 4; rr++) {
-                const int e = t + 256 * rr, j = e >> 8, rw = e & 255, h = rw & 1;
+                const int e = t + 256 * rr, j = e / TN, rw = e - j * TN, h = rw & 1;
+                if (4 * TN < 1024 && e >= 4 * TN) break;  // whole warps: 4 TN is a multiple of 32
                 float2 other;
                 other.x = __shfl_xor_sync(0xffffffffu, c.b[rr].x, 1);
                 other.y = __shfl_xor_sync(0xffffffffu, c.b[rr].y, 1);
@@ -478,6 +480,7 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
         for (int cb = 0; cb < 2; cb++) {
             float v[32];
             const int c0 = 64 * quarter + 32 * cb;  // real column of the tile
+            if (c0 >= TN) break;  // the accumulator's unused columns
             if (nchunks > 0 && live) {
                 tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
             } else {
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 float2 *dst = C + (size_t)gm * a.ldc + n0 + c0 / 2;
 #pragma unroll
                 for (int c = 0; c < 16; c++)
-                    if (n0 + c0 / 2 + c < a.N) dst[c] = make_float2(v[2 * c], v[2 * c + 1]);
+                    if (c0 / 2 + c < TNC && n0 + c0 / 2 + c < a.N) dst[c] = make_float2(v[2 * c], v[2 * c + 1]);
             }
         }
     }
