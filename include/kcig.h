@@ -491,9 +491,17 @@ int kcig_datum_sizes(const kcig_datum_params *p, const float *stable, const floa
  * (KCIG_MEM_DEVICE) memory.  Synchronous on `stream`.  Errors with the
  * reference's texts ("cmp must be 0 or 1.", "Receiver table too small.",
  * "Source table too small.", ...: KCIG_ERR_ARG), KCIG_ERR_NOMEM when the
- * spectra do not fit the device. */
+ * spectra do not fit the device.  The device buffers (the spectra: nfft/2+1
+ * x ns x nh x 8 bytes, the chunk buffers, the cubes of host-memory calls) and
+ * the cuFFT plans stay allocated for the next call on the same device: they
+ * only grow, a call that cannot allocate frees them and tries once more, and
+ * calls on one device run one at a time. */
 int kcig_datum_freq(const kcig_datum_params *p, const float *stable, const float *rtable, const float *in, float *out,
                     float *interm, int memory, void *stream);
+
+/* Frees the buffers and plans kcig_datum_freq keeps for the calling thread's
+ * current device (the next call allocates them again). */
+int kcig_datum_release(void);
 
 /* Device time of the stages of the last kcig_datum_freq call on this thread
  * (ms): forward transforms, operator tables, receiver side, source side,

@@ -160,6 +160,7 @@ def lib():
         L.kcig_datum_sizes.argtypes = [DP, fp, fp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.kcig_datum_freq.argtypes = [DP, vp, vp, vp, vp, vp, ctypes.c_int, vp]
         L.kcig_datum_last_timing.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)]
+        L.kcig_datum_release.argtypes = []
         L.kcig_green_slice.argtypes = ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 7
                                        + [vp, ctypes.c_int, vp])
         L.kcig_run_greensol_auto_cli.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
@@ -734,6 +735,12 @@ def datum_last_timing():
     n = ctypes.c_int()
     _check(lib().kcig_datum_last_timing(ms, ctypes.byref(n)))
     return list(ms), n.value
+
+
+def datum_release():
+    """Free the device buffers and cuFFT plans datum_freq keeps between calls
+    on the current device (kcig_datum_release)."""
+    _check(lib().kcig_datum_release())
 
 
 def green_slice(table, nz: int, nx: int, ngx: int, oz: float, ox: float, dz: float, dx: float, ogx: float,

@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "kcig_common.h"
@@ -750,7 +752,7 @@ int dalloc(DBuf &b, size_t bytes, const char *what)
     if (e != cudaSuccess) {
         cudaGetLastError();
         b.p = nullptr;
-        return set_error(KCIG_ERR_NOMEM, "kcig_datum_freq: cannot allocate %.3f GB for %s on the device",
+        return set_error(KCIG_ERR_NOMEM, "kcig_green_slice: cannot allocate %.3f GB for %s on the device",
                          bytes / 1e9, what);
     }
     return KCIG_OK;
@@ -764,18 +766,179 @@ int upload(DBuf &b, const std::vector<T> &v, cudaStream_t st, const char *what)
     return KCIG_OK;
 }
 
-struct CufftPlan {
-    cufftHandle h = 0;
-    bool ok = false;
-    ~CufftPlan()
-    {
-        if (ok) cufftDestroy(h);
-    }
-};
-
 int cufft_error(cufftResult r, const char *what)
 {
     return set_error(KCIG_ERR_CUDA, "%s failed: cufftResult %d", what, (int)r);
+}
+
+// ---- device buffers and transform plans kept between calls
+// The spectra alone take nw x traces x 8 bytes (10.5 GB for 400 x 400
+// traces and 8193 frequencies); allocating them, planning the transforms and
+// freeing it all again cost a fifth of a call.  One cache per device, held
+// by a call for its whole run (kcig_datum_freq is synchronous on its
+// stream), so calls on one device from several threads run one after the
+// other.  Buffers only grow.  A call that cannot allocate frees every cached
+// buffer and tries once more; kcig_datum_release frees a device's cache.
+enum CacheSlot {
+    CB_U,       // spectra, frequency-major [nw][ntr]
+    CB_UFULL,   // receiver-side spectra kept for interm
+    CB_UT,      // receiver-side spectra of one chunk of frequencies
+    CB_KR,      // receiver operator of one chunk
+    CB_KS,      // source operator of one chunk
+    CB_PAD,     // one batch of padded traces
+    CB_SPEC,    // one batch of trace-major spectra
+    CB_WORK,    // cuFFT work area, shared by the four plans
+    CB_IN,      // host-memory calls: the input, output and interm cubes
+    CB_OUT,
+    CB_INTERM,
+    CB_STATUS,  // tensor-core GEMM status word
+    CB_WTR,     // uploads: trace weights, operator entries, cmp = 1 walk tables
+    CB_RCV,
+    CB_SRC,
+    CB_CABS,
+    CB_GEOM,
+    CB_RTAU,
+    CB_STAU,
+    CB_SL,
+    CB_SR,
+    CB_IHM,
+    CB_IRL,
+    CB_IRH,
+    CB_COUNT
+};
+
+const char *const kSlotName[CB_COUNT] = {
+    "the spectra", "the receiver-side spectra", "the receiver-side chunk", "the receiver operator",
+    "the source operator", "the transform buffer", "the transform buffer", "the transform work area",
+    "the input traces", "the output traces", "the intermediate traces", "a status word", "trace weights",
+    "receiver terms", "source terms", "receiver indices", "receiver weights", "receiver pair times",
+    "source pair times", "gather ranges", "gather ranges", "gather traces", "gather ranges", "gather ranges"};
+
+struct CBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    template <class T>
+    T *as() const
+    {
+        return (T *)p;
+    }
+};
+
+// an R2C / C2R plan pair of one transform length and batch
+struct FftPair {
+    cufftHandle f = 0, b = 0;
+    bool ok = false;
+    int nfft = 0, batch = 0;
+    size_t work = 0;
+};
+
+struct DatumCache {
+    std::mutex mu;
+    CBuf buf[CB_COUNT];
+    FftPair full, tail;
+    std::vector<cudaEvent_t> ev;
+    cudaStream_t copy = nullptr;  // host-memory calls: the cubes' copies, batch by batch
+};
+
+std::mutex g_caches_mu;
+std::map<int, DatumCache *> g_caches;  // never destroyed: the process exit or kcig_datum_release frees them
+
+DatumCache &cache_of(int dev)
+{
+    std::lock_guard<std::mutex> g(g_caches_mu);
+    DatumCache *&c = g_caches[dev];
+    if (!c) c = new DatumCache;
+    return *c;
+}
+
+void free_buffers(DatumCache &c)
+{
+    for (CBuf &b : c.buf) {
+        if (b.p) cudaFree(b.p);
+        b = CBuf{};
+    }
+}
+
+void free_pair(FftPair &q)
+{
+    if (q.ok) {
+        cufftDestroy(q.f);
+        cufftDestroy(q.b);
+    }
+    q = FftPair{};
+}
+
+// the plan pair for (nfft, batch), work area left to the caller
+int make_pair(FftPair &q, int nfft, int nw, int batch)
+{
+    if (q.ok && q.nfft == nfft && q.batch == batch) return KCIG_OK;
+    free_pair(q);
+    cufftResult cr;
+    if ((cr = cufftCreate(&q.f)) != CUFFT_SUCCESS) return cufft_error(cr, "cufftCreate");
+    if ((cr = cufftCreate(&q.b)) != CUFFT_SUCCESS) {
+        cufftDestroy(q.f);
+        q = FftPair{};
+        return cufft_error(cr, "cufftCreate");
+    }
+    q.ok = true;
+    int n = nfft;
+    size_t wf = 0, wb = 0;
+    if ((cr = cufftSetAutoAllocation(q.f, 0)) != CUFFT_SUCCESS || (cr = cufftSetAutoAllocation(q.b, 0)) != CUFFT_SUCCESS) {
+        free_pair(q);
+        return cufft_error(cr, "cufftSetAutoAllocation");
+    }
+    if ((cr = cufftMakePlanMany(q.f, 1, &n, nullptr, 1, nfft, nullptr, 1, nw, CUFFT_R2C, batch, &wf)) != CUFFT_SUCCESS) {
+        free_pair(q);
+        return cufft_error(cr, "cufftPlanMany (R2C)");
+    }
+    if ((cr = cufftMakePlanMany(q.b, 1, &n, nullptr, 1, nw, nullptr, 1, nfft, CUFFT_C2R, batch, &wb)) != CUFFT_SUCCESS) {
+        free_pair(q);
+        return cufft_error(cr, "cufftPlanMany (C2R)");
+    }
+    q.nfft = nfft;
+    q.batch = batch;
+    q.work = std::max(wf, wb);
+    return KCIG_OK;
+}
+
+// every slot at least need[slot] bytes (0: not used by this call)
+int ensure_buffers(DatumCache &c, const size_t *need)
+{
+    for (int attempt = 0; attempt < 2; attempt++) {
+        int bad = -1;
+        for (int i = 0; i < CB_COUNT && bad < 0; i++) {
+            CBuf &b = c.buf[i];
+            if (need[i] == 0 || b.n >= need[i]) continue;
+            if (b.p) cudaFree(b.p);
+            b = CBuf{};
+            if (cudaMalloc(&b.p, need[i]) != cudaSuccess) {
+                cudaGetLastError();
+                b.p = nullptr;
+                bad = i;
+            } else {
+                b.n = need[i];
+            }
+        }
+        if (bad < 0) return KCIG_OK;
+        free_buffers(c);
+        if (attempt == 1)
+            return set_error(KCIG_ERR_NOMEM, "kcig_datum_freq: cannot allocate %.3f GB for %s on the device",
+                             need[bad] / 1e9, kSlotName[bad]);
+    }
+    return KCIG_OK;
+}
+
+template <class T>
+size_t upload_bytes(const std::vector<T> &v)
+{
+    return std::max<size_t>(16, v.size() * sizeof(T));
+}
+
+template <class T>
+int upload_to(const CBuf &b, const std::vector<T> &v, cudaStream_t st)
+{
+    if (!v.empty()) KCIG_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return KCIG_OK;
 }
 
 int validate(const kcig_datum_params &p)
@@ -981,12 +1144,12 @@ int build_source(const kcig_datum_params &p, const float *st, Host &h)
     return KCIG_OK;
 }
 
-int launch_op(const DBuf &ent, int ne, float2 *out, int f0, int nf, int nfft, int K, const kcig_datum_params &p,
+int launch_op(const DatEntry *ent, int ne, float2 *out, int f0, int nf, int nfft, int K, const kcig_datum_params &p,
               cudaStream_t st, int &launches)
 {
     if (ne <= 0) return KCIG_OK;
     DatOpArgs a;
-    a.ent = ent.as<DatEntry>();
+    a.ent = ent;
     a.ne = ne;
     a.out = out;
     a.f0 = f0;
@@ -1079,6 +1242,16 @@ bool gemm_on_tensor_cores()
     return !(e && strcmp(e, "simt") == 0);
 }
 
+// traces per transform batch: as many as keep a batch's padded traces at
+// 1 GB, or KCIG_DATUM_BATCH (smaller batches and a tail batch on small cases)
+long long transform_batch(long long ntr, int nfft)
+{
+    long long b = ((long long)1 << 28) / nfft;
+    const char *e = getenv("KCIG_DATUM_BATCH");
+    if (e && atoll(e) > 0) b = std::min(b, atoll(e));
+    return std::max<long long>(1, std::min<long long>(ntr, b));
+}
+
 }  // namespace
 }  // namespace kcig
 
@@ -1109,6 +1282,22 @@ extern "C" int kcig_datum_sizes(const kcig_datum_params *p, const float *stable,
     if (!p || !stable || !rtable || !nsam || !nfft) return set_error(KCIG_ERR_ARG, "kcig_datum_sizes: null argument");
     KCIG_TRY(validate(*p));
     return sizes(*p, stable, rtable, nsam, nfft);
+}
+
+extern "C" int kcig_datum_release(void)
+{
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    DatumCache &c = cache_of(dev);
+    std::lock_guard<std::mutex> hold(c.mu);
+    free_buffers(c);
+    free_pair(c.full);
+    free_pair(c.tail);
+    for (cudaEvent_t e : c.ev) cudaEventDestroy(e);
+    c.ev.clear();
+    if (c.copy) cudaStreamDestroy(c.copy);
+    c.copy = nullptr;
+    return KCIG_OK;
 }
 
 extern "C" int kcig_datum_last_timing(float *ms5, int *launches)
@@ -1195,140 +1384,179 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         for (int ih = 0; ih < nh; ih++) wtr[(size_t)is * nh + ih] = ws * edge_host(ih, nh, p.data_taper);
     }
 
-    // ---- device buffers
+    // ---- device buffers and transform plans, kept between calls on this device
+    int dev = 0;
+    KCIG_CUDA(cudaGetDevice(&dev));
+    DatumCache &c = cache_of(dev);
+    std::lock_guard<std::mutex> hold(c.mu);
+    // declared after the lock: on every return the stream is idle before
+    // the next call may reuse the buffers
+    struct StreamIdle {
+        cudaStream_t s, s2;
+        ~StreamIdle()
+        {
+            cudaStreamSynchronize(s);
+            if (s2) cudaStreamSynchronize(s2);
+        }
+    } idle{st, nullptr};
     int launches = 0;
     const size_t spec_bytes = (size_t)nw * ntr * sizeof(float2);
-    DBuf din, dout, dim, U, Ufull, dwtr, drcv, dsrc, dextra[8];
-    const float *d_in = in;
-    float *d_out = out, *d_interm = interm;
-    if (memory == KCIG_MEM_HOST) {
-        KCIG_TRY(dalloc(din, (size_t)ntr * nt * 4, "the input traces"));
-        KCIG_CUDA(cudaMemcpyAsync(din.p, in, (size_t)ntr * nt * 4, cudaMemcpyHostToDevice, st));
-        KCIG_TRY(dalloc(dout, (size_t)ntr * nt * 4, "the output traces"));
-        d_in = din.as<float>();
-        d_out = dout.as<float>();
-        if (interm) {
-            KCIG_TRY(dalloc(dim, (size_t)ntr * nt * 4, "the intermediate traces"));
-            d_interm = dim.as<float>();
-        }
-    }
-    KCIG_TRY(dalloc(U, spec_bytes, "the spectra"));
-    DBuf dstatus;
-    KCIG_TRY(dalloc(dstatus, sizeof(int), "a status word"));
-    KCIG_CUDA(cudaMemsetAsync(dstatus.p, 0, sizeof(int), st));
     const bool tcore = gemm_on_tensor_cores();
-    if (interm) KCIG_TRY(dalloc(Ufull, spec_bytes, "the receiver-side spectra"));
-    KCIG_TRY(upload(dwtr, wtr, st, "trace weights"));
-    KCIG_TRY(upload(drcv, h.rcv, st, "receiver terms"));
-    KCIG_TRY(upload(dsrc, h.src, st, "source terms"));
     // per-frequency bytes of a chunk: Utmp + both operators
     const size_t op_r = h.rcv.size(), op_s = shared_op ? 0 : h.src.size();
     const size_t per_f = (interm ? 0 : (size_t)ntr * sizeof(float2)) + (op_r + op_s) * sizeof(float2);
     int chunk = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1536 << 20) / std::max<size_t>(per_f, 1)));
     chunk = std::min(chunk, nw);
-    DBuf Ut, Kr, Ks;
-    if (!interm) KCIG_TRY(dalloc(Ut, (size_t)chunk * ntr * sizeof(float2), "the receiver-side chunk"));
-    KCIG_TRY(dalloc(Kr, (size_t)chunk * std::max<size_t>(op_r, 1) * sizeof(float2), "the receiver operator"));
-    KCIG_TRY(dalloc(Ks, (size_t)chunk * std::max<size_t>(op_s, 1) * sizeof(float2), "the source operator"));
-    DBuf dcabs, dgeom, drtau, dstau, dsl, dsr, dihm, dirl, dirh;
-    if (p.cmp == 1) {
-        KCIG_TRY(upload(dcabs, h.cabs, st, "receiver indices"));
-        KCIG_TRY(upload(dgeom, h.geom, st, "receiver weights"));
-        KCIG_TRY(upload(drtau, h.rtau, st, "receiver pair times"));
-        KCIG_TRY(upload(dstau, h.stau, st, "source pair times"));
-        KCIG_TRY(upload(dsl, h.sleft, st, "gather ranges"));
-        KCIG_TRY(upload(dsr, h.sright, st, "gather ranges"));
-        KCIG_TRY(upload(dihm, h.ihmap, st, "gather traces"));
-        KCIG_TRY(upload(dirl, h.ir_lo, st, "gather ranges"));
-        KCIG_TRY(upload(dirh, h.ir_hi, st, "gather ranges"));
-    }
     // transform batches
-    const long long bmax = std::max<long long>(1, std::min<long long>(ntr, ((long long)1 << 28) / nfft));
-    const int B = (int)bmax;
-    DBuf pad, spec;
-    KCIG_TRY(dalloc(pad, (size_t)B * nfft * 4, "the transform buffer"));
-    KCIG_TRY(dalloc(spec, (size_t)B * nw * sizeof(float2), "the transform buffer"));
-    CufftPlan pf, pb, pf_tail, pb_tail;
-    int n_fft = nfft;
-    cufftResult cr;
-    if ((cr = cufftPlanMany(&pf.h, 1, &n_fft, nullptr, 1, nfft, nullptr, 1, nw, CUFFT_R2C, B)) != CUFFT_SUCCESS)
-        return cufft_error(cr, "cufftPlanMany (R2C)");
-    pf.ok = true;
-    if ((cr = cufftPlanMany(&pb.h, 1, &n_fft, nullptr, 1, nw, nullptr, 1, nfft, CUFFT_C2R, B)) != CUFFT_SUCCESS)
-        return cufft_error(cr, "cufftPlanMany (C2R)");
-    pb.ok = true;
+    const int B = (int)transform_batch(ntr, nfft);
     const int tail = (int)(ntr % B);
-    if (tail) {
-        if ((cr = cufftPlanMany(&pf_tail.h, 1, &n_fft, nullptr, 1, nfft, nullptr, 1, nw, CUFFT_R2C, tail)) != CUFFT_SUCCESS)
-            return cufft_error(cr, "cufftPlanMany (R2C)");
-        pf_tail.ok = true;
-        if ((cr = cufftPlanMany(&pb_tail.h, 1, &n_fft, nullptr, 1, nw, nullptr, 1, nfft, CUFFT_C2R, tail)) != CUFFT_SUCCESS)
-            return cufft_error(cr, "cufftPlanMany (C2R)");
-        pb_tail.ok = true;
+    // plans first (their work area is sized with the buffers); a plan that
+    // does not fit beside the cached buffers gets a second try without them
+    for (int attempt = 0;; attempt++) {
+        int rc = make_pair(c.full, nfft, nw, B);
+        if (rc == KCIG_OK && tail) rc = make_pair(c.tail, nfft, nw, tail);
+        if (rc == KCIG_OK) break;
+        if (attempt == 1) return rc;
+        free_buffers(c);
     }
-    for (CufftPlan *q : {&pf, &pb, &pf_tail, &pb_tail})
-        if (q->ok && (cr = cufftSetStream(q->h, st)) != CUFFT_SUCCESS) return cufft_error(cr, "cufftSetStream");
-
-    cudaEvent_t ev[6];
-    for (auto &e : ev) KCIG_CUDA(cudaEventCreate(&e));
-    struct EvGuard {
-        cudaEvent_t *e;
-        ~EvGuard()
-        {
-            for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]);
+    size_t need[CB_COUNT] = {};
+    need[CB_U] = spec_bytes;
+    if (interm)
+        need[CB_UFULL] = spec_bytes;
+    else
+        need[CB_UT] = (size_t)chunk * ntr * sizeof(float2);
+    need[CB_KR] = (size_t)chunk * std::max<size_t>(op_r, 1) * sizeof(float2);
+    need[CB_KS] = (size_t)chunk * std::max<size_t>(op_s, 1) * sizeof(float2);
+    need[CB_PAD] = (size_t)B * nfft * 4;
+    need[CB_SPEC] = (size_t)B * nw * sizeof(float2);
+    need[CB_WORK] = std::max<size_t>(16, std::max(c.full.work, tail ? c.tail.work : 0));
+    if (memory == KCIG_MEM_HOST) {
+        need[CB_IN] = need[CB_OUT] = (size_t)ntr * nt * 4;
+        if (interm) need[CB_INTERM] = (size_t)ntr * nt * 4;
+    }
+    need[CB_STATUS] = sizeof(int);
+    need[CB_WTR] = upload_bytes(wtr);
+    need[CB_RCV] = upload_bytes(h.rcv);
+    need[CB_SRC] = upload_bytes(h.src);
+    if (p.cmp == 1) {
+        need[CB_CABS] = upload_bytes(h.cabs);
+        need[CB_GEOM] = upload_bytes(h.geom);
+        need[CB_RTAU] = upload_bytes(h.rtau);
+        need[CB_STAU] = upload_bytes(h.stau);
+        need[CB_SL] = upload_bytes(h.sleft);
+        need[CB_SR] = upload_bytes(h.sright);
+        need[CB_IHM] = upload_bytes(h.ihmap);
+        need[CB_IRL] = upload_bytes(h.ir_lo);
+        need[CB_IRH] = upload_bytes(h.ir_hi);
+    }
+    KCIG_TRY(ensure_buffers(c, need));
+    const CBuf *bf = c.buf;
+    cufftResult cr;
+    for (FftPair *q : {&c.full, &c.tail}) {
+        if (q == &c.tail && !tail) continue;
+        for (cufftHandle hq : {q->f, q->b}) {
+            if ((cr = cufftSetWorkArea(hq, bf[CB_WORK].p)) != CUFFT_SUCCESS) return cufft_error(cr, "cufftSetWorkArea");
+            if ((cr = cufftSetStream(hq, st)) != CUFFT_SUCCESS) return cufft_error(cr, "cufftSetStream");
         }
-    } evg{ev};
+    }
+    const float *d_in = in;
+    float *d_out = out, *d_interm = interm;
+    cudaStream_t cs = nullptr;
+    if (memory == KCIG_MEM_HOST) {
+        if (!c.copy) KCIG_CUDA(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking));
+        cs = idle.s2 = c.copy;
+        d_in = bf[CB_IN].as<float>();
+        d_out = bf[CB_OUT].as<float>();
+        if (interm) d_interm = bf[CB_INTERM].as<float>();
+    }
+    KCIG_CUDA(cudaMemsetAsync(bf[CB_STATUS].p, 0, sizeof(int), st));
+    KCIG_TRY(upload_to(bf[CB_WTR], wtr, st));
+    KCIG_TRY(upload_to(bf[CB_RCV], h.rcv, st));
+    KCIG_TRY(upload_to(bf[CB_SRC], h.src, st));
+    if (p.cmp == 1) {
+        KCIG_TRY(upload_to(bf[CB_CABS], h.cabs, st));
+        KCIG_TRY(upload_to(bf[CB_GEOM], h.geom, st));
+        KCIG_TRY(upload_to(bf[CB_RTAU], h.rtau, st));
+        KCIG_TRY(upload_to(bf[CB_STAU], h.stau, st));
+        KCIG_TRY(upload_to(bf[CB_SL], h.sleft, st));
+        KCIG_TRY(upload_to(bf[CB_SR], h.sright, st));
+        KCIG_TRY(upload_to(bf[CB_IHM], h.ihmap, st));
+        KCIG_TRY(upload_to(bf[CB_IRL], h.ir_lo, st));
+        KCIG_TRY(upload_to(bf[CB_IRH], h.ir_hi, st));
+    }
+    float2 *const U = bf[CB_U].as<float2>();
+    float2 *const Kr = bf[CB_KR].as<float2>(), *const Ks = bf[CB_KS].as<float2>();
+    float *const pad = bf[CB_PAD].as<float>();
+    float2 *const spec = bf[CB_SPEC].as<float2>();
+    int *const dstatus = bf[CB_STATUS].as<int>();
+    // events: four stage bounds, four per chunk of frequencies (read once
+    // the call has finished, so the chunks are queued back to back), and for
+    // host-memory calls per batch of traces: its input copied, its interm
+    // and output traces finished
+    const int nchunk = (nw + chunk - 1) / chunk;
+    const int nbatch = (int)((ntr + B - 1) / B);
+    while (c.ev.size() < 4 + 4 * (size_t)nchunk + 3 * (size_t)nbatch) {
+        cudaEvent_t e;
+        KCIG_CUDA(cudaEventCreate(&e));
+        c.ev.push_back(e);
+    }
+    cudaEvent_t *const ev = c.ev.data();
+    cudaEvent_t *const bev = ev + 4 + 4 * nchunk;
+    // host-memory calls: a batch's input goes over on the copy stream while
+    // the batch before it is transformed; its output comes back once its
+    // inverse transform is done, while later batches are transformed
+    auto copy_in = [&](int ib) -> int {
+        const long long t0 = (long long)ib * B;
+        const size_t n = (size_t)std::min<long long>(B, ntr - t0) * nt;
+        KCIG_CUDA(cudaMemcpyAsync(bf[CB_IN].as<float>() + t0 * nt, in + t0 * nt, n * 4, cudaMemcpyHostToDevice, cs));
+        KCIG_CUDA(cudaEventRecord(bev[ib], cs));
+        return KCIG_OK;
+    };
+    if (cs) KCIG_TRY(copy_in(0));
     const int tgrid = 148 * 8;
     KCIG_CUDA(cudaEventRecord(ev[0], st));
     // ---- forward: reverse, taper, pad, R2C, to frequency-major
-    for (long long t0 = 0; t0 < ntr; t0 += B) {
+    for (long long t0 = 0, ib = 0; t0 < ntr; t0 += B, ib++) {
         const int nb = (int)std::min<long long>(B, ntr - t0);
-        k_dat_prep<<<tgrid, 256, 0, st>>>(d_in, dwtr.as<float>(), pad.as<float>(), (int)t0, nb, nt, nfft);
+        if (cs) KCIG_CUDA(cudaStreamWaitEvent(st, bev[ib], 0));
+        k_dat_prep<<<tgrid, 256, 0, st>>>(d_in, bf[CB_WTR].as<float>(), pad, (int)t0, nb, nt, nfft);
         launches++;
         KCIG_CUDA(cudaGetLastError());
-        if ((cr = cufftExecR2C(nb == B ? pf.h : pf_tail.h, pad.as<cufftReal>(), spec.as<cufftComplex>())) != CUFFT_SUCCESS)
+        if ((cr = cufftExecR2C(nb == B ? c.full.f : c.tail.f, (cufftReal *)pad, (cufftComplex *)spec)) != CUFFT_SUCCESS)
             return cufft_error(cr, "cufftExecR2C");
         launches++;
-        k_dat_to_fmajor<<<dim3((nw + 31) / 32, (nb + 31) / 32), dim3(32, 8), 0, st>>>(spec.as<float2>(), U.as<float2>(),
-                                                                                     (int)t0, nb, nw, (int)ntr);
+        k_dat_to_fmajor<<<dim3((nw + 31) / 32, (nb + 31) / 32), dim3(32, 8), 0, st>>>(spec, U, (int)t0, nb, nw,
+                                                                                     (int)ntr);
         launches++;
         KCIG_CUDA(cudaGetLastError());
+        if (cs && ib + 1 < nbatch) KCIG_TRY(copy_in((int)ib + 1));
     }
     KCIG_CUDA(cudaEventRecord(ev[1], st));
     // ---- per chunk of frequencies: operators, receiver side, source side
-    float ms_op = 0.0f, ms_r = 0.0f, ms_s = 0.0f;
-    cudaEvent_t ce[4];
-    for (auto &e : ce) KCIG_CUDA(cudaEventCreate(&e));
-    struct EvGuard4 {
-        cudaEvent_t *e;
-        ~EvGuard4()
-        {
-            for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]);
-        }
-    } evg4{ce};
-    for (int f0 = 0; f0 < nw; f0 += chunk) {
+    for (int f0 = 0, ic = 0; f0 < nw; f0 += chunk, ic++) {
         const int nf = std::min(chunk, nw - f0);
-        float2 *Uc = U.as<float2>() + (size_t)f0 * ntr;
-        float2 *Utc = interm ? Ufull.as<float2>() + (size_t)f0 * ntr : Ut.as<float2>();
+        cudaEvent_t *const ce = ev + 4 + 4 * ic;
+        float2 *Uc = U + (size_t)f0 * ntr;
+        float2 *Utc = interm ? bf[CB_UFULL].as<float2>() + (size_t)f0 * ntr : bf[CB_UT].as<float2>();
         KCIG_CUDA(cudaEventRecord(ce[0], st));
-        KCIG_TRY(launch_op(drcv, (int)op_r, Kr.as<float2>(), f0, nf, nfft, K, p, st, launches));
-        if (op_s) KCIG_TRY(launch_op(dsrc, (int)op_s, Ks.as<float2>(), f0, nf, nfft, K, p, st, launches));
+        KCIG_TRY(launch_op(bf[CB_RCV].as<DatEntry>(), (int)op_r, Kr, f0, nf, nfft, K, p, st, launches));
+        if (op_s) KCIG_TRY(launch_op(bf[CB_SRC].as<DatEntry>(), (int)op_s, Ks, f0, nf, nfft, K, p, st, launches));
         KCIG_CUDA(cudaEventRecord(ce[1], st));
         if (p.cmp == 0) {
             if (tcore)
-                KCIG_TRY(launch_gemm_tc(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
-                                        p.aperture >= 0 ? p.aperture : 0, 0, nf, dstatus.as<int>(), st, launches));
+                KCIG_TRY(launch_gemm_tc(Uc, ntr, nh, Kr, (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
+                                        p.aperture >= 0 ? p.aperture : 0, 0, nf, dstatus, st, launches));
             else
-                KCIG_TRY(launch_gemm(Uc, ntr, nh, Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
+                KCIG_TRY(launch_gemm(Uc, ntr, nh, Kr, (long long)nh * nh, nh, Utc, ntr, nh, ns, nh, nh,
                                      p.aperture >= 0 ? p.aperture : 0, 0, nf, st, launches));
         } else {
             RcvCmp1Args a;
             a.U = Uc;
             a.Utmp = Utc;
-            a.P = Kr.as<float2>();
-            a.Ptau = drtau.as<float>();
-            a.cabs = dcabs.as<int>();
-            a.geom = dgeom.as<float>();
+            a.P = Kr;
+            a.Ptau = bf[CB_RTAU].as<float>();
+            a.cabs = bf[CB_CABS].as<int>();
+            a.geom = bf[CB_GEOM].as<float>();
             a.ns = ns;
             a.nh = nh;
             a.aper = p.aperture;
@@ -1343,26 +1571,26 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         KCIG_CUDA(cudaEventRecord(ce[2], st));
         if (p.cmp == 0) {
             if (tcore && shared_op)
-                KCIG_TRY(launch_gemm_tc(Kr.as<float2>(), (long long)nh * nh, nh, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
-                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus.as<int>(), st, launches, 1));
+                KCIG_TRY(launch_gemm_tc(Kr, (long long)nh * nh, nh, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus, st, launches, 1));
             else if (tcore)
-                KCIG_TRY(launch_gemm_tc(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
-                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus.as<int>(), st, launches));
+                KCIG_TRY(launch_gemm_tc(Ks, (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                                        p.aperture >= 0 ? p.aperture : 0, 1, nf, dstatus, st, launches));
             else
-                KCIG_TRY(launch_gemm(Ks.as<float2>(), (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
+                KCIG_TRY(launch_gemm(Ks, (long long)ns * ns, ns, Utc, ntr, nh, Uc, ntr, nh, ns, nh, ns,
                                      p.aperture >= 0 ? p.aperture : 0, 1, nf, st, launches));
         } else {
             KCIG_CUDA(cudaMemsetAsync(Uc, 0, (size_t)nf * ntr * sizeof(float2), st));
             SrcCmp1Args a;
             a.Utmp = Utc;
             a.Uout = Uc;
-            a.P = Ks.as<float2>();
-            a.Ptau = dstau.as<float>();
-            a.sleft = dsl.as<int>();
-            a.sright = dsr.as<int>();
-            a.ihmap = dihm.as<int>();
-            a.ir_lo = dirl.as<int>();
-            a.ir_hi = dirh.as<int>();
+            a.P = Ks;
+            a.Ptau = bf[CB_STAU].as<float>();
+            a.sleft = bf[CB_SL].as<int>();
+            a.sright = bf[CB_SR].as<int>();
+            a.ihmap = bf[CB_IHM].as<int>();
+            a.ir_lo = bf[CB_IRL].as<int>();
+            a.ir_hi = bf[CB_IRH].as<int>();
             a.ns = ns;
             a.nh = nh;
             a.nr = h.nr;
@@ -1377,8 +1605,53 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
             KCIG_CUDA(cudaGetLastError());
         }
         KCIG_CUDA(cudaEventRecord(ce[3], st));
-        KCIG_CUDA(cudaEventSynchronize(ce[3]));
-        float t;
+    }
+    KCIG_CUDA(cudaEventRecord(ev[2], st));
+    // ---- inverse: to trace-major, C2R, scale, reverse, trim
+    auto inverse = [&](const float2 *Usrc, float *dst, int reverse, cudaEvent_t *done) -> int {
+        for (long long t0 = 0, ib = 0; t0 < ntr; t0 += B, ib++) {
+            const int nb = (int)std::min<long long>(B, ntr - t0);
+            k_dat_to_tmajor<<<dim3((nb + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(Usrc, spec, (int)t0, nb, nw,
+                                                                                         (int)ntr);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+            if ((cr = cufftExecC2R(nb == B ? c.full.b : c.tail.b, (cufftComplex *)spec, (cufftReal *)pad)) != CUFFT_SUCCESS)
+                return cufft_error(cr, "cufftExecC2R");
+            launches++;
+            k_dat_finish<<<tgrid, 256, 0, st>>>(pad, dst, (int)t0, nb, nt, nfft, 1.0f / (float)nfft, reverse);
+            launches++;
+            KCIG_CUDA(cudaGetLastError());
+            if (cs) KCIG_CUDA(cudaEventRecord(done[ib], st));
+        }
+        return KCIG_OK;
+    };
+    cudaEvent_t *const done_im = bev + nbatch, *const done_out = bev + 2 * nbatch;
+    if (interm) KCIG_TRY(inverse(bf[CB_UFULL].as<float2>(), d_interm, 0, done_im));
+    KCIG_TRY(inverse(U, d_out, 1, done_out));
+    KCIG_CUDA(cudaEventRecord(ev[3], st));
+    if (cs) {
+        // queued after every inverse launch, so a copy to pageable memory
+        // (which holds the host until it is done) leaves the device busy
+        auto copy_out = [&](float *host, const float *dev_src, const cudaEvent_t *done) -> int {
+            for (long long t0 = 0, ib = 0; t0 < ntr; t0 += B, ib++) {
+                const size_t n = (size_t)std::min<long long>(B, ntr - t0) * nt;
+                KCIG_CUDA(cudaStreamWaitEvent(cs, done[ib], 0));
+                KCIG_CUDA(cudaMemcpyAsync(host + t0 * nt, dev_src + t0 * nt, n * 4, cudaMemcpyDeviceToHost, cs));
+            }
+            return KCIG_OK;
+        };
+        if (interm) KCIG_TRY(copy_out(interm, d_interm, done_im));
+        KCIG_TRY(copy_out(out, d_out, done_out));
+        KCIG_CUDA(cudaStreamSynchronize(cs));
+    }
+    int dev_status = 0;
+    KCIG_CUDA(cudaMemcpyAsync(&dev_status, dstatus, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KCIG_CUDA(cudaStreamSynchronize(st));
+    if (dev_status)
+        return set_error(KCIG_ERR_DEVICE, "kcig_datum_freq: a tensor-core GEMM gave up waiting (stage %d)", dev_status);
+    float t, ms_op = 0.0f, ms_r = 0.0f, ms_s = 0.0f;
+    for (int ic = 0; ic < nchunk; ic++) {
+        const cudaEvent_t *ce = ev + 4 + 4 * ic;
         cudaEventElapsedTime(&t, ce[0], ce[1]);
         ms_op += t;
         cudaEventElapsedTime(&t, ce[1], ce[2]);
@@ -1386,37 +1659,6 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         cudaEventElapsedTime(&t, ce[2], ce[3]);
         ms_s += t;
     }
-    KCIG_CUDA(cudaEventRecord(ev[2], st));
-    // ---- inverse: to trace-major, C2R, scale, reverse, trim
-    auto inverse = [&](const float2 *Usrc, float *dst, int reverse) -> int {
-        for (long long t0 = 0; t0 < ntr; t0 += B) {
-            const int nb = (int)std::min<long long>(B, ntr - t0);
-            k_dat_to_tmajor<<<dim3((nb + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(Usrc, spec.as<float2>(), (int)t0,
-                                                                                         nb, nw, (int)ntr);
-            launches++;
-            KCIG_CUDA(cudaGetLastError());
-            if ((cr = cufftExecC2R(nb == B ? pb.h : pb_tail.h, spec.as<cufftComplex>(), pad.as<cufftReal>())) != CUFFT_SUCCESS)
-                return cufft_error(cr, "cufftExecC2R");
-            launches++;
-            k_dat_finish<<<tgrid, 256, 0, st>>>(pad.as<float>(), dst, (int)t0, nb, nt, nfft, 1.0f / (float)nfft, reverse);
-            launches++;
-            KCIG_CUDA(cudaGetLastError());
-        }
-        return KCIG_OK;
-    };
-    if (interm) KCIG_TRY(inverse(Ufull.as<float2>(), d_interm, 0));
-    KCIG_TRY(inverse(U.as<float2>(), d_out, 1));
-    KCIG_CUDA(cudaEventRecord(ev[3], st));
-    if (memory == KCIG_MEM_HOST) {
-        KCIG_CUDA(cudaMemcpyAsync(out, d_out, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
-        if (interm) KCIG_CUDA(cudaMemcpyAsync(interm, d_interm, (size_t)ntr * nt * 4, cudaMemcpyDeviceToHost, st));
-    }
-    int dev_status = 0;
-    KCIG_CUDA(cudaMemcpyAsync(&dev_status, dstatus.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    KCIG_CUDA(cudaStreamSynchronize(st));
-    if (dev_status)
-        return set_error(KCIG_ERR_DEVICE, "kcig_datum_freq: a tensor-core GEMM gave up waiting (stage %d)", dev_status);
-    float t;
     cudaEventElapsedTime(&t, ev[0], ev[1]);
     g_last_ms[0] = t;
     g_last_ms[1] = ms_op;

@@ -240,3 +240,96 @@ def test_datum_shared_operator_vs_oracle():
         del os.environ["KCIG_DATUM_GEMM"]
     assert rel(out, b) < 2e-6
     assert ms[1] < ms_simt[1]   # one operator built instead of two
+
+
+def test_datum_buffers_kept_between_calls():
+    """the device buffers and cuFFT plans kept between calls: a survey run
+    on fresh buffers, after a larger survey (larger buffers, other plans),
+    after a cmp = 1 host-memory call with interm, and after datum_release
+    gives the same traces bit for bit; so does the larger one run again"""
+    ps, G, xs, o = _survey(40, 30, 20, 21)
+    pl, _, xl, _ = _survey(150, 140, 20, 22)
+    p1, d1, c1 = params_of("cmp1_jump")
+
+    def run(p, x, im=None):
+        out = np.empty_like(x)
+        kd.datum_freq(p, G, G, np.ascontiguousarray(x), out, im)
+        return out
+
+    kd.datum_release()
+    first = run(ps, xs)
+    big = run(pl, xl)
+    after_big = run(ps, xs)
+    im = np.empty_like(d1)
+    run(p1, d1, im)
+    after_cmp1 = run(ps, xs)
+    kd.datum_release()
+    after_release = run(ps, xs)
+    big_again = run(pl, xl)
+    for got in (after_big, after_cmp1, after_release):
+        assert np.array_equal(got, first)
+    assert np.array_equal(big_again, big)
+    assert rel(first, o.run(xs)) < 1e-5
+
+
+def test_datum_calls_from_two_threads():
+    """two threads calling at once (one device, so one after the other
+    inside the library) get what one thread gets"""
+    import threading
+    pa, G, xa, _ = _survey(60, 50, 20, 23)
+    pb, _, xb, _ = _survey(90, 40, 10, 24, cmp=1)
+    want = []
+    for p, x in ((pa, xa), (pb, xb)):
+        out = np.empty_like(x)
+        kd.datum_freq(p, G, G, x, out)
+        want.append(out)
+    got = [np.empty_like(xa), np.empty_like(xb)]
+    errors = []
+
+    def work(i, p, x):
+        try:
+            for _ in range(3):
+                kd.datum_freq(p, G, G, x, got[i])
+        except Exception as e:  # noqa: BLE001
+            errors.append(e)
+
+    th = [threading.Thread(target=work, args=(0, pa, xa)), threading.Thread(target=work, args=(1, pb, xb))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("memory", ["host", "device"])
+def test_datum_transform_batches(memory):
+    """traces transformed in batches of 500 (three batches, the last one of
+    200 traces on its own plan; the host-memory cube copied batch by batch
+    beside the transforms) give the one-batch result within FP32 rounding,
+    the oracle's within 1e-5, and host and device memory agree bit for bit"""
+    p, G, x, o = _survey(40, 30, 20, 25, cmp=1)
+    one = np.empty_like(x)
+    kd.datum_freq(p, G, G, x, one)
+    os.environ["KCIG_DATUM_BATCH"] = "500"
+    try:
+        if memory == "host":
+            got = np.empty_like(x)
+            im = np.empty_like(x)
+            kd.datum_freq(p, G, G, x, got, im)
+        else:
+            Gd = torch.from_numpy(G).cuda()
+            out_d = torch.empty((40, 30, 128), device="cuda")
+            im_d = torch.empty_like(out_d)
+            kd.datum_freq(p, Gd, Gd, torch.from_numpy(x).cuda(), out_d, im_d)
+            torch.cuda.synchronize()
+            got, im = out_d.cpu().numpy(), im_d.cpu().numpy()
+        other = np.empty_like(x)
+        kd.datum_freq(p, G, G, x, other)
+    finally:
+        del os.environ["KCIG_DATUM_BATCH"]
+    assert rel(got, one) < 1e-6
+    assert rel(got, o.run(x)) < 1e-5
+    assert np.array_equal(other, got)
+    want = o.run(x, interm=True)[1]
+    assert rel(im, want) < 1e-5
