@@ -195,8 +195,7 @@ int kcig_leg_fields_device(kcig_plan *plan, int is_source, double pos, double *T
  * the device tables [npos][nx][nz]; gradx/gradz are the optional device
  * gradient volumes (both or NULL); outputs are caller-owned device arrays
  * [nx][nz] (any may be NULL).  The first call on a device looks up the
- * scratch array's device address, so make that first call before any stream
- * capture.  The address is kept for the life of the process: do not call
+ * scratch array's device address.  The address is kept for the life of the process: do not call
  * this entry point again after cudaDeviceReset on that device.  All calls share the one array and leave the last call's contents
  * in it (every value is written before it is read, so nothing needs clearing);
  * calls that overlap on the GPU -- from other threads or other streams --
