@@ -731,7 +731,7 @@ def datum_section(steps: int, warmup: int, threads: int, T=None, data=None):
                         "useful_frac": datum_terms(NPOS, NPOS, DAT_ARGS["aperture"]) * 8.0 * 3 * nw
                                        / tensor_flops,
                         "note": "executed TF32 tensor flops (3 products per FP32 product, padded 128-row / "
-                                "128-column tiles); useful_frac = the exact operator's terms over the executed "
+                                "104-column tiles); useful_frac = the exact operator's terms over the executed "
                                 "products"},
            "unit_note": "a term is one (output trace, input trace, frequency) product of the exact operator, "
                         "receiver and source sides; the reference's butterfly approximates these sums"}

@@ -606,30 +606,41 @@ __global__ void __launch_bounds__(128) k_dat_src_cmp1(const SrcCmp1Args a)
     }
 }
 
-// reverse in time, edge taper and zero-pad one batch of traces (:287-306)
+// reverse in time, edge taper and zero-pad one batch of traces (:287-306):
+// a thread writes four consecutive samples of a padded trace (one 16-byte
+// store; nfft is a power of two >= 4), up to 1024 block rows walk the
+// batch's traces (several traces per block: ~10 waves at full size)
 __global__ void k_dat_prep(const float *in, const float *wtr, float *pad, int tr0, int nb, int nt, int nfft)
 {
-    const size_t n = (size_t)nb * nfft;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int b = (int)(i / nfft), t = (int)(i - (size_t)b * nfft);
-        float v = 0.0f;
-        if (t < nt) {
-            const float w = wtr[tr0 + b];
-            const float x = in[(size_t)(tr0 + b) * nt + (nt - 1 - t)];
-            v = w == 1.0f ? x : __fmul_rn(w, x);
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (nfft >> 2)) return;
+    for (int b = blockIdx.y; b < nb; b += gridDim.y) {
+        const float w = wtr[tr0 + b];
+        const float *src = in + (size_t)(tr0 + b) * nt + (nt - 1);  // src[-t]: sample nt - 1 - t
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int t = 4 * q + j;
+            float x = 0.0f;
+            if (t < nt) {
+                const float y = src[-t];
+                x = w == 1.0f ? y : __fmul_rn(w, y);
+            }
+            v[j] = x;
         }
-        pad[i] = v;
+        reinterpret_cast<float4 *>(pad + (size_t)b * nfft)[q] = make_float4(v[0], v[1], v[2], v[3]);
     }
 }
 
-// scale by 1/nfft, optionally reverse, trim to nt (:476-487)
+// scale by 1/nfft, optionally reverse, trim to nt (:476-487): threads along
+// the output samples, up to 1024 block rows walk the batch's traces
 __global__ void k_dat_finish(const float *pad, float *out, int tr0, int nb, int nt, int nfft, float scale, int reverse)
 {
-    const size_t n = (size_t)nb * nt;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int b = (int)(i / nt), t = (int)(i - (size_t)b * nt);
-        out[(size_t)(tr0 + b) * nt + t] = __fmul_rn(pad[(size_t)b * nfft + (reverse ? nt - 1 - t : t)], scale);
-    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int ts = reverse ? nt - 1 - t : t;
+    for (int b = blockIdx.y; b < nb; b += gridDim.y)
+        out[(size_t)(tr0 + b) * nt + t] = __fmul_rn(pad[(size_t)b * nfft + ts], scale);
 }
 
 // tiled transposes between spec[b][nw] (a batch of traces) and U[iw][ntr]
@@ -1360,6 +1371,7 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
     }
     int nsam = 0, nfft = 0;
     KCIG_TRY(sizes(p, stp, rtp, &nsam, &nfft));
+    if (nfft < 4) return set_error(KCIG_ERR_ARG, "kcig_datum_freq: transform length %d below 4", nfft);
     const int nw = nfft / 2 + 1, K = nsam - 1;
     const int ns = p.ns, nh = p.nh, nt = p.nt;
     const long long ntr = (long long)ns * nh;
@@ -1513,13 +1525,13 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
         return KCIG_OK;
     };
     if (cs) KCIG_TRY(copy_in(0));
-    const int tgrid = 148 * 8;
     KCIG_CUDA(cudaEventRecord(ev[0], st));
     // ---- forward: reverse, taper, pad, R2C, to frequency-major
     for (long long t0 = 0, ib = 0; t0 < ntr; t0 += B, ib++) {
         const int nb = (int)std::min<long long>(B, ntr - t0);
         if (cs) KCIG_CUDA(cudaStreamWaitEvent(st, bev[ib], 0));
-        k_dat_prep<<<tgrid, 256, 0, st>>>(d_in, bf[CB_WTR].as<float>(), pad, (int)t0, nb, nt, nfft);
+        k_dat_prep<<<dim3((nfft / 4 + 255) / 256, std::min(nb, 1024)), 256, 0, st>>>(d_in, bf[CB_WTR].as<float>(), pad,
+                                                                                    (int)t0, nb, nt, nfft);
         launches++;
         KCIG_CUDA(cudaGetLastError());
         if ((cr = cufftExecR2C(nb == B ? c.full.f : c.tail.f, (cufftReal *)pad, (cufftComplex *)spec)) != CUFFT_SUCCESS)
@@ -1618,7 +1630,8 @@ extern "C" int kcig_datum_freq(const kcig_datum_params *pp, const float *stable,
             if ((cr = cufftExecC2R(nb == B ? c.full.b : c.tail.b, (cufftComplex *)spec, (cufftReal *)pad)) != CUFFT_SUCCESS)
                 return cufft_error(cr, "cufftExecC2R");
             launches++;
-            k_dat_finish<<<tgrid, 256, 0, st>>>(pad, dst, (int)t0, nb, nt, nfft, 1.0f / (float)nfft, reverse);
+            k_dat_finish<<<dim3((nt + 255) / 256, std::min(nb, 1024)), 256, 0, st>>>(pad, dst, (int)t0, nb, nt, nfft,
+                                                                                  1.0f / (float)nfft, reverse);
             launches++;
             KCIG_CUDA(cudaGetLastError());
             if (cs) KCIG_CUDA(cudaEventRecord(done[ib], st));
