@@ -710,10 +710,11 @@ def datum_section(steps: int, warmup: int, threads: int, T=None, data=None):
     e2e_ms = min(e2e)
     same = bool(np.array_equal(hout, out.cpu().numpy()))
     gemm_ms = st_ms[2] + st_ms[3]
-    # executed tensor work of k_cgemm_tc: per side and frequency ceil(400/128) x ceil(400/104) tiles of a
-    # 128 x 208 real accumulator over 2 x 400 real k, three TF32 products each
-    tiles = math.ceil(NPOS / 128) * math.ceil(NPOS / 104)
-    tensor_flops = 2 * nw * tiles * (128 * 208 * 2 * NPOS) * 2.0 * 3
+    # executed tensor work of k_cgemm_tc: per side and frequency ceil(400/128) x ceil(400/208) tiles of
+    # 128 rows x 208 complex columns, four real products (Ar.Br, Ai.Bi, Ar.Bi, Ai.Br) over 400 k, three TF32
+    # products each
+    tiles = math.ceil(NPOS / 128) * math.ceil(NPOS / 208)
+    tensor_flops = 2 * nw * tiles * (128 * 208 * NPOS) * 2.0 * 4 * 3
     peak_bf16, peak_src = measured_peaks(kind="tensor")
     tf32_peak = peak_bf16 / 2
     res = {"workload": DAT_WORKLOAD, "nfft": nfft, "frequencies": nw, "nsam": nsam,
@@ -731,7 +732,7 @@ def datum_section(steps: int, warmup: int, threads: int, T=None, data=None):
                         "useful_frac": datum_terms(NPOS, NPOS, DAT_ARGS["aperture"]) * 8.0 * 3 * nw
                                        / tensor_flops,
                         "note": "executed TF32 tensor flops (3 products per FP32 product, padded 128-row / "
-                                "104-column tiles); useful_frac = the exact operator's terms over the executed "
+                                "208-column tiles); useful_frac = the exact operator's terms over the executed "
                                 "products"},
            "unit_note": "a term is one (output trace, input trace, frequency) product of the exact operator, "
                         "receiver and source sides; the reference's butterfly approximates these sums"}

@@ -243,37 +243,42 @@ __global__ void __launch_bounds__(256) k_cgemm(const CGemmArgs a)
 }
 
 // The same batched complex GEMM on the tensor cores (tcgen05, kind::tf32,
-// accumulator in TMEM) with FP32 accuracy from three TF32 products:
+// accumulators in TMEM) with FP32 accuracy from three TF32 products:
 // x = hi + lo (hi = TF32(x), lo = TF32(x - hi), both rounded to nearest),
 // a.b ~ ah.bh + ah.bl + al.bh,
 // the dropped al.bl and the TF32 rounding of lo being ~2^-22 relative.
-// The complex product is one real GEMM: A viewed as floats is the real
-// M x 2K matrix [.. Ar Ai ..], each complex entry of B becomes the 2x2 real
-// block [[Br, Bi], [-Bi, Br]] (rows k re/im, columns n re/im), and the real
-// M x 2N result is C in its interleaved layout.
-// CTA tile: 128 rows x 104 complex columns (a 128 x 208 FP32 accumulator in
-// 256 allocated TMEM columns; 104 covers 400 columns in four tiles with 4%
-// padding, against 28% for 128); K in chunks of 8 complex (16 real) through 4 pipeline
-// stages of 48 KB (hi and lo of A and of the expanded B, canonical K-major
-// layout; A's four 16-byte k-groups are 2080 bytes apart instead of 2048, so
-// that the eight lanes of a quarter-warp store to distinct banks).  Two
-// groups of 8 producer warps take alternate chunks: each loads its next
-// chunk while it splits and stores the current one, so two chunks' loads are
-// in flight; after the main loop all 16 warps read the accumulator out.
-// Warp 16 allocates TMEM and one of its lanes issues the MMAs.  One CTA per
-// SM.  Every mbarrier wait is bounded; a wait that gives up sets *status,
-// and the CTA stops issuing work, waits (bounded) for its own MMAs and frees
-// its TMEM.
+// The complex product runs as four real products on separate real and
+// imaginary planes of both operands: Cr = Ar.Br - Ai.Bi and Ci = Ar.Bi +
+// Ai.Br, the minus by the instruction's negate-A bit, so no operand value is
+// stored twice.  CTA tile: 128 rows x TNC complex columns (Cr and Ci each a
+// 128 x TNC FP32 accumulator in TMEM); K in chunks of 8 complex through S
+// pipeline stages, each holding the hi and lo of Ar, Ai (128 x 8) and Br, Bi
+// (TNC x 8) in the canonical K-major layout.  Two groups of 8 producer warps
+// take alternate chunks: each loads its next chunk while it splits and
+// stores the current one; after the main loop all 16 warps read the
+// accumulators out.  Warp 16 allocates TMEM and one of its lanes issues the
+// MMAs (12 per chunk).  One CTA per SM.  Every mbarrier wait is bounded; a
+// wait that gives up sets *status, and the CTA stops issuing work, waits
+// (bounded) for its own MMAs and frees its TMEM.
+#ifndef KCIG_CGEMM_TNC
+#define KCIG_CGEMM_TNC 208  // complex columns of a CTA tile: 400 columns in two tiles (4% padding)
+#endif
+#ifndef KCIG_CGEMM_STAGES
+#define KCIG_CGEMM_STAGES 4
+#endif
 namespace tcg {
-constexpr int TM = 128, TNC = 104, TN = 2 * TNC, KC = 8, KR = 16, S = 4;  // TN: a multiple of 16, <= 256
-constexpr int AK = TM * 16 + 32;                   // byte stride of A's k-groups (padded)
-constexpr int BK = TN * 16;                        // byte stride of B's k-groups
-constexpr int A_BYTES = 4 * AK;                    // one of hi / lo: 4 k-groups
-constexpr int B_BYTES = 4 * BK;
-constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;   // 48.25 KB
-constexpr int SMEM = S * STAGE + 128;              // + barriers and slots
-constexpr int PRODUCERS = 16;                      // warps
+constexpr int TM = 128, TNC = KCIG_CGEMM_TNC, KC = 8, S = KCIG_CGEMM_STAGES;
+static_assert(TNC % 16 == 0 && TNC >= 16 && TNC <= 256, "an M = 128 MMA takes N = 16 .. 256 in steps of 16");
+constexpr int TMEM_COLS = TNC <= 64 ? 128 : TNC <= 128 ? 256 : 512;  // Cr at column 0, Ci at TMEM_COLS / 2
+constexpr int AK = TM * 16 + 32;                    // byte stride of an A plane's two k-groups (padded)
+constexpr int BK = TNC * 16;                        // byte stride of a B plane's two k-groups
+constexpr int A_PLANE = 2 * AK, B_PLANE = 2 * BK;   // one plane: 8 real k = two 16-byte k-groups
+constexpr int STAGE = 4 * A_PLANE + 4 * B_PLANE;    // Ar, Ai, Br, Bi, each hi and lo
+constexpr int SMEM = S * STAGE + 128;               // + barriers and slots
+constexpr int PRODUCERS = 16;                       // warps
 constexpr int THREADS = 32 * (PRODUCERS + 1);
+constexpr int RB = (2 * TNC + 255) / 256;           // B items (column, k-group) per producer thread
+static_assert(SMEM <= 227 * 1024, "shared memory of one CTA");
 }  // namespace tcg
 
 // a bounded mbarrier wait: at most 2^22 polls, each suspending the thread for
@@ -317,6 +322,15 @@ __device__ __forceinline__ void tc_store_split(uint8_t *hi, uint8_t *lo, uint32_
     *reinterpret_cast<float4 *>(lo + off) = l;
 }
 
+// the real parts and the imaginary parts of four complex values, split into
+// TF32 hi / lo, into one 16-byte row segment of the four planes re_hi, re_lo,
+// im_hi, im_lo (`plane` bytes apart, in that order)
+__device__ __forceinline__ void tc_store_planes(uint8_t *base, int plane, uint32_t off, const float2 *v)
+{
+    tc_store_split(base, base + plane, off, make_float4(v[0].x, v[1].x, v[2].x, v[3].x));
+    tc_store_split(base + 2 * plane, base + 3 * plane, off, make_float4(v[0].y, v[1].y, v[2].y, v[3].y));
+}
+
 __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a, int *status)
 {
     using namespace tcg;
@@ -335,8 +349,8 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
     int k_lo = 0, k_hi = a.K;
     if (a.band >= 0) {
         const int c0 = a.band_rows ? m0 : n0, c1 = (a.band_rows ? min(a.M, m0 + TM) : min(a.N, n0 + TNC)) - 1;
-        // even start (a 16-byte load covers k, k+1); the term added below the
-        // band has a zero operator entry
+        // even start (16-byte loads of A cover k, k+1); the terms added below
+        // the band have zero operator entries
         k_lo = max(0, c0 - a.band) & ~1;
         k_hi = min(a.K, c1 + a.band + 1);
     }
@@ -349,7 +363,7 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
         tc::mbar_init(done, 1);
         *abort_flag = 0;
     }
-    if (warp == PRODUCERS) tc::tmem_alloc(tslot, 256);
+    if (warp == PRODUCERS) tc::tmem_alloc(tslot, TMEM_COLS);
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
@@ -357,52 +371,52 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
 
     if (warp < PRODUCERS) {
         // ---- producers: group g (warps 8g .. 8g+7) stores chunks g, g+2, ...
-        // into stage i % S.
+        // into stage i % S.  A item: (row t % 128, k-group t / 128), four
+        // complex k; B item e: (column e % TNC, k-group e / TNC), four complex k
         const int g = warp >> 3, t = threadIdx.x & 255;
-        // the operands of one chunk as this thread loads them: A[2][2], B[4]
         struct Chunk {
-            float2 a[2][2], b[4];
+            float2 a[4], b[RB][4];
         };
+        const int arow = t & 127, aj = t >> 7;
         auto load = [&](int i, Chunk &c) {
-            const int k0 = k_lo + i * KC;
+            const int k0 = k_lo + i * KC + 4 * aj;  // even
+            const int gm = m0 + arow;
 #pragma unroll
-            for (int rr = 0; rr < 2; rr++) {
-                // row-major A: 4 lanes per row, along k; transposed A: lanes along the rows
-                const int e = t + 256 * rr;
-                const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
-                const int gm = m0 + row, gk = k0 + 2 * j;
-                c.a[rr][0] = c.a[rr][1] = make_float2(0.0f, 0.0f);
-                if (gm < a.M) {
-                    if (a.a_trans) {
-                        if (gk < k_hi) c.a[rr][0] = A[(size_t)gk * a.lda + gm];
-                        if (gk + 1 < k_hi) c.a[rr][1] = A[(size_t)(gk + 1) * a.lda + gm];
+            for (int q = 0; q < 4; q++) c.a[q] = make_float2(0.0f, 0.0f);
+            if (gm < a.M) {
+                if (a.a_trans) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        if (k0 + q < k_hi) c.a[q] = A[(size_t)(k0 + q) * a.lda + gm];
+                } else {
+                    const float2 *src = A + (size_t)gm * a.lda + k0;
+                    if (a.a_vec && k0 + 3 < k_hi) {  // two 16-byte loads
+                        const float4 p = *reinterpret_cast<const float4 *>(src);
+                        const float4 r = *reinterpret_cast<const float4 *>(src + 2);
+                        c.a[0] = make_float2(p.x, p.y);
+                        c.a[1] = make_float2(p.z, p.w);
+                        c.a[2] = make_float2(r.x, r.y);
+                        c.a[3] = make_float2(r.z, r.w);
                     } else {
-                        const float2 *src = A + (size_t)gm * a.lda;
-                        if (a.a_vec && gk + 1 < k_hi) {  // gk is even: one 16-byte load
-                            const float4 q = *reinterpret_cast<const float4 *>(src + gk);
-                            c.a[rr][0] = make_float2(q.x, q.y);
-                            c.a[rr][1] = make_float2(q.z, q.w);
-                        } else {
-                            if (gk < k_hi) c.a[rr][0] = src[gk];
-                            if (gk + 1 < k_hi) c.a[rr][1] = src[gk + 1];
-                        }
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            if (k0 + q < k_hi) c.a[q] = src[q];
                     }
                 }
             }
-            // B: the two lanes of a pair (rows 2n and 2n+1 of the same column)
-            // each load one of the chunk's two k rows; they swap them when the
-            // chunk is stored, so nothing waits on the load here
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const int e = t + 256 * rr, j = e / TN, nc = (e - j * TN) >> 1, h = e & 1, gn = n0 + nc;
-                const int gk = k0 + 2 * j + h;
-                c.b[rr] = make_float2(0.0f, 0.0f);
-                if (e < 4 * TN && gn < a.N && gk < k_hi) c.b[rr] = B[(size_t)gk * a.ldb + gn];
+            for (int rr = 0; rr < RB; rr++) {
+                const int e = t + 256 * rr, j = e / TNC, n = e - j * TNC, gn = n0 + n;
+                const int kb = k_lo + i * KC + 4 * j;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    c.b[rr][q] = make_float2(0.0f, 0.0f);
+                    if (e < 2 * TNC && gn < a.N && kb + q < k_hi) c.b[rr][q] = B[(size_t)(kb + q) * a.ldb + gn];
+                }
             }
         };
         // group g takes chunks g, g+2, g+4, ...: the loads of its next chunk
-        // are issued before the current one is split and stored (holding two
-        // chunks ahead in registers measured slower)
+        // are issued before the current one is split and stored
         Chunk nxt;
         if (g < nchunks) load(g, nxt);
         for (int i = g; i < nchunks; i += 2) {
@@ -413,38 +427,26 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
                 atomicExch(status, 1);
                 *abort_flag = 1;
             }
-            if (__any_sync(0xffffffffu, *abort_flag)) break;  // warp-uniform: the stores below shuffle
+            if (__any_sync(0xffffffffu, *abort_flag)) break;  // warp-uniform, as the arrival below is per warp
             uint8_t *st = smem + slot * STAGE;
-            uint8_t *a_hi = st, *a_lo = st + A_BYTES, *b_hi = st + 2 * A_BYTES, *b_lo = b_hi + B_BYTES;
-            // A: 128 rows x 4 pairs of complex k -> one 16-byte row segment of a k-group
+            // row r of a plane, k-group j: j * stride + (r / 8) * 128 + (r % 8) * 16
+            tc_store_planes(st, A_PLANE, (uint32_t)(aj * AK + (arow >> 3) * 128 + (arow & 7) * 16), c.a);
 #pragma unroll
-            for (int rr = 0; rr < 2; rr++) {
-                const int e = t + 256 * rr;
-                const int row = a.a_trans ? (e & 127) : (e >> 2), j = a.a_trans ? (e >> 7) : (e & 3);
-                const uint32_t off = (uint32_t)(j * AK + (row >> 3) * 128 + (row & 7) * 16);
-                tc_store_split(a_hi, a_lo, off, make_float4(c.a[rr][0].x, c.a[rr][0].y, c.a[rr][1].x, c.a[rr][1].y));
-            }
-            // B: 4 pairs of complex k x 104 complex n, each expanded to the two
-            // real rows 2n (C real) and 2n+1 (C imaginary)
-#pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const int e = t + 256 * rr, j = e / TN, rw = e - j * TN, h = rw & 1;
-                if (4 * TN < 1024 && e >= 4 * TN) break;  // whole warps: 4 TN is a multiple of 32
-                float2 other;
-                other.x = __shfl_xor_sync(0xffffffffu, c.b[rr].x, 1);
-                other.y = __shfl_xor_sync(0xffffffffu, c.b[rr].y, 1);
-                const float2 y0 = h ? other : c.b[rr], y1 = h ? c.b[rr] : other;
-                const float4 v = h ? make_float4(y0.y, y0.x, y1.y, y1.x) : make_float4(y0.x, -y0.y, y1.x, -y1.y);
-                const uint32_t off = (uint32_t)(j * BK + (rw >> 3) * 128 + (rw & 7) * 16);
-                tc_store_split(b_hi, b_lo, off, v);
+            for (int rr = 0; rr < RB; rr++) {
+                const int e = t + 256 * rr, j = e / TNC, n = e - j * TNC;
+                if (e < 2 * TNC)
+                    tc_store_planes(st + 4 * A_PLANE, B_PLANE, (uint32_t)(j * BK + (n >> 3) * 128 + (n & 7) * 16),
+                                    c.b[rr]);
             }
             tc::fence_async_smem();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&full[slot]);
         }
     } else if (lane == 0) {
-        // ---- MMA issuer
-        const uint32_t idesc = tc::idesc_tf32(TM, TN);
+        // ---- MMA issuer: Cr += Ar.Br - Ai.Bi, Ci += Ar.Bi + Ai.Br, three
+        // TF32 products each
+        const uint32_t id = tc::idesc_tf32(TM, TNC), id_neg = id | (1u << 13);  // bit 13: negate A
+        const uint32_t Dr = tmem, Di = tmem + TMEM_COLS / 2;
         for (int i = 0; i < nchunks; i++) {
             const int slot = i % S;
             if (!dat_wait(&full[slot], (i / S) & 1)) {
@@ -453,53 +455,63 @@ __global__ void __launch_bounds__(tcg::THREADS, 1) k_cgemm_tc(const CGemmArgs a,
             }
             if (*abort_flag) break;
             tc::fence_after();
-            const uint32_t st = tc::smem_u32(smem + slot * STAGE);
-            const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
-#pragma unroll
-            for (int s = 0; s < KR / 8; s++) {
-                const uint32_t ao = s * 2 * AK, bo = s * 2 * BK;
-                const uint64_t dah = tc::sdesc(ah + ao, AK, 128), dal = tc::sdesc(al + ao, AK, 128);
-                const uint64_t dbh = tc::sdesc(bh + bo, BK, 128), dbl = tc::sdesc(bl + bo, BK, 128);
-                tc::mma_tf32(tmem, dah, dbh, idesc, (i > 0 || s > 0) ? 1u : 0u);
-                tc::mma_tf32(tmem, dah, dbl, idesc, 1u);
-                tc::mma_tf32(tmem, dal, dbh, idesc, 1u);
-            }
+            const uint32_t st = tc::smem_u32(smem + slot * STAGE), sb = st + 4 * A_PLANE;
+            const uint64_t arh = tc::sdesc(st, AK, 128), arl = tc::sdesc(st + A_PLANE, AK, 128);
+            const uint64_t aih = tc::sdesc(st + 2 * A_PLANE, AK, 128), ail = tc::sdesc(st + 3 * A_PLANE, AK, 128);
+            const uint64_t brh = tc::sdesc(sb, BK, 128), brl = tc::sdesc(sb + B_PLANE, BK, 128);
+            const uint64_t bih = tc::sdesc(sb + 2 * B_PLANE, BK, 128), bil = tc::sdesc(sb + 3 * B_PLANE, BK, 128);
+            const uint32_t acc = i > 0 ? 1u : 0u;
+            tc::mma_tf32(Dr, arh, brh, id, acc);
+            tc::mma_tf32(Dr, arh, brl, id, 1u);
+            tc::mma_tf32(Dr, arl, brh, id, 1u);
+            tc::mma_tf32(Dr, aih, bih, id_neg, 1u);
+            tc::mma_tf32(Dr, aih, bil, id_neg, 1u);
+            tc::mma_tf32(Dr, ail, bih, id_neg, 1u);
+            tc::mma_tf32(Di, arh, bih, id, acc);
+            tc::mma_tf32(Di, arh, bil, id, 1u);
+            tc::mma_tf32(Di, arl, bih, id, 1u);
+            tc::mma_tf32(Di, aih, brh, id, 1u);
+            tc::mma_tf32(Di, aih, brl, id, 1u);
+            tc::mma_tf32(Di, ail, brh, id, 1u);
             tc::commit(&empty[slot]);
         }
         tc::commit(done);  // tracks every MMA issued, also after an abort
     }
     __syncwarp();
-    // ---- epilogue: warps 0-15 read the accumulator; warp w owns TMEM lanes
-    // 32 (w % 4) .. +31 and real columns 64 (w / 4) .. +63
+    // ---- epilogue: warps 0-15 read the accumulators; warp w owns TMEM lanes
+    // 32 (w % 4) .. +31 and a quarter of the columns, 32 at a time
     bool ok = true;
     if (warp < PRODUCERS || lane == 0) ok = dat_wait(done, 0);
     if (!ok) atomicExch(status, 3);
     if (warp < PRODUCERS) {
         tc::fence_after();
+        constexpr int QC = (TNC / 4 + 31) / 32 * 32;  // columns per quarter, whole 32-column loads
         const int q = warp & 3, quarter = warp >> 2;
         const int gm = m0 + 32 * q + lane;
+        const uint32_t lanes = (uint32_t)(32 * q) << 16;
         const bool live = __all_sync(0xffffffffu, ok && !*abort_flag);  // warp-uniform: TMEM loads are collective
-        for (int cb = 0; cb < 2; cb++) {
-            float v[32];
-            const int c0 = 64 * quarter + 32 * cb;  // real column of the tile
-            if (c0 >= TN) break;  // the accumulator's unused columns
+        for (int cb = 0; cb < QC; cb += 32) {
+            const int c0 = quarter * QC + cb;
+            if (c0 >= TNC) break;  // the accumulators' unused columns
+            float vr[32], vi[32];
             if (nchunks > 0 && live) {
-                tc::tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
+                tc::tmem_ld32(tmem + lanes + c0, vr);
+                tc::tmem_ld32(tmem + lanes + TMEM_COLS / 2 + c0, vi);
             } else {
 #pragma unroll
-                for (int c = 0; c < 32; c++) v[c] = 0.0f;
+                for (int c = 0; c < 32; c++) vr[c] = vi[c] = 0.0f;
             }
             if (gm < a.M && live) {
-                float2 *dst = C + (size_t)gm * a.ldc + n0 + c0 / 2;
+                float2 *dst = C + (size_t)gm * a.ldc + n0 + c0;
 #pragma unroll
-                for (int c = 0; c < 16; c++)
-                    if (c0 / 2 + c < TNC && n0 + c0 / 2 + c < a.N) dst[c] = make_float2(v[2 * c], v[2 * c + 1]);
+                for (int c = 0; c < 32; c++)
+                    if (c0 + c < TNC && n0 + c0 + c < a.N) dst[c] = make_float2(vr[c], vi[c]);
             }
         }
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == PRODUCERS) tc::tmem_free(tmem, 256);
+    if (warp == PRODUCERS) tc::tmem_free(tmem, TMEM_COLS);
 }
 
 // cmp = 1 receiver side (:493-546 with s_abs = s0 + is ds): one thread per
