@@ -151,8 +151,9 @@ __global__ void __launch_bounds__(128) k_dat_op(const DatOpArgs a)
                 si = ti;
             }
         }
-        // exp(-i w m) with the phase reduced exactly: (iw m) mod nfft
-        const long long red = ((long long)iw * m) % (long long)a.nfft;
+        // exp(-i w m) with the phase reduced exactly: (iw m) mod nfft, nfft a
+        // power of two and iw m >= 0
+        const long long red = ((long long)iw * m) & (long long)(a.nfft - 1);
         float es, ec;
         sincospif(__fdiv_rn(2.0f * (float)red, (float)a.nfft), &es, &ec);
         const double lr = (1.0 - delta) + delta * zr, li = delta * zi;  // (1-delta) + delta exp(+i w)
