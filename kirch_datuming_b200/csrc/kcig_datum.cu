@@ -59,21 +59,44 @@ struct DatOpArgs {
     float dt, antialias;
 };
 
-// antialias_weight_iw (:197-226), in the reference's float arithmetic
-__device__ __forceinline__ float dat_aa(float antialias, int iw, float dtau, int nfft, float dt)
+// antialias_weight_iw (:197-226), in the reference's float arithmetic, its
+// per-term part (fnyq, fmax, fpass) taken once per term and the frequency
+// iw / (nfft dt) once per chunk: the same float operations, the same weights.
+// mode 1: the weight is 1 at every frequency; 0: 0 at iw > 0; 2: the taper
+// between fpass and fmax
+struct DatAa {
+    int mode;
+    float fpass, fmax, den;
+};
+
+__device__ __forceinline__ DatAa dat_aa_term(float antialias, float dtau, float dt)
 {
-    if (antialias <= 0.0f || iw <= 0) return 1.0f;
+    DatAa t{1, 0.0f, 0.0f, 0.0f};
+    if (antialias <= 0.0f) return t;
     dtau = __fmul_rn(fabsf(dtau), antialias);
-    if (dtau <= 1e-12f || !isfinite(dtau)) return 1.0f;
-    const float freq = __fdiv_rn((float)iw, __fmul_rn((float)nfft, dt));
+    if (dtau <= 1e-12f || !isfinite(dtau)) return t;
     const float fnyq = __fdiv_rn(0.5f, dt);
     const float fmax = __fdiv_rn(0.5f, dtau);
-    if (fmax >= fnyq) return 1.0f;
-    if (fmax <= 0.0f) return 0.0f;
-    const float fpass = __fmul_rn(0.8f, fmax);
-    if (freq <= fpass) return 1.0f;
-    if (freq >= fmax) return 0.0f;
-    const float x = __fdiv_rn(__fsub_rn(freq, fpass), __fsub_rn(fmax, fpass));
+    if (fmax >= fnyq) return t;
+    if (fmax <= 0.0f) {
+        t.mode = 0;
+        return t;
+    }
+    t.mode = 2;
+    t.fmax = fmax;
+    t.fpass = __fmul_rn(0.8f, fmax);
+    t.den = __fsub_rn(fmax, t.fpass);
+    return t;
+}
+
+// freq = iw / (nfft dt) as dat_aa forms it
+__device__ __forceinline__ float dat_aa_at(const DatAa &t, int iw, float freq)
+{
+    if (t.mode == 1 || iw <= 0) return 1.0f;
+    if (t.mode == 0) return 0.0f;
+    if (freq <= t.fpass) return 1.0f;
+    if (freq >= t.fmax) return 0.0f;
+    const float x = __fdiv_rn(__fsub_rn(freq, t.fpass), t.den);
     return __fmul_rn(0.5f, __fadd_rn(1.0f, cospif(x)));
 }
 
@@ -91,12 +114,15 @@ __device__ __forceinline__ double dat_root(int j, double dt_over_tau)
 // (1-delta) exp(-i w m) + delta exp(-i w (m-1)), m = ceil(tau/dt) (:128-181).
 __global__ void __launch_bounds__(128) k_dat_op(const DatOpArgs a)
 {
-    extern __shared__ double zs[];  // [nf][2]: cos w, sin w of the chunk's frequencies
+    extern __shared__ double zs[];  // [nf][2]: cos w, sin w of the chunk's frequencies; then [nf] frequencies
+    float *fq = reinterpret_cast<float *>(zs + 2 * a.nf);
+    const float fden = __fmul_rn((float)a.nfft, a.dt);
     for (int c = threadIdx.x; c < a.nf; c += blockDim.x) {
         double s, co;
         sincospi(2.0 * (double)(a.f0 + c) / (double)a.nfft, &s, &co);
         zs[2 * c] = co;
         zs[2 * c + 1] = s;
+        fq[c] = __fdiv_rn((float)(a.f0 + c), fden);
     }
     __syncthreads();
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,9 +148,10 @@ __global__ void __launch_bounds__(128) k_dat_op(const DatOpArgs a)
     }
     const double q = (double)d.tau * inv_dt, mceil = ceil(q), delta = mceil - q;
     const long long m = (long long)mceil;
+    const DatAa aa = dat_aa_term(a.antialias, d.dtau, a.dt);
     for (int c = 0; c < a.nf; c++) {
         const int iw = a.f0 + c;
-        const float wa = __fmul_rn(d.w, dat_aa(a.antialias, iw, d.dtau, a.nfft, a.dt));
+        const float wa = __fmul_rn(d.w, dat_aa_at(aa, iw, fq[c]));
         if (fabsf(wa) < 1e-20f) {  // the reference skips these terms (:525)
             o[(size_t)c * a.ne] = make_float2(0.0f, 0.0f);
             continue;
@@ -1182,7 +1209,7 @@ int launch_op(const DatEntry *ent, int ne, float2 *out, int f0, int nf, int nfft
     a.K = K;
     a.dt = p.dt;
     a.antialias = p.antialias;
-    k_dat_op<<<(ne + 127) / 128, 128, (size_t)nf * 2 * sizeof(double), st>>>(a);
+    k_dat_op<<<(ne + 127) / 128, 128, (size_t)nf * (2 * sizeof(double) + sizeof(float)), st>>>(a);
     launches++;
     KCIG_CUDA(cudaGetLastError());
     return KCIG_OK;
